@@ -1,0 +1,385 @@
+"""Benchmark: bond-force updates/s of the per-step force path on B200.
+
+One bench "step" is one full specimen run: ``--sim-steps`` velocity-Verlet
+time steps (default: the workload's configured count) starting from the
+same initial state, i.e. one pass of the hot path over one batch of
+synthetic input.
+
+  value     device time with the state resident in HBM (CUDA events on the
+            library's stream), state/bond reset and an L2 flush between
+            iterations (outside the timed region).
+  e2e       the same run through the public API with host buffers: upload
+            of y, v from pinned memory, the run, download of y, v and damage,
+            all inside the timed region.
+  roofline  the bond-force kernel's algorithmic bytes per launch over its
+            average launch time (events around each launch, live).
+
+``--impl reference`` times the CPU restatement of the reference loop
+(oracle/, OpenMP over particles on all host cores) on a bounded sample of
+the same workload.
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torch.distributed.run, one rank per GPU, each rank advancing its own
+specimen (independent specimens: weak scaling, no data-path collective).
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bond-force updates/s"
+UNIT = "bond-updates/s"
+
+
+def build_workload(name, args):
+    from peridyn_b200 import configs
+
+    if name == "lps_bar":
+        return configs.lps_bar()
+    if name == "pmb_cube":
+        return configs.pmb_cube()
+    if name == "batched":
+        return configs.batched_cubes(nspec=args.nspec)
+    if name == "disk_impact":
+        return configs.disk_impact()
+    raise SystemExit(f"unknown workload {name}")
+
+
+# bytes per particle the bond-force kernel must move, by precision and kind
+# ("Algorithmic bytes"); bond term: 4 B index + 1 intact bit
+BOND_BYTES = 4.125
+
+
+def particle_bytes(precision, lps):
+    if precision == "fp64_serial":
+        return 104 + (16 if lps else 0)  # x4 32 + y 32 + f 32 + cnt/tinfo 8 (+ m,theta 16)
+    if precision == "fp64":
+        return 104 + (16 if lps else 0)
+    return 84 + (8 if lps else 0)  # fp32c
+
+
+class ClockSampler:
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_sample(work, seconds, nthreads):
+    """Oracle (CPU restatement of the reference loop) on a bounded sample."""
+    from oracle import oracle
+
+    ora = oracle.OracleEnv(work["materials"], work["contacts"], work["bcs"], work["dt"], nthreads=nthreads)
+    ora.apply_bc_at0()
+    bonds0 = sum(int(B.intact.sum()) for B in ora.blocks)
+    t0 = time.perf_counter()
+    ora.vv_step()
+    one = time.perf_counter() - t0
+    nsteps = max(1, min(10000, int(seconds / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        ora.vv_step()
+    dt = time.perf_counter() - t0
+    bonds1 = sum(int(B.intact.sum()) for B in ora.blocks)
+    rate = 0.5 * (bonds0 + bonds1) * nsteps / dt
+    return rate, nsteps, dt
+
+
+def traffic_for(workload, precision):
+    """Per-launch DRAM bytes of the bond kernel from a committed ncu
+    summary (profiles/roofline_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(f"{workload}/{precision}")
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    work = build_workload(args.workload, args)
+    nthreads = os.cpu_count() or 1
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    samples = []
+    for k in range(args.warmup + args.steps):
+        rate, n, dt = cpu_sample(work, per_step, nthreads)
+        if k >= args.warmup:
+            vals.append(rate)
+            samples.append((n, dt))
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": work["workload"], "precision": "fp64", "particles": None},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"{samples[0][0]} velocity-Verlet steps per bench step of "
+                                       f"{work['workload']} (OpenMP, atomic scatter)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lps_bar", choices=["lps_bar", "pmb_cube", "batched", "disk_impact"])
+    ap.add_argument("--precision", default="fp64_serial", choices=["fp64_serial", "fp64", "fp32c"])
+    ap.add_argument("--sim-steps", type=int, default=0, help="VV steps per bench step (default: workload's)")
+    ap.add_argument("--nspec", type=int, default=256)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import peridyn_b200 as pb
+    from peridyn_b200 import _abi
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    work = build_workload(args.workload, args)
+    sim_steps = args.sim_steps or work["steps"]
+    env = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision=args.precision,
+                 device=local)
+    L = _abi.lib()
+    stream_ptr = ctypes_void()
+    _abi.check(L.pd_env_stream(env._h, ctypes.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=torch.device("cuda", local))
+    lps = any(m.specific.kind == 1 for m in work["materials"])
+    y0, v0, _, _ = env.get_state()
+    # pinned host copies for the end-to-end arm
+    hy = torch.from_numpy(np.ascontiguousarray(y0.T)).pin_memory()
+    hv = torch.from_numpy(np.ascontiguousarray(v0.T)).pin_memory()
+    out_y = torch.empty_like(hy).pin_memory()
+    out_v = torch.empty_like(hv).pin_memory()
+    out_d = torch.empty(env.N, dtype=torch.float64).pin_memory()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def reset():
+        env.set_state(y=y0, v=v0, f=np.zeros_like(y0))
+        _abi.check(L.pd_env_reset_bonds(env._h))
+        env.time_step = 0
+        if work["bcs"]:
+            pb.apply_bc_at0(env, 0)
+        pb.update_neighs(env)
+        pb.update_acc(env)  # the run's initial force evaluation (save_state! at t0)
+
+    def one_run():
+        _abi.check(L.pd_env_vv_steps(env._h, sim_steps))
+
+    bonds_start = None
+    # warm-up
+    for _ in range(args.warmup):
+        reset()
+        one_run()
+    # timed: device-resident
+    times = []
+    bonds = []
+    launches0 = _abi.kernel_launches()
+    _abi.check(L.pd_env_profile(env._h, 1))
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            reset()
+            b0 = env.num_bonds()
+            flush.zero_()
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            one_run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+            b1 = env.num_bonds()
+            bonds.append(0.5 * (b0 + b1) * sim_steps)
+            bonds_start = b0
+    launches = _abi.kernel_launches() - launches0
+    prof_ms = ctypes_double()
+    prof_n = ctypes_i64()
+    _abi.check(L.pd_env_profile_read(env._h, ctypes.byref(prof_ms), ctypes.byref(prof_n)))
+    _abi.check(L.pd_env_profile(env._h, 0))
+    t_total = float(sum(times))
+    if dist is not None:
+        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+        nb = torch.tensor([sum(bonds)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(nb, op=dist.ReduceOp.SUM)
+        total_bonds = float(nb.item())
+    else:
+        total_bonds = float(sum(bonds))
+    value = total_bonds / t_total
+    # end-to-end through the public API with host buffers
+    h2d = hy.numel() * 8 + hv.numel() * 8
+    d2h = out_y.numel() * 8 + out_v.numel() * 8 + out_d.numel() * 8
+    e2e_times = []
+    for _ in range(args.steps):
+        _abi.check(L.pd_env_reset_bonds(env._h))
+        env.time_step = 0
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        yv = hy.numpy().T
+        vv = hv.numpy().T
+        _abi.check(L.pd_env_set_state(env._h, _abi.dptr(np.asfortranarray(yv)), _abi.dptr(np.asfortranarray(vv)),
+                                      None))
+        if work["bcs"]:
+            pb.apply_bc_at0(env, 0)
+        pb.update_neighs(env)
+        pb.update_acc(env)
+        one_run()
+        ybuf = out_y.numpy()
+        vbuf = out_v.numpy()
+        _abi.check(L.pd_env_get_state(env._h, ybuf.ctypes.data_as(_abi.c_dp), vbuf.ctypes.data_as(_abi.c_dp),
+                                      None, None))
+        _abi.check(L.pd_env_damage(env._h, out_d.numpy().ctypes.data_as(_abi.c_dp)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    e2e_t = float(sum(e2e_times))
+    if dist is not None:
+        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = total_bonds / e2e_t
+    # roofline of the bond-force kernel
+    n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
+    bytes_launch = bonds_start * BOND_BYTES + n_int * particle_bytes(args.precision, lps)
+    avg_ms = prof_ms.value / max(1, prof_n.value)
+    achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = traffic_for(work["workload"], args.precision)
+    clk = clocks.summary()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp64_serial": "f64", "fp64": "f64", "fp32c": "f32 (f64 position accumulator)"}[args.precision],
+        "data": "synthetic",
+        "config": {"workload": work["workload"], "precision": args.precision, "particles": int(env.N),
+                   "intact_bonds": int(bonds_start), "vv_steps_per_step": int(sim_steps), "dt": work["dt"],
+                   "l2": "256 MB buffer written between timed iterations",
+                   "parallelism": f"specimen replicas x{world}" if world > 1 else "1 GPU"},
+        "hbm_gbs_algorithmic": bytes_launch * sim_steps * args.steps / t_total / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "bond force (k_force_serial)" if args.precision == "fp64_serial" else "bond force",
+                     "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms, "launches_timed": int(prof_n.value),
+                     "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured"
+                     else "fallback 6650 GB/s"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        rate, n, dt = cpu_sample(work, args.cpu_sample_s, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"{n} velocity-Verlet steps of {work['workload']} in {dt:.1f} s "
+                                          f"(OpenMP over particles, atomic scatter)"}
+    env.close()
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def ctypes_void():
+    import ctypes
+
+    return ctypes.c_void_p()
+
+
+def ctypes_double():
+    import ctypes
+
+    return ctypes.c_double()
+
+
+def ctypes_i64():
+    import ctypes
+
+    return ctypes.c_int64()
+
+
+if __name__ == "__main__":
+    main()

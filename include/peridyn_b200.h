@@ -1,0 +1,245 @@
+/*
+ * peridyn_b200.h -- C ABI of libperidyn_b200.so, the B200 (sm_100a)
+ * implementation of PeriDyn's per-step force path.
+ *
+ * The library is the body behind the reference's CUDA dispatch points:
+ *   force_density_T!(f, y, limits, mat, ::Type{Val{:cuda}})
+ *       reference: src/materials/general_material.jl:388-390 (throws today)
+ *   dilatation!(theta, ..., ::Type{Val{:cuda}})     src/peri.jl:283-315
+ *   short_range_contact!(..., ::Type{Val{:cuda}})   src/contacts/contacts.jl:189-336
+ *   update_contact_neighs!(..., ::Type{Val{:cuda}}) src/contacts/contacts.jl:434-639
+ *   apply_solver!(env, ::DSVelocityVerlet)           src/solvers/velocity_verlet.jl:27
+ *   apply_solver!(env, ::QSDrag)                     src/solvers/minimize.jl:74
+ *   update_acc!(env)                                 src/solvers/solvers.jl:320-336
+ *   cal_damage(env)                                  src/peri.jl:587-594
+ *
+ * Conventions
+ *  - Host arrays use the reference's layouts: positions/velocities/
+ *    accelerations are 3xN column-major Float64 (x[3*i + d]); family is
+ *    M'xN column-major Int64, 1-based block-local indices in descending order
+ *    with 0 padding; intact is M'xN Bool (uint8).
+ *  - Every function returns a pd_status; 0 is success.  No C++ exception
+ *    and no abort crosses the ABI.  pd_last_error() returns a message for
+ *    the most recent failure on the calling thread.
+ *  - The library copies host inputs into device-owned memory; no host
+ *    pointer is kept after a call returns.
+ *  - An environment is not thread-safe: one host thread per pd_env.  Each
+ *    environment owns one CUDA stream on its device.
+ *  - There is no CPU fallback: without a usable CUDA device every compute
+ *    call fails with PD_ERR_NO_DEVICE.
+ */
+#ifndef PERIDYN_B200_H
+#define PERIDYN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PD_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define PD_API __attribute__((visibility("default")))
+#else
+#define PD_API
+#endif
+
+typedef int32_t pd_status;
+enum {
+    PD_OK = 0,
+    PD_ERR_ARG = 1,             /* invalid argument / inconsistent sizes        */
+    PD_ERR_OOM = 2,             /* device or host allocation failed             */
+    PD_ERR_FAMILY_OVERFLOW = 3, /* a family does not fit max_neigh (reference:
+                                   BoundsError in cal_family!/GeneralMaterial) */
+    PD_ERR_NAN = 4,             /* NaN/Inf detected by pd_env_check_finite      */
+    PD_ERR_CUDA = 5,            /* CUDA runtime error                           */
+    PD_ERR_TIMEOUT = 6,         /* a bounded device wait gave up                */
+    PD_ERR_STATE = 7,           /* call not valid in the environment's state    */
+    PD_ERR_NO_DEVICE = 8,       /* no usable CUDA device                        */
+    PD_ERR_UNSUPPORTED = 9      /* valid input the chosen mode does not support */
+};
+
+/* Material kinds: src/materials/bond_based.jl, ordinary_state_based.jl,
+ * skip_specific.jl. */
+enum { PD_MAT_BOND_BASED = 0, PD_MAT_ORDINARY_STATE_BASED = 1, PD_MAT_SKIP = 2 };
+
+/* Arithmetic modes.
+ * PD_PREC_FP64_SERIAL: FP64, no fused multiply-add, every particle's
+ *   force summed in the exact order of the reference's serial loop
+ *   (general_material.jl:330-368) -> bit-identical forces, trajectories and
+ *   broken-bond sets.
+ * PD_PREC_FP64: FP64, one gather pass per bond pair side, FMA allowed.
+ * PD_PREC_FP32C: FP32 bond arithmetic on FP32 displacements with the
+ *   cancellation-free stretch, FP64 position accumulator. */
+enum { PD_PREC_FP64_SERIAL = 0, PD_PREC_FP64 = 1, PD_PREC_FP32C = 2 };
+
+/* Boundary conditions: FixBC.jl, ToFroBC.jl (MoveBC = ToFroBC, freq=Inf). */
+enum { PD_BC_FIX = 0, PD_BC_TOFRO = 1 };
+
+/* Contact models: contacts.jl ContactModel12 (two blocks) / ContactModel11
+ * (self contact of one block); force law nonlinearspring.jl:124-145. */
+enum { PD_CONTACT_12 = 0, PD_CONTACT_11 = 1 };
+
+typedef struct pd_env pd_env;
+
+/* Specific-material parameters of one block (reference: BondBasedSpecific /
+ * OrdinaryStateBasedSpecific / SkipSpecific).  Matrices are ntypes x ntypes
+ * column-major and must be symmetric; density has ntypes entries.  Types are
+ * the reference's global type ids; the block's types are
+ * type_start .. type_start+ntypes-1 (mat.type = minimum:maximum). */
+typedef struct pd_material_desc {
+    int32_t kind;                   /* PD_MAT_*                                  */
+    int32_t ntypes;                 /* >= 1, <= 255                              */
+    int64_t type_start;             /* first global type id of the block         */
+    const double *bond_stiffness;   /* PMB: 18K/(pi*horizon^4) (bond_based.jl:58) */
+    const double *bulk_modulus;     /* LPS: K                                     */
+    const double *shear_modulus;    /* LPS: G                                     */
+    const double *critical_stretch; /* all kinds (SKIP: ignored)                  */
+    const double *density;          /* ntypes                                     */
+    double horizon;
+    double particle_size;           /* GeneralMaterial particle_size              */
+    int64_t max_neigh;              /* GeneralMaterial max_neigh                  */
+} pd_material_desc;
+
+/* ---------------------------------------------------------------------- */
+/* Library                                                                 */
+/* ---------------------------------------------------------------------- */
+PD_API int pd_abi_version(void);
+PD_API const char *pd_status_string(pd_status s);
+PD_API const char *pd_last_error(void);
+/* Number of CUDA devices visible (0 when none). */
+PD_API pd_status pd_device_count(int32_t *count);
+
+/* ---------------------------------------------------------------------- */
+/* Environment assembly: Env(id, materials, contacts, bcs, dt)             */
+/* (src/environment.jl:166-235)                                           */
+/* ---------------------------------------------------------------------- */
+PD_API pd_status pd_env_create(pd_env **out, int32_t device, int32_t precision, double dt);
+PD_API pd_status pd_env_destroy(pd_env *env);
+
+/* Append one material block (GeneralMaterial(y0, v0, x, volume, type,
+ * horizon; max_neigh), general_material.jl:81-98).  Blocks occupy
+ * consecutive particle ranges in call order.  x, y, v: 3xn; volume: n;
+ * type: n global type ids. */
+PD_API pd_status pd_env_add_block(pd_env *env, int64_t n, const double *x, const double *y,
+                           const double *v, const double *volume, const int64_t *type,
+                           const pd_material_desc *mat, int64_t *out_block);
+
+/* Replace the family of a block with one computed by the host (the
+ * reference layout: rows x n, 1-based block-local, descending, 0 pad).
+ * intact may be NULL (all entries > 0 intact).  Must precede finalize. */
+PD_API pd_status pd_env_set_family(pd_env *env, int64_t block, int64_t rows, const int64_t *family,
+                            const uint8_t *intact);
+
+/* Contact model between blocks (kind PD_CONTACT_12, block1 -> pair[1],
+ * block2 -> pair[2]) or within block1 (PD_CONTACT_11, block2 ignored).
+ * equi_dist, distance, max_neighs as computed by ContactModel12_gcal /
+ * ContactModel11_gcal (contacts.jl:76-124). */
+PD_API pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block1, int64_t block2,
+                             double exponent, double stiffness, double equi_dist,
+                             double distance, int64_t max_neighs, int64_t *out_contact);
+
+/* Boundary condition over all N particles of the environment (mask: N
+ * bytes).  dims: 3 flags; rate: 3 values (TOFRO); freq: direction flip
+ * period (INFINITY for MoveBC); applyafter: steps before flipping starts. */
+PD_API pd_status pd_env_add_bc(pd_env *env, int32_t kind, const uint8_t *mask, const uint8_t *dims,
+                        const double *rate, double freq, int64_t applyafter,
+                        int32_t onlyatstart, int64_t *out_bc);
+
+/* Build everything on the device: families (GPU cell binning + sort,
+ * peri.jl:459-576 and general_material.jl:85-90, unless set by
+ * pd_env_set_family), weighted volumes (peri.jl:342-354), intact0
+ * (environment.jl:169), masses/densities (environment.jl:173-214). */
+PD_API pd_status pd_env_finalize(pd_env *env);
+
+/* Sizes after finalize. */
+PD_API pd_status pd_env_num_particles(const pd_env *env, int64_t *n);
+PD_API pd_status pd_env_num_bonds(pd_env *env, int64_t *intact_bonds);
+PD_API pd_status pd_env_family_rows(const pd_env *env, int64_t block, int64_t *rows);
+/* Family / intact of a block in the reference layout (rows x n). */
+PD_API pd_status pd_env_get_family(pd_env *env, int64_t block, int64_t *family, uint8_t *intact);
+/* Weighted volume m of a block (n). */
+PD_API pd_status pd_env_get_weighted_volume(pd_env *env, int64_t block, double *m);
+/* Dilatation theta of an LPS block as of the last force evaluation (n). */
+PD_API pd_status pd_env_get_theta(pd_env *env, int64_t block, double *theta);
+
+/* ---------------------------------------------------------------------- */
+/* State                                                                   */
+/* ---------------------------------------------------------------------- */
+/* Any pointer may be NULL.  3xN column-major. */
+PD_API pd_status pd_env_get_state(pd_env *env, double *y, double *v, double *f, double *p);
+PD_API pd_status pd_env_set_state(pd_env *env, const double *y, const double *v, const double *f);
+/* Per-particle mass, volume and density (N each; NULL skips). */
+PD_API pd_status pd_env_get_mass(pd_env *env, double *mass, double *volume, double *density);
+PD_API pd_status pd_env_get_time_step(const pd_env *env, int64_t *time_step);
+PD_API pd_status pd_env_set_time_step(pd_env *env, int64_t time_step);
+/* Reset every intact flag to the state right after finalize. */
+PD_API pd_status pd_env_reset_bonds(pd_env *env);
+
+/* ---------------------------------------------------------------------- */
+/* Solver entry points                                                     */
+/* ---------------------------------------------------------------------- */
+/* apply_bc_at0 (solvers.jl:200-206): snapshot BC.last = y[dims, bool]. */
+PD_API pd_status pd_env_apply_bc_at0(pd_env *env);
+/* update_acc! (solvers.jl:320-336): f = material + contact accelerations,
+ * p = m v; breaks bonds with s >= critical stretch. */
+PD_API pd_status pd_env_update_acc(pd_env *env);
+/* nsteps x velocity_verlet_step! (velocity_verlet.jl:57-89). */
+PD_API pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps);
+/* minimize! (minimize.jl:105-231): one QSDrag solver step.  *iters
+ * receives the iteration count (NULL allowed). */
+PD_API pd_status pd_env_qsdrag(pd_env *env, double step_size, double drag, int64_t max_iter,
+                        double x_tol, double f_tol, int64_t *iters);
+/* update_neighs! (solvers.jl:351-361): contact neighbour lists. */
+PD_API pd_status pd_env_update_neighs(pd_env *env, int64_t max_part);
+/* Contact neighbour list in the reference layout (rows x n1 Int64, 1-based
+ * into the pair[2] subset for 12, block-local for 11).  *rows receives
+ * the row count; neighs may be NULL to query it. */
+PD_API pd_status pd_env_get_contact_neighs(pd_env *env, int64_t contact, int64_t *rows,
+                                    int64_t *neighs);
+
+/* ---------------------------------------------------------------------- */
+/* Diagnostics                                                             */
+/* ---------------------------------------------------------------------- */
+/* cal_damage (peri.jl:587-594): N values. */
+PD_API pd_status pd_env_damage(pd_env *env, double *damage);
+/* printdata (environment.jl:308-320): out[0..2] = sum p, out[3..5] =
+ * sum f, out[6] = mean damage, out[7] = intact bond count. */
+PD_API pd_status pd_env_diagnostics(pd_env *env, double *out8);
+/* 1 when every block has left the undeformed state (general_material.jl:
+ * 243-255 gate), per block in flags (NULL allowed). */
+PD_API pd_status pd_env_deformed(pd_env *env, uint8_t *flags);
+/* PD_ERR_NAN when y, v or f holds a NaN or Inf (const_macros.jl:60-74). */
+PD_API pd_status pd_env_check_finite(pd_env *env);
+
+/* ---------------------------------------------------------------------- */
+/* Device-pointer entry point for a single block                           */
+/* ---------------------------------------------------------------------- */
+/* force_density_T!(f, y, limits, mat, Val{:cuda}) for block `block`, on
+ * caller-owned DEVICE arrays of the whole environment (3xN column-major,
+ * e.g. a CuArray's pointer): adds the block's accelerations into f over
+ * its particle range and updates the block's intact flags, exactly as the
+ * reference CPU loop does.  Runs the dilatation pass first for LPS.
+ * stream: cudaStream_t (NULL = the environment's stream). */
+PD_API pd_status pd_force_density_device(pd_env *env, int64_t block, double *f_dev,
+                                  const double *y_dev, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Instrumentation                                                         */
+/* ---------------------------------------------------------------------- */
+/* The environment's CUDA stream (cudaStream_t) -- for timing with events. */
+PD_API pd_status pd_env_stream(pd_env *env, void **stream);
+/* Total kernel launches issued by the library since it was loaded. */
+PD_API pd_status pd_kernel_launches(int64_t *count);
+/* enable != 0: bracket every bond-force kernel launch with CUDA events;
+ * resets the accumulated time.  pd_env_profile_read returns the summed
+ * device time (ms) and the number of timed launches since enabling. */
+PD_API pd_status pd_env_profile(pd_env *env, int32_t enable);
+PD_API pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PERIDYN_B200_H */

@@ -1,0 +1,61 @@
+"""Build libperidyn_b200.so in-tree for sm_100a with nvcc.
+
+The exact-arithmetic translation units (the serial-order FP64 path, the
+contact models and the solver pieces) are compiled with -fmad=false so
+that no multiply-add is fused; the throughput path (pd_fast.cu) keeps FMA.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libperidyn_b200.so")
+BUILD = os.path.join(HERE, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+          "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+
+# (source, extra flags)
+UNITS = [
+    ("pd_exact.cu", ["-fmad=false"]),
+    ("pd_contact.cu", ["-fmad=false"]),
+    ("pd_solver.cu", ["-fmad=false"]),
+    ("pd_env.cu", ["-fmad=false"]),
+    ("pd_fast.cu", ["-fmad=true"]),
+]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed for " + cmd[-1])
+    return r.stdout + r.stderr
+
+
+def build(verbose=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")]
+    headers.append(os.path.join(HERE, "..", "include", "peridyn_b200.h"))
+    hdr_mtime = max(os.path.getmtime(h) for h in headers)
+    objs = []
+    for src, flags in UNITS:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if (not force and os.path.exists(o) and os.path.getmtime(o) > os.path.getmtime(s)
+                and os.path.getmtime(o) > hdr_mtime):
+            continue
+        out = _run([NVCC] + ARCH + COMMON + flags + ["-c", "-o", o, s])
+        if verbose and out:
+            print(out)
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static", "-lrt", "-lpthread", "-ldl"])
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,1001 @@
+// pd_env.cu -- the C ABI (include/peridyn_b200.h): environment assembly,
+// device memory ownership, family construction and the solver sequencing of
+// src/solvers/*.jl on one CUDA stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pd_env_impl.h"
+
+using namespace pd;
+
+#include <atomic>
+
+namespace {
+thread_local std::string g_err;
+std::atomic<int64_t> g_launches{0};
+}  // namespace
+
+namespace pd {
+
+pd_status fail(pd_status s, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void prof_begin(pd_env *env, cudaStream_t st) {
+    if (!env->prof) return;
+    if (env->prof_used + 2 > env->prof_ev.size()) {
+        if (env->prof_ev.size() >= 16384) return;
+        for (int k = 0; k < 256; ++k) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            env->prof_ev.push_back(e);
+        }
+    }
+    cudaEventRecord(env->prof_ev[env->prof_used], st);
+}
+
+void prof_end(pd_env *env, cudaStream_t st) {
+    if (!env->prof || env->prof_used + 2 > env->prof_ev.size()) return;
+    cudaEventRecord(env->prof_ev[env->prof_used + 1], st);
+    env->prof_used += 2;
+}
+
+pd_status cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+    pd_status s = e == cudaErrorMemoryAllocation ? PD_ERR_OOM : PD_ERR_CUDA;
+    return fail(s, "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+}  // namespace pd
+
+pd::Geo pd_env::geo() const {
+    pd::Geo g;
+    g.N = N;
+    g.x4 = x4.p;
+    g.tinfo = tinfo.p;
+    g.blocks = blocks_d.p;
+    g.pairs = pairs.p;
+    g.tdens = tdens.p;
+    g.slice_ptr = slice_ptr.p;
+    g.cnt = cnt.p;
+    g.nbr = nbr.p;
+    g.deformed = deformed.p;
+    return g;
+}
+
+
+// ---------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------
+namespace {
+
+inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+bool symmetric(const std::vector<double> &m, int nt) {
+    for (int i = 0; i < nt; ++i)
+        for (int j = 0; j < nt; ++j)
+            if (!(m[i + j * nt] == m[j + i * nt]) && !(std::isnan(m[i + j * nt]) && std::isnan(m[j + i * nt])))
+                return false;
+    return true;
+}
+
+pd_status check_env(const pd_env *env) {
+    if (!env) return fail(PD_ERR_ARG, "environment handle is NULL");
+    return PD_OK;
+}
+
+pd_status need_final(const pd_env *env) {
+    PD_TRY(check_env(env));
+    if (!env->finalized) return fail(PD_ERR_STATE, "environment is not finalized (call pd_env_finalize)");
+    return PD_OK;
+}
+
+// Binning for the family search: cubic cells one horizon (times 1+1e-9)
+// wide, stable counting sort by cell.  Any binning whose cells are at
+// least a horizon wide yields the same family sets; the order is fixed
+// afterwards by sorting.
+struct Cells {
+    int3 dims;
+    std::vector<int32_t> cell_of, start, list;
+};
+
+Cells bin_block(const HostBlock &b, int64_t first_int) {
+    Cells c;
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = 0; i < b.n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            mn[d] = std::min(mn[d], b.x[3 * i + d]);
+            mx[d] = std::max(mx[d], b.x[3 * i + d]);
+        }
+    double cell = b.horizon * (1.0 + 1e-9);
+    int dims[3];
+    for (int d = 0; d < 3; ++d) {
+        double span = b.n > 0 ? (mx[d] - mn[d]) / cell : 0.0;
+        double nd = std::floor(span) + 1.0;
+        if (!(nd >= 1.0)) nd = 1.0;
+        if (nd > 1024.0) nd = 1024.0;  // wider domains fold into the edge cells
+        dims[d] = (int)nd;
+    }
+    c.dims = make_int3(dims[0], dims[1], dims[2]);
+    int64_t ncell = (int64_t)dims[0] * dims[1] * dims[2];
+    c.cell_of.resize(b.n);
+    std::vector<int32_t> count(ncell + 1, 0);
+    for (int64_t i = 0; i < b.n; ++i) {
+        int ijk[3];
+        for (int d = 0; d < 3; ++d) {
+            double q = std::floor((b.x[3 * i + d] - mn[d]) / cell);
+            if (!(q >= 0.0)) q = 0.0;
+            if (q > dims[d] - 1) q = dims[d] - 1;
+            ijk[d] = (int)q;
+        }
+        int32_t cid = ijk[0] + dims[0] * (ijk[1] + dims[1] * ijk[2]);
+        c.cell_of[i] = cid;
+        count[cid + 1]++;
+    }
+    for (int64_t k = 0; k < ncell; ++k) count[k + 1] += count[k];
+    c.start = count;
+    c.list.resize(b.n);
+    std::vector<int32_t> fill(ncell, 0);
+    for (int64_t i = 0; i < b.n; ++i) {
+        int32_t cid = c.cell_of[i];
+        c.list[c.start[cid] + fill[cid]++] = (int32_t)(first_int + i);
+    }
+    return c;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------
+// ABI: library
+// ---------------------------------------------------------------------
+extern "C" int pd_abi_version(void) { return PD_ABI_VERSION; }
+
+extern "C" const char *pd_status_string(pd_status s) {
+    switch (s) {
+        case PD_OK: return "ok";
+        case PD_ERR_ARG: return "invalid argument";
+        case PD_ERR_OOM: return "out of memory";
+        case PD_ERR_FAMILY_OVERFLOW: return "family exceeds max_neigh";
+        case PD_ERR_NAN: return "non-finite value";
+        case PD_ERR_CUDA: return "CUDA error";
+        case PD_ERR_TIMEOUT: return "device wait timed out";
+        case PD_ERR_STATE: return "invalid state";
+        case PD_ERR_NO_DEVICE: return "no CUDA device";
+        case PD_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+extern "C" const char *pd_last_error(void) { return g_err.c_str(); }
+
+extern "C" pd_status pd_device_count(int32_t *count) {
+    if (!count) return fail(PD_ERR_ARG, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// ABI: environment assembly
+// ---------------------------------------------------------------------
+extern "C" pd_status pd_env_create(pd_env **out, int32_t device, int32_t precision, double dt) {
+    if (!out) return fail(PD_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (precision < PD_PREC_FP64_SERIAL || precision > PD_PREC_FP32C)
+        return fail(PD_ERR_ARG, "unknown precision mode %d", precision);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(PD_ERR_NO_DEVICE, "no CUDA device is visible; libperidyn_b200 has no CPU path");
+    }
+    if (device < 0 || device >= n) return fail(PD_ERR_ARG, "device %d out of range (%d visible)", device, n);
+    std::unique_ptr<pd_env> env(new (std::nothrow) pd_env());
+    if (!env) return fail(PD_ERR_OOM, "host allocation failed");
+    env->device = device;
+    env->precision = precision;
+    env->dt = dt;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&env->st, cudaStreamNonBlocking));
+    *out = env.release();
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_destroy(pd_env *env) {
+    if (!env) return PD_OK;
+    cudaSetDevice(env->device);
+    if (env->st) cudaStreamSynchronize(env->st);
+    env->release_device();
+    for (cudaEvent_t e : env->prof_ev) cudaEventDestroy(e);
+    if (env->st) cudaStreamDestroy(env->st);
+    delete env;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_add_block(pd_env *env, int64_t n, const double *x, const double *y,
+                                      const double *v, const double *volume,
+                                      const int64_t *type, const pd_material_desc *mat,
+                                      int64_t *out_block) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (!env->hbc.empty()) return fail(PD_ERR_STATE, "blocks must be added before boundary conditions");
+    if (n <= 0 || !x || !y || !v || !volume || !type || !mat)
+        return fail(PD_ERR_ARG, "pd_env_add_block: NULL array or n <= 0");
+    if (n > (int64_t)1 << 30) return fail(PD_ERR_ARG, "block too large (%lld)", (long long)n);
+    if (mat->kind < PD_MAT_BOND_BASED || mat->kind > PD_MAT_SKIP)
+        return fail(PD_ERR_ARG, "unknown material kind %d", mat->kind);
+    if (mat->ntypes < 1 || mat->ntypes > 255) return fail(PD_ERR_ARG, "ntypes must be 1..255");
+    if (!mat->density) return fail(PD_ERR_ARG, "density is NULL");
+    if (!(mat->horizon > 0.0) && mat->kind != PD_MAT_SKIP) return fail(PD_ERR_ARG, "horizon must be > 0");
+    const int nt = mat->ntypes;
+    const size_t nt2 = (size_t)nt * nt;
+    HostBlock b;
+    b.n = n;
+    b.kind = mat->kind;
+    b.nt = nt;
+    b.type_start = mat->type_start;
+    b.horizon = mat->horizon;
+    b.particle_size = mat->particle_size;
+    b.max_neigh = mat->max_neigh;
+    b.x.assign(x, x + 3 * n);
+    b.y.assign(y, y + 3 * n);
+    b.v.assign(v, v + 3 * n);
+    b.vol.assign(volume, volume + n);
+    b.type.assign(type, type + n);
+    for (int64_t i = 0; i < n; ++i)
+        if (type[i] < mat->type_start || type[i] >= mat->type_start + nt)
+            return fail(PD_ERR_ARG, "particle %lld has type %lld outside the block's type range", (long long)i,
+                        (long long)type[i]);
+    b.dens.assign(mat->density, mat->density + nt);
+    b.cs.assign(nt2, INFINITY);
+    b.c.assign(nt2, 0.0);
+    b.K.assign(nt2, 0.0);
+    b.G.assign(nt2, 0.0);
+    if (mat->kind != PD_MAT_SKIP) {
+        if (!mat->critical_stretch) return fail(PD_ERR_ARG, "critical_stretch is NULL");
+        b.cs.assign(mat->critical_stretch, mat->critical_stretch + nt2);
+        if (!symmetric(b.cs, nt)) return fail(PD_ERR_ARG, "critical_stretch must be symmetric");
+        if (mat->max_neigh < 1) return fail(PD_ERR_ARG, "max_neigh must be >= 1");
+    }
+    if (mat->kind == PD_MAT_BOND_BASED) {
+        if (!mat->bond_stiffness) return fail(PD_ERR_ARG, "bond_stiffness is NULL");
+        b.c.assign(mat->bond_stiffness, mat->bond_stiffness + nt2);
+    }
+    if (mat->kind == PD_MAT_ORDINARY_STATE_BASED) {
+        if (!mat->bulk_modulus || !mat->shear_modulus) return fail(PD_ERR_ARG, "bulk/shear modulus is NULL");
+        b.K.assign(mat->bulk_modulus, mat->bulk_modulus + nt2);
+        b.G.assign(mat->shear_modulus, mat->shear_modulus + nt2);
+        if (!symmetric(b.K, nt) || !symmetric(b.G, nt))
+            return fail(PD_ERR_ARG, "bulk_modulus/shear_modulus must be symmetric");
+    }
+    b.first_env = env->N_env;
+    env->N_env += n;
+    env->hb.push_back(std::move(b));
+    if (out_block) *out_block = (int64_t)env->hb.size() - 1;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_set_family(pd_env *env, int64_t block, int64_t rows,
+                                       const int64_t *family, const uint8_t *intact) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (block < 0 || block >= (int64_t)env->hb.size()) return fail(PD_ERR_ARG, "no block %lld", (long long)block);
+    HostBlock &b = env->hb[block];
+    if (rows < 1 || !family) return fail(PD_ERR_ARG, "family is NULL or rows < 1");
+    size_t tot = (size_t)rows * (size_t)b.n;
+    for (int64_t i = 0; i < b.n; ++i) {
+        int64_t prev = INT64_MAX;
+        bool zero_seen = false;
+        for (int64_t r = 0; r < rows; ++r) {
+            int64_t j = family[(size_t)i * rows + r];
+            if (j < 0 || j > b.n) return fail(PD_ERR_ARG, "family entry out of range");
+            if (j == 0) {
+                zero_seen = true;
+                continue;
+            }
+            if (zero_seen) return fail(PD_ERR_ARG, "family column %lld has an entry after padding", (long long)i);
+            if (j >= prev) return fail(PD_ERR_ARG, "family column %lld is not in descending order", (long long)i);
+            if (j == i + 1) return fail(PD_ERR_ARG, "family column %lld contains the particle itself", (long long)i);
+            prev = j;
+            if (intact && intact[(size_t)i * rows + r] > 1) return fail(PD_ERR_ARG, "intact must be 0/1");
+        }
+    }
+    b.host_family = true;
+    b.rows = rows;
+    b.family.assign(family, family + tot);
+    b.intact.resize(tot);
+    for (size_t e = 0; e < tot; ++e) b.intact[e] = intact ? (uint8_t)(intact[e] && family[e] > 0) : (uint8_t)(family[e] > 0);
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_add_bc(pd_env *env, int32_t kind, const uint8_t *mask,
+                                   const uint8_t *dims, const double *rate, double freq,
+                                   int64_t applyafter, int32_t onlyatstart, int64_t *out_bc) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (kind != PD_BC_FIX && kind != PD_BC_TOFRO) return fail(PD_ERR_ARG, "unknown BC kind %d", kind);
+    if (!mask || !dims) return fail(PD_ERR_ARG, "mask/dims is NULL");
+    if (kind == PD_BC_TOFRO && !rate) return fail(PD_ERR_ARG, "rate is NULL");
+    if (env->hbc.size() >= 64) return fail(PD_ERR_UNSUPPORTED, "at most 64 boundary conditions");
+    HostBC bc;
+    bc.kind = kind;
+    bc.dims = (dims[0] ? 1 : 0) | (dims[1] ? 2 : 0) | (dims[2] ? 4 : 0);
+    for (int d = 0; d < 3; ++d) bc.rate[d] = kind == PD_BC_TOFRO ? rate[d] : 0.0;
+    bc.freq = freq;
+    bc.applyafter = applyafter;
+    bc.onlyatstart = onlyatstart;
+    bc.dir = 1;
+    for (int64_t e = 0; e < env->N_env; ++e)
+        if (mask[e]) bc.env_idx.push_back(e);
+    env->hbc.push_back(std::move(bc));
+    if (out_bc) *out_bc = (int64_t)env->hbc.size() - 1;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block1, int64_t block2,
+                                        double exponent, double stiffness, double equi_dist,
+                                        double distance, int64_t max_neighs, int64_t *out_contact) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (kind != PD_CONTACT_12 && kind != PD_CONTACT_11) return fail(PD_ERR_ARG, "unknown contact kind %d", kind);
+    int64_t nb = (int64_t)env->hb.size();
+    if (block1 < 0 || block1 >= nb) return fail(PD_ERR_ARG, "no block %lld", (long long)block1);
+    if (kind == PD_CONTACT_12 && (block2 < 0 || block2 >= nb || block2 == block1))
+        return fail(PD_ERR_ARG, "contact-12 needs two distinct blocks");
+    if (max_neighs < 1) return fail(PD_ERR_ARG, "max_neighs must be >= 1");
+    if (!(equi_dist > 0.0) || !(distance > 0.0)) return fail(PD_ERR_ARG, "equi_dist/distance must be > 0");
+    HostContact c;
+    c.kind = kind;
+    c.b1 = block1;
+    c.b2 = kind == PD_CONTACT_12 ? block2 : block1;
+    c.exponent = exponent;
+    c.stiffness = stiffness;
+    c.equi_dist = equi_dist;
+    c.distance = distance;
+    c.max_neighs = max_neighs;
+    env->hc.push_back(std::move(c));
+    if (out_contact) *out_contact = (int64_t)env->hc.size() - 1;
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// finalize: layout, upload, families, weighted volume, intact0
+// ---------------------------------------------------------------------
+extern "C" pd_status pd_env_finalize(pd_env *env) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (env->hb.empty()) return fail(PD_ERR_STATE, "environment has no material blocks");
+    CK(cudaSetDevice(env->device));
+    cudaStream_t st = env->st;
+
+    // --- internal layout ---
+    int64_t N = 0;
+    for (auto &b : env->hb) {
+        b.first_int = N;
+        N += round_up(b.n, kSlice);
+    }
+    env->N = N;
+    const int64_t NE = env->N_env;
+    env->map_h.resize(NE);
+    for (auto &b : env->hb)
+        for (int64_t i = 0; i < b.n; ++i) env->map_h[b.first_env + i] = b.first_int + i;
+
+    std::vector<double4> x4(N, make_double4(0, 0, 0, 0)), y4(N, make_double4(0, 0, 0, 0)),
+        v4(N, make_double4(0, 0, 0, 0));
+    std::vector<int32_t> tinfo(N, -1);
+    std::vector<double> mass(N, 0.0), dens(N, 0.0);
+    std::vector<DevBlock> blocks;
+    std::vector<PairParam> pairs;
+    std::vector<double> tdens;
+    env->deformed_h.assign(env->hb.size(), 0);
+    for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+        HostBlock &b = env->hb[bi];
+        DevBlock d{};
+        d.kind = b.kind;
+        d.nt = b.nt;
+        d.pair_base = (int32_t)pairs.size();
+        d.type_base = (int32_t)tdens.size();
+        d.first = b.first_int;
+        d.n = b.n;
+        d.c11 = b.c[0];
+        d.c11f = (float)b.c[0];
+        double cen[3] = {0, 0, 0};
+        for (int64_t i = 0; i < b.n; ++i)
+            for (int k = 0; k < 3; ++k) cen[k] += b.x[3 * i + k];
+        d.center = make_double3(cen[0] / b.n, cen[1] / b.n, cen[2] / b.n);
+        for (int j = 0; j < b.nt; ++j)
+            for (int i = 0; i < b.nt; ++i) {
+                size_t e = (size_t)i + (size_t)j * b.nt;
+                PairParam pp;
+                pp.cs = b.cs[e];
+                pp.k35 = 3 * b.K[e] - 5 * b.G[e];
+                pp.g15 = 15 * b.G[e];
+                pp.pad = 0.0;
+                pairs.push_back(pp);
+            }
+        for (int t = 0; t < b.nt; ++t) tdens.push_back(b.dens[t]);
+        blocks.push_back(d);
+        bool deformed = false;
+        for (int64_t i = 0; i < b.n; ++i) {
+            int64_t p = b.first_int + i;
+            x4[p] = make_double4(b.x[3 * i], b.x[3 * i + 1], b.x[3 * i + 2], b.vol[i]);
+            y4[p] = make_double4(b.y[3 * i], b.y[3 * i + 1], b.y[3 * i + 2], 0.0);
+            v4[p] = make_double4(b.v[3 * i], b.v[3 * i + 1], b.v[3 * i + 2], 0.0);
+            int t = (int)(b.type[i] - b.type_start);
+            tinfo[p] = ((int32_t)bi << 8) | t;
+            // environment.jl:173-180,214: mass = volume * rho[t]; density = mass / volume
+            mass[p] = b.vol[i] * b.dens[t];
+            dens[p] = mass[p] / b.vol[i];
+            for (int k = 0; k < 3; ++k) deformed |= !(b.y[3 * i + k] == b.x[3 * i + k]);
+        }
+        // general_material.jl:92-96: deformed = (y0 != x)
+        env->deformed_h[bi] = deformed ? 1 : 0;
+    }
+    env->blocks_h = blocks;
+
+    PD_TRY(env->x4.alloc(N));
+    PD_TRY(env->y.alloc(N));
+    PD_TRY(env->v.alloc(N));
+    PD_TRY(env->f.alloc(N));
+    PD_TRY(env->p.alloc(N));
+    PD_TRY(env->tinfo.alloc(N));
+    PD_TRY(env->mass.alloc(N));
+    PD_TRY(env->dens.alloc(N));
+    PD_TRY(env->mth.alloc(N));
+    PD_TRY(env->cnt.alloc(N));
+    PD_TRY(env->intact0.alloc(N));
+    PD_TRY(env->map.alloc(NE));
+    PD_TRY(env->blocks_d.alloc(blocks.size()));
+    PD_TRY(env->pairs.alloc(pairs.size()));
+    PD_TRY(env->tdens.alloc(tdens.size()));
+    PD_TRY(env->deformed.alloc(blocks.size()));
+    PD_TRY(env->partials.alloc(3 * 256));
+    PD_TRY(env->out3.alloc(8));
+    PD_TRY(env->flag.alloc(4));
+    PD_TRY(env->stage.alloc(3 * (size_t)std::max<int64_t>(NE, 1)));
+    CK(cudaMemcpyAsync(env->x4.p, x4.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->y.p, y4.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->v.p, v4.data(), N * sizeof(double4), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(env->f.p, 0, N * sizeof(double4), st));
+    CK(cudaMemsetAsync(env->p.p, 0, N * sizeof(double4), st));
+    CK(cudaMemsetAsync(env->mth.p, 0, N * sizeof(double2), st));
+    CK(cudaMemcpyAsync(env->tinfo.p, tinfo.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->mass.p, mass.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->dens.p, dens.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->map.p, env->map_h.data(), NE * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->blocks_d.p, blocks.data(), blocks.size() * sizeof(DevBlock),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->pairs.p, pairs.data(), pairs.size() * sizeof(PairParam), cudaMemcpyHostToDevice,
+                       st));
+    CK(cudaMemcpyAsync(env->tdens.p, tdens.data(), tdens.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       st));
+    {
+        std::vector<int32_t> df(env->deformed_h.begin(), env->deformed_h.end());
+        CK(cudaMemcpyAsync(env->deformed.p, df.data(), df.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           st));
+        CK(cudaStreamSynchronize(st));
+    }
+
+    // --- family sizes: GPU neighbour count per GPU-built block ---
+    std::vector<int32_t> cnt(N, 0);
+    std::vector<Cells> cells(env->hb.size());
+    std::vector<int64_t> cell_base(env->hb.size(), 0);
+    DBuf<int32_t> d_cell_of, d_cell_start, d_cell_list;
+    {
+        int64_t tot_cells = 0, tot_part = 0;
+        for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+            HostBlock &b = env->hb[bi];
+            if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+            cells[bi] = bin_block(b, b.first_int);
+            cell_base[bi] = tot_cells;
+            tot_cells += (int64_t)cells[bi].dims.x * cells[bi].dims.y * cells[bi].dims.z;
+            tot_part += b.n;
+        }
+        if (tot_part > 0) {
+            std::vector<int32_t> cell_of_all, start_all, list_all;
+            std::vector<int64_t> part_off(env->hb.size(), 0);
+            start_all.reserve(tot_cells + 1);
+            for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+                HostBlock &b = env->hb[bi];
+                if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+                part_off[bi] = (int64_t)cell_of_all.size();
+                int32_t list_off = (int32_t)list_all.size();
+                for (int32_t c : cells[bi].cell_of) cell_of_all.push_back(c + (int32_t)cell_base[bi]);
+                int64_t nc = (int64_t)cells[bi].start.size() - 1;
+                for (int64_t k = 0; k < nc; ++k) start_all.push_back(cells[bi].start[k] + list_off);
+                for (int32_t v : cells[bi].list) list_all.push_back(v);
+            }
+            start_all.push_back((int32_t)list_all.size());
+            PD_TRY(d_cell_of.alloc(cell_of_all.size()));
+            PD_TRY(d_cell_start.alloc(start_all.size()));
+            PD_TRY(d_cell_list.alloc(list_all.size()));
+            CK(cudaMemcpyAsync(d_cell_of.p, cell_of_all.data(), cell_of_all.size() * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_cell_start.p, start_all.data(), start_all.size() * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_cell_list.p, list_all.data(), list_all.size() * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(env->cnt.p, 0, N * sizeof(int32_t), st));
+            for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+                HostBlock &b = env->hb[bi];
+                if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+                launch_count_neighbors(st, b.n, b.first_int, env->x4.p, d_cell_of.p + part_off[bi],
+                                       d_cell_start.p, d_cell_list.p, cell_base[bi], cells[bi].dims,
+                                       b.horizon, env->cnt.p);
+                cells[bi].cell_of.clear();
+                cells[bi].cell_of.shrink_to_fit();
+                cells[bi].list.clear();
+                cells[bi].start.clear();
+                cells[bi].dims = cells[bi].dims;
+                b.cell_part_off = part_off[bi];
+            }
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(cnt.data(), env->cnt.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+    }
+    // host-provided families
+    for (auto &b : env->hb) {
+        if (!b.host_family) continue;
+        for (int64_t i = 0; i < b.n; ++i) {
+            int32_t c = 0;
+            for (int64_t r = 0; r < b.rows; ++r) c += b.family[(size_t)i * b.rows + r] > 0;
+            cnt[b.first_int + i] = c;
+        }
+    }
+    // overflow check and reference row counts (general_material.jl:88)
+    for (auto &b : env->hb) {
+        int64_t maxc = 0;
+        for (int64_t i = 0; i < b.n; ++i) maxc = std::max<int64_t>(maxc, cnt[b.first_int + i]);
+        if (b.kind == PD_MAT_SKIP && !b.host_family) {
+            b.rows = 1;
+            continue;
+        }
+        if (!b.host_family) {
+            int64_t mn = std::min<int64_t>(b.max_neigh, b.n);
+            if (maxc >= mn)
+                return fail(PD_ERR_FAMILY_OVERFLOW,
+                            "a family has %lld members but max_neigh allows at most %lld (reference: BoundsError)",
+                            (long long)maxc, (long long)(mn - 1));
+            b.rows = maxc + 1;
+        }
+    }
+    // SELL-32 slice table
+    const int64_t S = N / kSlice;
+    std::vector<int64_t> slice_ptr(S + 1, 0);
+    for (int64_t s = 0; s < S; ++s) {
+        int32_t m = 0;
+        for (int l = 0; l < kSlice; ++l) m = std::max(m, cnt[s * kSlice + l]);
+        slice_ptr[s + 1] = slice_ptr[s] + (int64_t)kSlice * round_up(m, 32);
+    }
+    env->nnz = slice_ptr[S];
+    env->slice_ptr_h = slice_ptr;
+    env->cnt_h = cnt;
+    PD_TRY(env->slice_ptr.alloc(S + 1));
+    PD_TRY(env->nbr.alloc(std::max<int64_t>(env->nnz, 32)));
+    PD_TRY(env->words[0].alloc(std::max<int64_t>(env->nnz / 32, 1)));
+    PD_TRY(env->words[1].alloc(std::max<int64_t>(env->nnz / 32, 1)));
+    PD_TRY(env->words0.alloc(std::max<int64_t>(env->nnz / 32, 1)));
+    CK(cudaMemcpyAsync(env->slice_ptr.p, slice_ptr.data(), (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(env->nbr.p, 0, std::max<int64_t>(env->nnz, 32) * sizeof(int32_t), st));
+    CK(cudaMemsetAsync(env->words[0].p, 0, std::max<int64_t>(env->nnz / 32, 1) * 4, st));
+    CK(cudaMemsetAsync(env->words[1].p, 0, std::max<int64_t>(env->nnz / 32, 1) * 4, st));
+    // GPU-built families: fill + sort; initial intact = all bonds
+    for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+        HostBlock &b = env->hb[bi];
+        if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+        launch_fill_neighbors(st, b.n, b.first_int, env->x4.p, d_cell_of.p + b.cell_part_off, d_cell_start.p,
+                              d_cell_list.p, cell_base[bi], cells[bi].dims, b.horizon, env->slice_ptr.p,
+                              env->nbr.p);
+    }
+    launch_sort_neighbors(st, N, env->slice_ptr.p, env->cnt.p, env->nbr.p);
+    launch_init_intact(st, N, env->slice_ptr.p, env->cnt.p, env->words[0].p);
+    CK(cudaGetLastError());
+    // host-provided families (already descending): write entries and bits
+    bool any_host = false;
+    for (auto &b : env->hb) any_host |= b.host_family;
+    if (any_host) {
+        std::vector<int32_t> nbr_h(env->nnz, 0);
+        std::vector<uint32_t> w_h(env->nnz / 32, 0);
+        CK(cudaMemcpyAsync(nbr_h.data(), env->nbr.p, env->nnz * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(w_h.data(), env->words[0].p, (env->nnz / 32) * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (auto &b : env->hb) {
+            if (!b.host_family) continue;
+            for (int64_t i = 0; i < b.n; ++i) {
+                int64_t p = b.first_int + i;
+                int64_t base = slice_ptr[p / 32] + (p % 32), wb = slice_ptr[p / 32] / 32 + (p % 32);
+                int64_t k = 0;
+                for (int64_t r = 0; r < b.rows; ++r) {
+                    int64_t j = b.family[(size_t)i * b.rows + r];
+                    if (j <= 0) continue;
+                    nbr_h[base + 32 * k] = (int32_t)(b.first_int + j - 1);
+                    uint32_t bit = 1u << (k % 32);
+                    uint32_t &w = w_h[wb + 32 * (k / 32)];
+                    if (b.intact[(size_t)i * b.rows + r]) w |= bit;
+                    else w &= ~bit;
+                    ++k;
+                }
+            }
+        }
+        // symmetry of the bond set (the serial-order gather relies on it)
+        if (env->precision == PD_PREC_FP64_SERIAL) {
+            for (auto &b : env->hb) {
+                if (!b.host_family) continue;
+                for (int64_t i = 0; i < b.n; ++i) {
+                    int64_t p = b.first_int + i;
+                    int64_t base = slice_ptr[p / 32] + (p % 32), wb = slice_ptr[p / 32] / 32 + (p % 32);
+                    for (int64_t k = 0; k < cnt[p]; ++k) {
+                        int64_t q = nbr_h[base + 32 * k];
+                        bool bit = (w_h[wb + 32 * (k / 32)] >> (k % 32)) & 1u;
+                        int64_t qb = slice_ptr[q / 32] + (q % 32), qwb = slice_ptr[q / 32] / 32 + (q % 32);
+                        bool found = false;
+                        for (int64_t kk = 0; kk < cnt[q]; ++kk)
+                            if (nbr_h[qb + 32 * kk] == p) {
+                                found = ((w_h[qwb + 32 * (kk / 32)] >> (kk % 32)) & 1u) == bit;
+                                break;
+                            }
+                        if (!found)
+                            return fail(PD_ERR_ARG,
+                                        "family/intact are not symmetric (bond %lld-%lld); the serial-order "
+                                        "mode requires symmetric bonds",
+                                        (long long)i + 1, (long long)(q - b.first_int + 1));
+                    }
+                }
+            }
+        }
+        CK(cudaMemcpyAsync(env->nbr.p, nbr_h.data(), env->nnz * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(env->words[0].p, w_h.data(), (env->nnz / 32) * 4, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    env->cur = 0;
+    CK(cudaMemcpyAsync(env->words0.p, env->words[0].p, std::max<int64_t>(env->nnz / 32, 1) * 4,
+                       cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(env->words[1].p, env->words[0].p, std::max<int64_t>(env->nnz / 32, 1) * 4,
+                       cudaMemcpyDeviceToDevice, st));
+    // weighted volume (peri.jl:342-354) and intact0 (environment.jl:169)
+    launch_weighted_volume(st, env->geo(), env->mth.p);
+    launch_popcount(st, N, env->slice_ptr.p, env->cnt.p, env->words[0].p, env->intact0.p);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+
+    // --- boundary conditions ---
+    for (auto &hb : env->hbc) {
+        DevBC d;
+        std::vector<int32_t> idx(hb.env_idx.size());
+        for (size_t j = 0; j < idx.size(); ++j) idx[j] = (int32_t)env->map_h[hb.env_idx[j]];
+        PD_TRY(d.idx.alloc(std::max<size_t>(idx.size(), 1)));
+        PD_TRY(d.last.alloc(std::max<size_t>(idx.size(), 1)));
+        if (!idx.empty()) {
+            CK(cudaMemcpyAsync(d.idx.p, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(d.last.p, 0, idx.size() * sizeof(double4), st));
+        }
+        d.n = (int64_t)idx.size();
+        env->bcs.push_back(std::move(d));
+    }
+    PD_TRY(pd::contacts_finalize(env));
+    CK(cudaStreamSynchronize(st));
+    env->finalized = true;
+    // release host copies of the big per-particle inputs
+    for (auto &b : env->hb) {
+        b.y.clear();
+        b.y.shrink_to_fit();
+        b.v.clear();
+        b.v.shrink_to_fit();
+        b.family.clear();
+        b.family.shrink_to_fit();
+        b.intact.clear();
+        b.intact.shrink_to_fit();
+    }
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// sizes / families
+// ---------------------------------------------------------------------
+extern "C" pd_status pd_env_num_particles(const pd_env *env, int64_t *n) {
+    PD_TRY(check_env(env));
+    if (!n) return fail(PD_ERR_ARG, "n is NULL");
+    *n = env->N_env;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_num_bonds(pd_env *env, int64_t *intact_bonds) {
+    PD_TRY(need_final(env));
+    if (!intact_bonds) return fail(PD_ERR_ARG, "intact_bonds is NULL");
+    CK(cudaSetDevice(env->device));
+    DBuf<int32_t> tmp;
+    PD_TRY(tmp.alloc(env->N));
+    launch_popcount(env->st, env->N, env->slice_ptr.p, env->cnt.p, env->words[env->cur].p, tmp.p);
+    std::vector<int32_t> h(env->N);
+    CK(cudaMemcpyAsync(h.data(), tmp.p, env->N * 4, cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    int64_t s = 0;
+    for (int32_t c : h) s += c;
+    *intact_bonds = s;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_family_rows(const pd_env *env, int64_t block, int64_t *rows) {
+    PD_TRY(need_final(env));
+    if (block < 0 || block >= (int64_t)env->hb.size() || !rows) return fail(PD_ERR_ARG, "bad block or NULL rows");
+    *rows = env->hb[block].rows;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_family(pd_env *env, int64_t block, int64_t *family, uint8_t *intact) {
+    PD_TRY(need_final(env));
+    if (block < 0 || block >= (int64_t)env->hb.size()) return fail(PD_ERR_ARG, "no block %lld", (long long)block);
+    CK(cudaSetDevice(env->device));
+    const HostBlock &b = env->hb[block];
+    int64_t s0 = b.first_int / 32, s1 = (b.first_int + round_up(b.n, 32)) / 32;
+    int64_t e0 = env->slice_ptr_h[s0], e1 = env->slice_ptr_h[s1];
+    std::vector<int32_t> nb(e1 - e0);
+    std::vector<uint32_t> w((e1 - e0) / 32);
+    if (e1 > e0) {
+        CK(cudaMemcpyAsync(nb.data(), env->nbr.p + e0, (e1 - e0) * 4, cudaMemcpyDeviceToHost, env->st));
+        CK(cudaMemcpyAsync(w.data(), env->words[env->cur].p + e0 / 32, (e1 - e0) / 32 * 4, cudaMemcpyDeviceToHost,
+                           env->st));
+        CK(cudaStreamSynchronize(env->st));
+    }
+    const int64_t R = b.rows;
+    if (family) std::fill(family, family + (size_t)R * b.n, 0);
+    if (intact) std::fill(intact, intact + (size_t)R * b.n, 0);
+    for (int64_t i = 0; i < b.n; ++i) {
+        int64_t p = b.first_int + i;
+        int64_t base = env->slice_ptr_h[p / 32] - e0 + (p % 32), wb = (env->slice_ptr_h[p / 32] - e0) / 32 + (p % 32);
+        for (int64_t k = 0; k < env->cnt_h[p] && k < R; ++k) {
+            if (family) family[(size_t)i * R + k] = nb[base + 32 * k] - b.first_int + 1;
+            if (intact) intact[(size_t)i * R + k] = (w[wb + 32 * (k / 32)] >> (k % 32)) & 1u;
+        }
+    }
+    return PD_OK;
+}
+
+static pd_status get_block_scalar(pd_env *env, int64_t block, double *out, int comp) {
+    PD_TRY(need_final(env));
+    if (block < 0 || block >= (int64_t)env->hb.size() || !out) return fail(PD_ERR_ARG, "bad block or NULL output");
+    CK(cudaSetDevice(env->device));
+    const HostBlock &b = env->hb[block];
+    std::vector<double2> h(b.n);
+    CK(cudaMemcpyAsync(h.data(), env->mth.p + b.first_int, b.n * sizeof(double2), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    for (int64_t i = 0; i < b.n; ++i) out[i] = comp == 0 ? h[i].x : h[i].y;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_weighted_volume(pd_env *env, int64_t block, double *m) {
+    return get_block_scalar(env, block, m, 0);
+}
+
+extern "C" pd_status pd_env_get_theta(pd_env *env, int64_t block, double *theta) {
+    return get_block_scalar(env, block, theta, 1);
+}
+
+// ---------------------------------------------------------------------
+// state
+// ---------------------------------------------------------------------
+static pd_status download3(pd_env *env, const double4 *src, double *dst) {
+    if (!dst) return PD_OK;
+    launch_pack3(env->st, env->N_env, src, env->map.p, env->stage.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst, env->stage.p, 3 * env->N_env * sizeof(double), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
+}
+
+static pd_status upload3(pd_env *env, const double *src, double4 *dst) {
+    if (!src) return PD_OK;
+    CK(cudaMemcpyAsync(env->stage.p, src, 3 * env->N_env * sizeof(double), cudaMemcpyHostToDevice, env->st));
+    launch_unpack3(env->st, env->N_env, env->stage.p, env->map.p, dst);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_state(pd_env *env, double *y, double *v, double *f, double *p) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(download3(env, env->y.p, y));
+    PD_TRY(download3(env, env->v.p, v));
+    PD_TRY(download3(env, env->f.p, f));
+    PD_TRY(download3(env, env->p.p, p));
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_set_state(pd_env *env, const double *y, const double *v, const double *f) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(upload3(env, y, env->y.p));
+    PD_TRY(upload3(env, v, env->v.p));
+    PD_TRY(upload3(env, f, env->f.p));
+    env->fast_valid = false;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_mass(pd_env *env, double *mass, double *volume, double *density) {
+    PD_TRY(need_final(env));
+    for (const auto &b : env->hb)
+        for (int64_t i = 0; i < b.n; ++i) {
+            double m = b.vol[i] * b.dens[b.type[i] - b.type_start];
+            if (mass) mass[b.first_env + i] = m;
+            if (volume) volume[b.first_env + i] = b.vol[i];
+            if (density) density[b.first_env + i] = m / b.vol[i];
+        }
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_time_step(const pd_env *env, int64_t *ts) {
+    PD_TRY(check_env(env));
+    if (!ts) return fail(PD_ERR_ARG, "time_step is NULL");
+    *ts = env->ts;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_set_time_step(pd_env *env, int64_t ts) {
+    PD_TRY(check_env(env));
+    env->ts = ts;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_reset_bonds(pd_env *env) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    size_t nw = std::max<int64_t>(env->nnz / 32, 1) * 4;
+    CK(cudaMemcpyAsync(env->words[0].p, env->words0.p, nw, cudaMemcpyDeviceToDevice, env->st));
+    CK(cudaMemcpyAsync(env->words[1].p, env->words0.p, nw, cudaMemcpyDeviceToDevice, env->st));
+    env->cur = 0;
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// diagnostics
+// ---------------------------------------------------------------------
+static pd_status damage_internal(pd_env *env, std::vector<double> &dint) {
+    DBuf<double> d;
+    PD_TRY(d.alloc(env->N));
+    launch_damage(env->st, env->N, env->slice_ptr.p, env->cnt.p, env->words[env->cur].p, env->intact0.p,
+                  env->tinfo.p, d.p);
+    CK(cudaGetLastError());
+    dint.resize(env->N);
+    CK(cudaMemcpyAsync(dint.data(), d.p, env->N * sizeof(double), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_damage(pd_env *env, double *damage) {
+    PD_TRY(need_final(env));
+    if (!damage) return fail(PD_ERR_ARG, "damage is NULL");
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env));
+    std::vector<double> dint;
+    PD_TRY(damage_internal(env, dint));
+    for (int64_t e = 0; e < env->N_env; ++e) damage[e] = dint[env->map_h[e]];
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_diagnostics(pd_env *env, double *out8) {
+    PD_TRY(need_final(env));
+    if (!out8) return fail(PD_ERR_ARG, "out is NULL");
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env));
+    double h[3];
+    launch_sum4(env->st, env->N, env->p.p, env->partials.p, env->out3.p);
+    CK(cudaMemcpyAsync(h, env->out3.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    out8[0] = h[0];
+    out8[1] = h[1];
+    out8[2] = h[2];
+    launch_sum4(env->st, env->N, env->f.p, env->partials.p, env->out3.p);
+    CK(cudaMemcpyAsync(h, env->out3.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    out8[3] = h[0];
+    out8[4] = h[1];
+    out8[5] = h[2];
+    std::vector<double> dint;
+    PD_TRY(damage_internal(env, dint));
+    double s = 0.0;
+    for (int64_t e = 0; e < env->N_env; ++e) s += dint[env->map_h[e]];
+    out8[6] = env->N_env > 0 ? s / (double)env->N_env : 0.0;
+    int64_t nb = 0;
+    PD_TRY(pd_env_num_bonds(env, &nb));
+    out8[7] = (double)nb;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_deformed(pd_env *env, uint8_t *flags) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    std::vector<int32_t> h(env->hb.size());
+    CK(cudaMemcpyAsync(h.data(), env->deformed.p, h.size() * 4, cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    bool all = true;
+    for (size_t b = 0; b < h.size(); ++b) {
+        env->deformed_h[b] = h[b];
+        if (flags) flags[b] = (uint8_t)(h[b] != 0);
+        if (env->hb[b].kind != PD_MAT_SKIP) all &= h[b] != 0;
+    }
+    (void)all;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_check_finite(pd_env *env) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env));
+    CK(cudaMemsetAsync(env->flag.p, 0, 4, env->st));
+    launch_nonfinite(env->st, env->N, env->y.p, env->flag.p);
+    launch_nonfinite(env->st, env->N, env->v.p, env->flag.p);
+    launch_nonfinite(env->st, env->N, env->f.p, env->flag.p);
+    int32_t h = 0;
+    CK(cudaMemcpyAsync(&h, env->flag.p, 4, cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    if (h) return fail(PD_ERR_NAN, "NaN or Inf in y, v or f");
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------
+extern "C" pd_status pd_env_stream(pd_env *env, void **stream) {
+    PD_TRY(check_env(env));
+    if (!stream) return fail(PD_ERR_ARG, "stream is NULL");
+    *stream = (void *)env->st;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_kernel_launches(int64_t *count) {
+    if (!count) return fail(PD_ERR_ARG, "count is NULL");
+    *count = g_launches.load(std::memory_order_relaxed);
+    return PD_OK;
+}
+
+static pd_status prof_collect(pd_env *env) {
+    if (env->prof_used == 0) return PD_OK;
+    CK(cudaStreamSynchronize(env->st));
+    for (size_t k = 0; k + 1 < env->prof_used; k += 2) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, env->prof_ev[k], env->prof_ev[k + 1]));
+        env->prof_ms += ms;
+        env->prof_launches += 1;
+    }
+    env->prof_used = 0;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_profile(pd_env *env, int32_t enable) {
+    PD_TRY(check_env(env));
+    CK(cudaSetDevice(env->device));
+    PD_TRY(prof_collect(env));
+    env->prof = enable != 0;
+    env->prof_ms = 0.0;
+    env->prof_launches = 0;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t *launches) {
+    PD_TRY(check_env(env));
+    CK(cudaSetDevice(env->device));
+    PD_TRY(prof_collect(env));
+    if (total_ms) *total_ms = env->prof_ms;
+    if (launches) *launches = env->prof_launches;
+    return PD_OK;
+}

@@ -1,0 +1,194 @@
+// pd_env_impl.h -- host-side environment object and helpers shared by the
+// host translation units (pd_env.cu, pd_solver.cu, pd_contact.cu,
+// pd_fast.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pd_internal.h"
+
+namespace pd {
+pd_status fail(pd_status s, const char *fmt, ...);
+pd_status cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+}  // namespace pd
+
+#define PD_TRY(expr)                       \
+    do {                                   \
+        pd_status s_ = (expr);             \
+        if (s_ != PD_OK) return s_;        \
+    } while (0)
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) return pd::cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+namespace pd {
+
+// Owning device buffer.
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DBuf &operator=(DBuf &&o) noexcept {
+        reset();
+        p = o.p;
+        n = o.n;
+        o.p = nullptr;
+        o.n = 0;
+        return *this;
+    }
+    ~DBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    pd_status alloc(size_t count) {
+        reset();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return fail(PD_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+                        cudaGetErrorString(e));
+        }
+        n = count;
+        return PD_OK;
+    }
+};
+
+struct HostBlock {
+    int64_t n = 0;
+    int32_t kind = 0, nt = 1;
+    int64_t type_start = 1;
+    double horizon = 0, particle_size = 0;
+    int64_t max_neigh = 100;
+    std::vector<double> x, y, v, vol;
+    std::vector<int64_t> type;
+    std::vector<double> c, K, G, cs, dens;
+    bool host_family = false;
+    int64_t rows = 0;  // reference family rows M'
+    std::vector<int64_t> family;
+    std::vector<uint8_t> intact;
+    int64_t first_env = 0, first_int = 0;
+    int64_t cell_part_off = 0;
+};
+
+struct HostBC {
+    int32_t kind = 0, dims = 7, onlyatstart = 0;
+    double rate[3] = {0, 0, 0};
+    double freq = 0;
+    int64_t applyafter = 0;
+    int dir = 1;
+    std::vector<int64_t> env_idx;
+};
+
+struct DevBC {
+    DBuf<int32_t> idx;
+    DBuf<double4> last;
+    int64_t n = 0;
+};
+
+struct HostContact {
+    int32_t kind = 0;
+    int64_t b1 = 0, b2 = 0;
+    double exponent = 1, stiffness = 0, equi_dist = 0, distance = 0;
+    int64_t max_neighs = 50;
+    int64_t rows = 0;  // neighbour rows of the reference layout
+};
+
+// Device state of one contact model.
+struct DevContact {
+    int64_t n1 = 0, n2 = 0;       // particles of pair[1] / pair[2] (block sizes)
+    int64_t first1 = 0, first2 = 0;  // internal first index of the two blocks
+    int64_t rows = 0;
+    DBuf<int32_t> nb;       // n1 x rows, internal indices of set-2 particles, -1 pad
+    DBuf<int32_t> rev_off;  // n2+1 reverse-list offsets
+    DBuf<int32_t> rev;      // reverse lists (internal indices of set-1 particles, ascending)
+    DBuf<int32_t> rev_cnt;  // n2 scratch
+    int64_t rev_cap = 0;
+    bool has_neighs = false;
+};
+
+}  // namespace pd
+
+struct pd_env {
+    int device = 0, precision = 0;
+    double dt = 0;
+    int64_t ts = 0;
+    cudaStream_t st = nullptr;
+    bool finalized = false;
+
+    std::vector<pd::HostBlock> hb;
+    std::vector<pd::HostBC> hbc;
+    std::vector<pd::HostContact> hc;
+    int64_t N_env = 0;  // particles in environment order
+    int64_t N = 0;      // internal (padded) particles
+    std::vector<int64_t> map_h;
+    std::vector<pd::DevBlock> blocks_h;
+    std::vector<int> deformed_h;
+    std::vector<int64_t> slice_ptr_h;
+    std::vector<int32_t> cnt_h;
+    int64_t nnz = 0;
+
+    pd::DBuf<int64_t> map;
+    pd::DBuf<double4> x4, y, v, f, p;
+    pd::DBuf<double> mass, dens, tdens;
+    pd::DBuf<int32_t> tinfo, cnt, intact0, deformed;
+    pd::DBuf<int64_t> slice_ptr;
+    pd::DBuf<int32_t> nbr;
+    pd::DBuf<uint32_t> words[2], words0;
+    int cur = 0;
+    pd::DBuf<double2> mth;
+    pd::DBuf<pd::DevBlock> blocks_d;
+    pd::DBuf<pd::PairParam> pairs;
+    pd::DBuf<double> partials, out3, stage;
+    pd::DBuf<int32_t> flag;
+    std::vector<pd::DevBC> bcs;
+    std::vector<pd::DevContact> contacts;
+
+    // scratch for the device-pointer entry point and solvers
+    pd::DBuf<double4> tmp_y, tmp_f, opt;
+    pd::DBuf<int32_t> free_mask;
+    pd::DBuf<double> red;
+
+    // optional CUDA-event timing of the bond-force kernel launches
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+    size_t prof_used = 0;
+    double prof_ms = 0.0;
+    int64_t prof_launches = 0;
+
+    // fast (FP64 / FP32C) state; see pd_fast.cu
+    bool fast_valid = false;
+    void *fast = nullptr;
+
+    pd::Geo geo() const;
+    void release_device();
+};
+
+namespace pd {
+// Bracket one launch of the bond-force kernel with timing events (no-op
+// unless profiling is enabled on the environment).
+void prof_begin(pd_env *env, cudaStream_t st);
+void prof_end(pd_env *env, cudaStream_t st);
+pd_status contacts_finalize(pd_env *env);
+pd_status contacts_update_neighs(pd_env *env, int64_t max_part);
+pd_status contacts_force(pd_env *env);
+pd_status sync_state_to_fp64(pd_env *env);
+void fast_release(pd_env *env);
+pd_status fast_vv_steps(pd_env *env, int64_t nsteps);
+pd_status update_acc_serial(pd_env *env);
+}  // namespace pd

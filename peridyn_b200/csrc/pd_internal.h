@@ -1,0 +1,140 @@
+// pd_internal.h -- device data layout and launcher declarations shared by
+// the translation units of libperidyn_b200.so.
+//
+// Layout in HBM (one environment):
+//  * Particles are stored in "internal" order: the environment order with
+//    each material block padded to a multiple of 32 particles, so that a
+//    32-particle slice never straddles two blocks.  Padding particles have
+//    tinfo == -1 and no bonds.
+//  * Per particle (array of structures, 32-byte aligned):
+//      x4[i]  = (x0, x1, x2, volume)        reference configuration
+//      y[i]   = (y0, y1, y2, -)             deformed position (FP64)
+//      v[i], f[i], p[i]                     velocity, acceleration, momentum
+//      mth[i] = (m, theta)                  weighted volume, dilatation
+//      tinfo[i] = block << 8 | local type   (-1 for padding)
+//  * Families in SELL-32 form: slice s holds particles 32s..32s+31; the
+//    k-th bond of lane l lives at nbr[slice_ptr[s] + 32k + l] (coalesced
+//    across a warp).  Bonds of a particle are in descending index order,
+//    the reference's family column order (general_material.jl:88-90).
+//    slice lengths are multiples of 32, so slice_ptr[s] is a multiple of
+//    1024 and the intact bit of bond k sits in word
+//    slice_ptr[s]/32 + 32*(k/32) + l, bit k%32.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/peridyn_b200.h"
+
+namespace pd {
+
+constexpr int kSlice = 32;
+
+// Counts every kernel launch the library issues (pd_kernel_launches).
+void note_launch();
+
+struct DevBlock {
+    int32_t kind;       // PD_MAT_*
+    int32_t nt;         // types in the block
+    int32_t pair_base;  // first PairParam of the block (nt*nt, column-major)
+    int32_t type_base;  // first per-type density of the block
+    int64_t first;      // first internal particle index (multiple of 32)
+    int64_t n;          // particles (without padding)
+    double c11;         // PMB bond stiffness bond_stiffness[1,1]
+    float c11f;         // FP32 copy
+    float pad0;
+    double3 center;     // FP32C coordinate origin of the block
+};
+
+struct PairParam {
+    double cs;    // critical stretch
+    double k35;   // 3K - 5G   (LPS)
+    double g15;   // 15G       (LPS)
+    double pad;
+};
+
+// Everything a bond kernel reads (passed by value).
+struct Geo {
+    int64_t N;                 // internal particle count (multiple of 32)
+    const double4 *x4;         // (x, vol)
+    const int32_t *tinfo;
+    const DevBlock *blocks;
+    const PairParam *pairs;
+    const double *tdens;       // per block-type density
+    const int64_t *slice_ptr;  // N/32 entries
+    const int32_t *cnt;        // bonds per particle
+    const int32_t *nbr;        // SELL neighbour indices (internal)
+    const int32_t *deformed;   // per block
+};
+
+struct BCDev {
+    int32_t kind;
+    int32_t dims;      // bit d set: dimension d constrained
+    double rate[3];
+    int64_t n;
+    const int32_t *idx;  // internal indices, ascending
+    double4 *last;       // BC.last per constrained particle
+};
+
+// ---------------------------------------------------------------------
+// Launchers (pd_exact.cu, compiled with -fmad=false)
+// ---------------------------------------------------------------------
+// Family build.
+void launch_cell_ids(cudaStream_t st, int64_t n, const double4 *x4, int64_t first,
+                     double3 origin, double inv_cell, int3 dims, int64_t cell_base,
+                     int32_t *cell_of);
+void launch_cell_scatter(cudaStream_t st, int64_t n, int64_t first, const int32_t *cell_of,
+                         int32_t *cursor, int32_t *cell_list);
+void launch_count_neighbors(cudaStream_t st, int64_t n, int64_t first, const double4 *x4,
+                            const int32_t *cell_of, const int32_t *cell_start,
+                            const int32_t *cell_list, int64_t cell_base, int3 dims,
+                            double horizon, int32_t *cnt);
+void launch_fill_neighbors(cudaStream_t st, int64_t n, int64_t first, const double4 *x4,
+                           const int32_t *cell_of, const int32_t *cell_start,
+                           const int32_t *cell_list, int64_t cell_base, int3 dims,
+                           double horizon, const int64_t *slice_ptr, int32_t *nbr);
+void launch_sort_neighbors(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
+                           const int32_t *cnt, int32_t *nbr);
+void launch_init_intact(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
+                        const int32_t *cnt, uint32_t *words);
+void launch_popcount(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                     const uint32_t *words, int32_t *out);
+void launch_weighted_volume(cudaStream_t st, const Geo &g, double2 *mth);
+
+// Serial-order FP64 force path.
+void launch_theta_serial(cudaStream_t st, const Geo &g, const double4 *y, const uint32_t *win,
+                         double2 *mth, int64_t p0, int64_t p1);
+void launch_force_serial(cudaStream_t st, const Geo &g, const double4 *y, const double2 *mth,
+                         const uint32_t *win, uint32_t *wout, double4 *f, int accumulate,
+                         int64_t p0, int64_t p1);
+
+// Elementwise velocity-Verlet pieces (exact FP64 arithmetic).
+void launch_kick_drift(cudaStream_t st, int64_t N, double c, double dt, const double4 *f,
+                       double4 *v, double4 *y);
+void launch_kick(cudaStream_t st, int64_t N, double c, const double4 *f, double4 *v);
+void launch_bc_pos(cudaStream_t st, const BCDev &bc, double dt, int dir, double4 *y);
+void launch_bc_vel(cudaStream_t st, const BCDev &bc, int dir, double4 *v);
+void launch_bc_snapshot(cudaStream_t st, const BCDev &bc, const double4 *y);
+void launch_momentum(cudaStream_t st, int64_t N, const double *mass, const double4 *v,
+                     double4 *p);
+void launch_zero4(cudaStream_t st, int64_t N, double4 *a);
+
+// Deformed gate (general_material.jl:243-255).
+void launch_gate(cudaStream_t st, int64_t first, int64_t n, const double4 *x4,
+                 const double4 *y, double *partials, int32_t *deformed_flag);
+
+// Damage / diagnostics.
+void launch_damage(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                   const uint32_t *words, const int32_t *intact0, const int32_t *tinfo,
+                   double *damage);
+void launch_sum4(cudaStream_t st, int64_t N, const double4 *a, double *partials, double *out3);
+
+// Layout conversion between the reference's 3xN column-major arrays and
+// internal double4 arrays.  map[e] = internal index of environment index e.
+void launch_unpack3(cudaStream_t st, int64_t n, const double *src3, const int64_t *map,
+                    double4 *dst);
+void launch_pack3(cudaStream_t st, int64_t n, const double4 *src, const int64_t *map,
+                  double *dst3);
+void launch_nonfinite(cudaStream_t st, int64_t N, const double4 *a, int32_t *flag);
+
+}  // namespace pd

@@ -1,0 +1,217 @@
+"""Pins the CPU oracle (oracle/) with analytical known answers derived from
+the reference's formulas, and checks the GPU algorithm's summation order
+on the CPU.  The reference ships no tests or fixtures of its own."""
+import math
+
+import numpy as np
+import pytest
+
+from peridyn_b200 import (BondBasedSpecific, GeneralMaterial, OrdinaryStateBasedSpecific, PeridynamicsMaterial,
+                          configs, julia_pow_int, lattice, make_matrix)
+from tests import gather_order
+
+
+def lattice_block(n, spacing, horizon_factor, kind="pmb", stretch=1.0, jitter=0.0, cs=0.5, centered=True, seed=1,
+                  K=1.0e9, G=0.6e9, rho=1000.0):
+    x, vol = lattice.cuboid(n, n, n, spacing, jitter=jitter, seed=seed, centered=centered)
+    y = np.asfortranarray(stretch * x)
+    v = np.zeros_like(x, order="F")
+    gen = GeneralMaterial(y, v, x, vol, np.ones(x.shape[1], dtype=np.int64), horizon_factor * spacing,
+                          max_neigh=200)
+    spc = BondBasedSpecific([K], [cs], [rho]) if kind == "pmb" else OrdinaryStateBasedSpecific([K], [G], [cs], [rho])
+    return PeridynamicsMaterial(gen, spc)
+
+
+def integer_vectors_below(r2):
+    r = int(math.ceil(math.sqrt(r2)))
+    cnt = 0
+    for i in range(-r, r + 1):
+        for j in range(-r, r + 1):
+            for k in range(-r, r + 1):
+                if 0 < i * i + j * j + k * k < r2:
+                    cnt += 1
+    return cnt
+
+
+def test_fld_matches_julia_semantics(oracle):
+    L = oracle.lib()
+    # Julia: fld(1.0, 0.1) == 9.0 (exact remainder semantics), fld(7.0, 2.0) == 3.0
+    assert L.or_fld(1.0, 0.1) == 9.0
+    assert L.or_fld(7.0, 2.0) == 3.0
+    assert L.or_fld(-1.0, 3.0) == -1.0
+    assert L.or_fld(6.0, 3.0) == 2.0
+    assert L.or_fld(0.0, 3.0) == 0.0
+
+
+def test_pow_restatements_agree(oracle):
+    rng = np.random.default_rng(0)
+    L = oracle.lib()
+    for x in rng.uniform(0.0, 3.0, 200):
+        for n in (1, 2, 3, 4, 5, 7):
+            assert julia_pow_int(float(x), n) == L.or_pow(float(x), float(n))
+    assert julia_pow_int(0.3, 2) == 0.3 * 0.3
+
+
+def test_make_matrix():
+    m = make_matrix([1.0, 2.0, 3.0])
+    assert m.shape == (2, 2) and m[0, 0] == 1 and m[0, 1] == 2 and m[1, 0] == 2 and m[1, 1] == 3
+    assert make_matrix([5.0]).shape == (1, 1)
+
+
+@pytest.mark.parametrize("hf,expected", [(3.015, 122), (3.0, 92)])
+def test_lattice_neighbour_counts(oracle, hf, expected):
+    # integer lattice (spacing 1): d^2 is exact, the strict d^2 < h^2 of
+    # peri.jl:545 excludes |v|^2 = 9 for h = 3
+    assert integer_vectors_below(hf * hf) == expected
+    x, _ = lattice.cuboid(9, 9, 9, 1.0, centered=False)
+    fam, intact = oracle.cal_family(x, hf, 200)
+    counts = intact.sum(axis=0)
+    centre = 4 + 9 * (4 + 9 * 4)
+    assert counts[centre] == expected
+    assert fam.shape[0] == counts.max() + 1  # trimmed to max count + 1 rows
+    # descending, zero padded, symmetric
+    for i in range(x.shape[1]):
+        col = fam[:, i]
+        nz = col[col > 0]
+        assert np.all(np.diff(nz) < 0) and np.all(col[len(nz):] == 0)
+    pairs = {(i, j - 1) for i in range(x.shape[1]) for j in fam[:, i] if j > 0}
+    assert all((j, i) in pairs for i, j in pairs)
+
+
+def test_family_overflow_raises(oracle):
+    x, _ = lattice.cuboid(7, 7, 7, 1.0)
+    with pytest.raises(IndexError):
+        oracle.cal_family(x, 3.015, 122)  # needs max_neigh > 122
+    oracle.cal_family(x, 3.015, 123)
+
+
+def test_homogeneous_stretch_lps_dilatation(oracle):
+    k = 1.002
+    mat = lattice_block(7, 1.0e-3, 3.015, kind="lps", stretch=k)
+    env = oracle.OracleEnv([mat], [], [], 1e-9)
+    env.update_acc()
+    th = env.blocks[0].theta
+    # theta_i = 3/m_i sum |xi| (k-1)|xi| V_j = 3(k-1)  (peri.jl:168, 349)
+    assert np.allclose(th, 3 * (k - 1), rtol=1e-9, atol=0)
+
+
+def test_homogeneous_stretch_pmb_interior_zero_and_breaks(oracle):
+    cs = 0.01
+    for k, expect_broken in ((1 + 0.5 * cs, False), (1 + 1.5 * cs, True)):
+        mat = lattice_block(9, 1.0e-3, 3.015, kind="pmb", stretch=k, cs=cs)
+        env = oracle.OracleEnv([mat], [], [], 1e-9)
+        env.update_acc()
+        B = env.blocks[0]
+        n_bonds = int((B.family > 0).sum())
+        if expect_broken:
+            assert B.intact.sum() == 0 and np.all(env.f == 0)
+            assert np.all(env.damage() == 1.0)
+        else:
+            assert B.intact.sum() == n_bonds
+            centre = 4 + 9 * (4 + 9 * 4)
+            scale = np.abs(env.f).max()
+            assert np.abs(env.f[:, centre]).max() <= 1e-9 * scale
+            assert np.all(env.damage() == 0.0)
+
+
+def test_rigid_translation_is_gated(oracle):
+    mat = lattice_block(6, 1.0e-3, 3.015)
+    mat.general.y[:] = mat.general.x + np.array([[1e-4], [-2e-4], [3e-4]])
+    mat.general.deformed[0] = True  # y0 != x, but a rigid translate
+    env = oracle.OracleEnv([mat], [], [], 1e-9)
+    env.blocks[0].deformed = False
+    env.update_acc()
+    assert np.all(env.f == 0.0) and env.blocks[0].deformed is False
+
+
+def test_momentum_conservation(oracle):
+    w = configs.pmb_cube(n=8, spacing=1e-3, jitter=1e-5)
+    env = oracle.OracleEnv(w["materials"], [], [], w["dt"])
+    for _ in range(5):
+        env.vv_step()
+    mf = env.mass * env.f
+    assert np.abs(mf.sum(axis=1)).max() <= 1e-9 * np.abs(mf).sum()
+
+
+@pytest.mark.parametrize("kind", ["pmb", "lps"])
+def test_gather_order_reproduces_serial_loop(oracle, kind):
+    """The GPU's per-particle A/B/C gather equals the reference's serial
+    scatter bit for bit, including the set of bonds broken."""
+    rng = np.random.default_rng(7)
+    mat = lattice_block(6, 1.0e-3, 3.015, kind=kind, jitter=2e-5, cs=0.002)
+    env = oracle.OracleEnv([mat], [], [], 1e-9)
+    B = env.blocks[0]
+    env.y[:] = B.x + rng.normal(0.0, 1.5e-6, size=B.x.shape)
+    intact_before = B.intact.copy()
+    env.update_acc()
+    assert 0 < (intact_before.sum() - B.intact.sum()) < intact_before.sum()  # some, not all, broke
+    spc = mat.specific
+    theta = None
+    if kind == "lps":
+        theta = gather_order.gather_theta(B.x, env.y, B.family, intact_before.astype(bool), B.vol, B.m)
+        assert np.array_equal(theta, B.theta)
+    f, intact_after = gather_order.gather_force(
+        0 if kind == "pmb" else 1, B.x, env.y, B.family, intact_before.astype(bool), B.type_rel, B.cs, B.density,
+        B.vol, B.c, m=B.m, theta=theta, K=getattr(spc, "bulk_modulus", None), G=getattr(spc, "shear_modulus", None))
+    assert np.array_equal(f, env.f)
+    assert np.array_equal(intact_after, B.intact.astype(bool))
+
+
+def test_threaded_oracle_matches_serial(oracle):
+    w1 = configs.pmb_cube(n=8, spacing=1e-3, jitter=1e-5)
+    e1 = oracle.OracleEnv(w1["materials"], [], [], w1["dt"], nthreads=1)
+    e4 = oracle.OracleEnv(w1["materials"], [], [], w1["dt"], nthreads=4)
+    for _ in range(3):
+        e1.vv_step()
+        e4.vv_step()
+    assert np.allclose(e1.y, e4.y, rtol=1e-13, atol=0)
+    assert np.array_equal(e1.blocks[0].intact, e4.blocks[0].intact)
+
+
+def test_contact11_merge_walk_only_matches_first_member(oracle):
+    """The reference's merge walk (contacts.jl:539-573) scans the family
+    column from its largest entry, so only that entry can become a contact
+    neighbour -- the closed form the GPU kernel uses."""
+    rng = np.random.default_rng(3)
+    x, vol = lattice.cuboid(7, 7, 4, 1.0, jitter=0.05, seed=5)
+    fam, intact = oracle.cal_family(x, 3.015, 200)
+    intact = np.asfortranarray(intact & (rng.random(intact.shape) > 0.3), dtype=np.uint8)
+    y = np.asfortranarray(x + rng.normal(0, 0.1, size=x.shape))
+    n = x.shape[1]
+    rows = 50
+    for equi in (1.0, 1.5, 3.5):
+        nb = np.zeros((rows, n), dtype=np.int64, order="F")
+        oracle.lib().or_contact11_neighs(n, oracle._d(y), fam.shape[0], oracle._i(fam), oracle._u(intact), 5.0, equi,
+                                         30, rows, oracle._i(nb))
+        assert np.all(nb[1:] == 0)
+        for i in range(n):
+            q = fam[0, i]
+            expect = 0
+            if q > 0 and not intact[0, i]:
+                d = y[:, i] - y[:, q - 1]
+                if d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < equi * equi:
+                    expect = q
+            assert nb[0, i] == expect
+
+
+def test_contact12_neighs_bruteforce(oracle):
+    rng = np.random.default_rng(11)
+    x1 = np.asfortranarray(rng.uniform(0, 4, size=(3, 300)))
+    x2 = np.asfortranarray(rng.uniform(2, 6, size=(3, 400)))
+    dist, rows = 0.9, 7
+    nb = np.zeros((rows, 300), dtype=np.int64, order="F")
+    oracle.lib().or_contact12_neighs(300, oracle._d(x1), 400, oracle._d(x2), dist, rows, oracle._i(nb))
+    lo = np.maximum(x1.min(axis=1) - dist, x2.min(axis=1) - dist)
+    hi = np.minimum(x1.max(axis=1) + dist, x2.max(axis=1) + dist)
+    in2 = np.all((x2 > lo[:, None]) & (x2 < hi[:, None]), axis=0)
+    for i in range(300):
+        if not np.all((x1[:, i] > lo) & (x1[:, i] < hi)):
+            assert np.all(nb[:, i] == 0)
+            continue
+        d = x1[:, i:i + 1] - x2
+        d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2]
+        cand = np.nonzero(in2 & (d2 < dist * dist))[0] + 1
+        expect = np.zeros(rows, dtype=np.int64)
+        top = np.sort(cand)[::-1][:rows]
+        expect[: top.size] = top
+        assert np.array_equal(nb[:, i], expect)
