@@ -55,8 +55,9 @@ def build_workload(name, args):
     raise SystemExit(f"unknown workload {name}")
 
 
-# bytes per particle the bond-force kernel must move, by precision and kind
-# ("Algorithmic bytes"); bond term: 4 B index + 1 intact bit
+# Algorithmic bytes of one bond-force launch: per intact directed bond the
+# int32 neighbour index plus one intact bit; per particle the state the
+# kernel must stream (listed per precision below).
 BOND_BYTES = 4.125
 
 
