@@ -226,6 +226,19 @@ PD_API pd_status pd_env_check_finite(pd_env *env);
 PD_API pd_status pd_force_density_device(pd_env *env, int64_t block, double *f_dev,
                                   const double *y_dev, void *stream);
 
+/* Same computation as pd_force_density_device, for callers that cannot
+ * allocate device memory during the call (a host whose GPU memory belongs
+ * to another allocator's pool, or a time-step loop that must not take the
+ * implicit synchronisation of cudaMalloc/cudaFree).  It has no counterpart
+ * in the reference.  Its scratch is a fixed device array compiled into the
+ * library (4 MiB per GPU, held until exit): the block may hold at most 65536
+ * particles (padded to a multiple of 32), larger blocks get
+ * PD_ERR_UNSUPPORTED.  All calls on one GPU share that array, so calls that
+ * overlap on the GPU race; the first call on each device looks the array
+ * up and should precede any stream capture on that device. */
+PD_API pd_status pd_force_density_device_static(pd_env *env, int64_t block, double *f_dev,
+                                                const double *y_dev, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Instrumentation                                                         */
 /* ---------------------------------------------------------------------- */

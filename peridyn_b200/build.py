@@ -25,6 +25,7 @@ UNITS = [
     ("pd_solver.cu", ["-fmad=false"]),
     ("pd_env.cu", ["-fmad=false"]),
     ("pd_fast.cu", ["-fmad=true"]),
+    ("pd_noalloc.cu", ["-fmad=false"]),
 ]
 
 

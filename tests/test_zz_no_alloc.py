@@ -1,0 +1,75 @@
+"""pd_force_density_device_static: the allocation-free variant of
+pd_force_density_device, for hosts that cannot allocate device memory while
+a time step runs (their GPU memory belongs to another allocator's pool, or
+an allocation's implicit synchronisation is not acceptable there).
+
+Both entry points run, through the C ABI, on two identical environments;
+their outputs must agree exactly (the tolerance of the serial-order FP64
+path) on two calls in a row, the second call seeing the flags the first
+one broke and the array contents the first call left behind.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import peridyn_b200 as pb
+from peridyn_b200 import _abi, configs
+
+pytestmark = pytest.mark.gpu
+
+
+def _env(w):
+    return pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision="fp64_serial")
+
+
+def _call(fn, env, f, y):
+    import torch
+
+    yd = torch.from_numpy(np.ascontiguousarray(y.T)).cuda()
+    fd = torch.from_numpy(np.ascontiguousarray(f.T)).cuda()
+    _abi.check(fn(env._h, 0, ctypes.c_void_p(fd.data_ptr()), ctypes.c_void_p(yd.data_ptr()), None))
+    torch.cuda.synchronize()
+    return fd.cpu().numpy().T.copy()
+
+
+@pytest.mark.parametrize("builder", [lambda: configs.lps_bar(nx=30, ny=8, nz=8),
+                                     lambda: configs.pmb_cube(n=12)])
+def test_static_scratch_matches_allocating_entry_point(builder):
+    pytest.importorskip("torch")
+    L = _abi.lib()
+    w = builder()
+    env_a = _env(w)
+    env_b = _env(w)
+    rng = np.random.default_rng(21)
+    y0, _, _, _ = env_a.get_state()
+    for call in range(2):
+        y = np.asfortranarray(y0 + rng.normal(0.0, 3e-6, size=y0.shape))
+        f = np.asfortranarray(rng.normal(0.0, 1.0, size=y0.shape))
+        fa = _call(L.pd_force_density_device, env_a, f, y)
+        fb = _call(L.pd_force_density_device_static, env_b, f, y)
+        assert np.array_equal(fa, fb), f"call {call}: outputs differ"
+        fam_a, intact_a = env_a._family(0)
+        fam_b, intact_b = env_b._family(0)
+        assert np.array_equal(intact_a, intact_b), f"call {call}: bond flags differ"
+    assert intact_a.sum() < (fam_a > 0).sum()  # the calls broke bonds
+    env_a.close()
+    env_b.close()
+
+
+def test_static_scratch_rejects_large_blocks():
+    pytest.importorskip("torch")
+    import torch
+
+    L = _abi.lib()
+    w = configs.pmb_cube(dims=(42, 40, 40))  # 67200 particles > 65536
+    env = _env(w)
+    y, _, _, _ = env.get_state()
+    yd = torch.from_numpy(np.ascontiguousarray(y.T)).cuda()
+    fd = torch.zeros_like(yd)
+    st = L.pd_force_density_device_static(env._h, 0, ctypes.c_void_p(fd.data_ptr()),
+                                          ctypes.c_void_p(yd.data_ptr()), None)
+    assert st == _abi.PD_ERR_UNSUPPORTED
+    assert b"static scratch holds at most 65536" in L.pd_last_error()
+    assert torch.count_nonzero(fd).item() == 0
+    env.close()
