@@ -65,8 +65,40 @@ def particle_bytes(precision, lps):
     if precision == "fp64_serial":
         return 104 + (16 if lps else 0)  # x4 32 + y 32 + f 32 + cnt/tinfo 8 (+ m,theta 16)
     if precision == "fp64":
-        return 104 + (16 if lps else 0)
-    return 84 + (8 if lps else 0)  # fp32c
+        # x4 32, u 32 read + 32 write, v 32 + 32, cnt/tinfo 8, 1/rho 8 (+ theta/m, 1/m 16)
+        return 176 + (16 if lps else 0)
+    # fp32c: x 16, u32 16 read + 16 write, FP64 accumulator 24 + 24, v 16 + 16,
+    # cnt/tinfo 8, 1/rho 4, BC flags 1 (+ theta/m, 1/m 8)
+    return 141 + (8 if lps else 0)
+
+
+def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
+    """Error of a throughput-mode run against the serial-order FP64 path
+    (bit-identical to the CPU oracle) over the same run."""
+    import peridyn_b200 as pb
+
+    ref = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision="fp64_serial",
+                 device=device)
+    if work["bcs"]:
+        pb.apply_bc_at0(ref, 0)
+    pb.update_neighs(ref)
+    pb.update_acc(ref)
+    pb.velocity_verlet_step(ref, nsteps=sim_steps)
+    yr, vr, _, _ = ref.get_state()
+    yf, vf, _, _ = env_fast.get_state()
+    x = np.hstack([m.general.x for m in work["materials"]])
+    mism = 0
+    broken = 0
+    for b in range(len(work["materials"])):
+        fr, ir = ref._family(b)
+        _, i_f = env_fast._family(b)
+        mism += int((ir != i_f).sum())
+        broken += int((fr > 0).sum() - ir.sum())
+    ref.close()
+    l2 = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return {"vs": "fp64_serial GPU path (bit-identical to the CPU oracle)", "vv_steps": int(sim_steps),
+            "displacement_rel_l2": l2(yf - x, yr - x), "velocity_rel_l2": l2(vf, vr),
+            "broken_bonds_fp64": broken, "broken_bond_mismatch": mism}
 
 
 class ClockSampler:
@@ -184,6 +216,7 @@ def main():
     ap.add_argument("--nspec", type=int, default=256)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -314,6 +347,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_t = float(t.item())
     e2e_value = total_bonds / e2e_t
+    # the state now holds one complete run from the initial state
+    accuracy = None
+    if args.precision != "fp64_serial" and rank == 0 and not args.no_accuracy:
+        accuracy = accuracy_vs_serial(work, args.precision, sim_steps, env, local)
     # roofline of the bond-force kernel
     n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
     bytes_launch = bonds_start * BOND_BYTES + n_int * particle_bytes(args.precision, lps)
@@ -345,13 +382,14 @@ def main():
         "hbm_gbs_algorithmic": bytes_launch * sim_steps * args.steps / t_total / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "bond force (k_force_serial)" if args.precision == "fp64_serial" else "bond force",
+                     "kernel": "k_force_serial" if args.precision == "fp64_serial" else "k_step (fused bond force + velocity-Verlet)",
                      "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms, "launches_timed": int(prof_n.value),
                      "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured"
                      else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "accuracy": accuracy,
     }
     if world == 1 and not args.no_cpu_baseline:
         rate, n, dt = cpu_sample(work, args.cpu_sample_s, os.cpu_count() or 1)

@@ -771,6 +771,7 @@ static pd_status get_block_scalar(pd_env *env, int64_t block, double *out, int c
     PD_TRY(need_final(env));
     if (block < 0 || block >= (int64_t)env->hb.size() || !out) return fail(PD_ERR_ARG, "bad block or NULL output");
     CK(cudaSetDevice(env->device));
+    PD_TRY(pd::sync_state_to_fp64(env, false));
     const HostBlock &b = env->hb[block];
     std::vector<double2> h(b.n);
     CK(cudaMemcpyAsync(h.data(), env->mth.p + b.first_int, b.n * sizeof(double2), cudaMemcpyDeviceToHost, env->st));
@@ -811,7 +812,7 @@ static pd_status upload3(pd_env *env, const double *src, double4 *dst) {
 extern "C" pd_status pd_env_get_state(pd_env *env, double *y, double *v, double *f, double *p) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
-    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(pd::sync_state_to_fp64(env, false));
     PD_TRY(download3(env, env->y.p, y));
     PD_TRY(download3(env, env->v.p, v));
     PD_TRY(download3(env, env->f.p, f));
@@ -885,7 +886,7 @@ extern "C" pd_status pd_env_damage(pd_env *env, double *damage) {
     PD_TRY(need_final(env));
     if (!damage) return fail(PD_ERR_ARG, "damage is NULL");
     CK(cudaSetDevice(env->device));
-    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(pd::sync_state_to_fp64(env, false));
     std::vector<double> dint;
     PD_TRY(damage_internal(env, dint));
     for (int64_t e = 0; e < env->N_env; ++e) damage[e] = dint[env->map_h[e]];
@@ -896,7 +897,7 @@ extern "C" pd_status pd_env_diagnostics(pd_env *env, double *out8) {
     PD_TRY(need_final(env));
     if (!out8) return fail(PD_ERR_ARG, "out is NULL");
     CK(cudaSetDevice(env->device));
-    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(pd::sync_state_to_fp64(env, false));
     double h[3];
     launch_sum4(env->st, env->N, env->p.p, env->partials.p, env->out3.p);
     CK(cudaMemcpyAsync(h, env->out3.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, env->st));
@@ -940,7 +941,7 @@ extern "C" pd_status pd_env_deformed(pd_env *env, uint8_t *flags) {
 extern "C" pd_status pd_env_check_finite(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
-    PD_TRY(pd::sync_state_to_fp64(env));
+    PD_TRY(pd::sync_state_to_fp64(env, false));
     CK(cudaMemsetAsync(env->flag.p, 0, 4, env->st));
     launch_nonfinite(env->st, env->N, env->y.p, env->flag.p);
     launch_nonfinite(env->st, env->N, env->v.p, env->flag.p);

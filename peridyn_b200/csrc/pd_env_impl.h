@@ -187,8 +187,12 @@ void prof_end(pd_env *env, cudaStream_t st);
 pd_status contacts_finalize(pd_env *env);
 pd_status contacts_update_neighs(pd_env *env, int64_t max_part);
 pd_status contacts_force(pd_env *env);
-pd_status sync_state_to_fp64(pd_env *env);
+// Bring the FP64 arrays up to date with the throughput-mode state; with
+// invalidate the throughput state is rebuilt from them on its next use
+// (for callers that modify y, v, f or the dilatation).
+pd_status sync_state_to_fp64(pd_env *env, bool invalidate = true);
 void fast_release(pd_env *env);
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps);
+pd_status fast_update_acc(pd_env *env);
 pd_status update_acc_serial(pd_env *env);
 }  // namespace pd

@@ -1,19 +1,922 @@
-// pd_fast.cu -- throughput modes (PD_PREC_FP64, PD_PREC_FP32C).
+// pd_fast.cu -- throughput modes PD_PREC_FP32C and PD_PREC_FP64.
+//
+// One launch per velocity-Verlet step (two for state-based blocks): the
+// thread of particle p gathers p's bond forces once (no serial replay), and
+// then, still in registers, applies the second half kick, the boundary
+// velocities, the next step's half kick, the drift and the boundary
+// positions, writing the next displacement into the other half of a double
+// buffer that neighbours read in the next launch.
+//
+// FP32C: bond arithmetic in FP32 on FP32 displacements u = y - x, with the
+// cancellation-free extension e = (2 xi.eta + eta.eta) / (|xi+eta| + |xi|);
+// positions are accumulated in FP64 (u64) and rounded to FP32 once per step.
+// Reference positions are stored in FP32 relative to the block's centre.
+// FP64: the same single-pass algorithm in FP64 throughout.
+//
+// Per bond (general_material.jl:332-362 restated with the identities
+// w|xi| = 1 and e*w = s):
+//   s   = e / |xi|                          (break when s >= cs)
+//   PMB t = c s                             (bond_based.jl:195-231)
+//   LPS t = (3K-5G)(theta_p/m_p + theta_q/m_q) + 15G s (1/m_p + 1/m_q)
+//                                           (ordinary_state_based.jl:176-187)
+//   f_p += (t / (2|Y|)) V_q Y  ... scaled by 1/rho_p once per particle.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "pd_env_impl.h"
 
 namespace pd {
+namespace {
 
-pd_status sync_state_to_fp64(pd_env *env) {
-    (void)env;
+constexpr int kT = 128;
+inline unsigned gridn(int64_t n, int t = kT) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+template <class R>
+struct Tr;
+template <>
+struct Tr<float> {
+    using V4 = float4;
+    using V2 = float2;
+    static __device__ __forceinline__ float rsq(float a) { return rsqrtf(a); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+};
+template <>
+struct Tr<double> {
+    using V4 = double4;
+    using V2 = double2;
+    static __device__ __forceinline__ double rsq(double a) { return rsqrt(a); }
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+};
+
+template <class R>
+struct FBlock {
+    int32_t kind, nt, pair_base, pad;
+    R c11;
+};
+template <class R>
+struct FPair {
+    R cs, k35, g15, pad;
+};
+
+constexpr int kMaxFastBC = 8;
+struct FBC {
+    int32_t kind, dims;
+    double rate[3];
+    int64_t n;
+    const int32_t *idx;  // ascending internal indices
+    double4 *last;
+};
+
+template <class R>
+struct StepArgs {
+    int64_t N;
+    const typename Tr<R>::V4 *x;  // (x, vol): FP32C relative to the block centre
+    const typename Tr<R>::V4 *ucur;
+    typename Tr<R>::V4 *unext;
+    double *ax, *ay, *az;  // FP64 displacement accumulator (FP32C)
+    typename Tr<R>::V4 *v, *f, *p;
+    const R *irho, *mass;
+    typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
+    const int32_t *tinfo, *cnt, *nbr;
+    const int64_t *slice_ptr;
+    uint32_t *words;
+    const FBlock<R> *fb;
+    const FPair<R> *fp;
+    const int32_t *deformed;
+    const double4 *x64;
+    const uint8_t *bcbits;
+    R c;
+    double dt;
+    int nbc;
+    uint32_t dir_vel, dir_pos;  // bit k set: BC k moves in the negative direction
+    FBC bc[kMaxFastBC];
+};
+
+__device__ __forceinline__ int64_t lower_bound_i32(const int32_t *a, int64_t n, int32_t key) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double &cmp(double4 &a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
+
+// Gather of p's bonds.  Returns the acceleration before the 1/rho scaling.
+template <class R, int KIND, bool kBreak>
+__device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, const FBlock<R> &B, int tp,
+                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
+                                            R &fz) {
+    using V4 = typename Tr<R>::V4;
+    const int32_t n = a.cnt[p];
+    const int64_t sp = a.slice_ptr[p >> 5];
+    const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+    R Ap = 0, Bp = 0;
+    if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
+        typename Tr<R>::V2 m = a.mab[p];
+        Ap = m.x;
+        Bp = m.y;
+    }
+    FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
+    for (int32_t w0 = 0; w0 < n; w0 += 32) {
+        const uint32_t w = a.words[wb + 32 * (int64_t)(w0 >> 5)];
+        uint32_t m = w, nw = w;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t k = w0 + j;
+            const int32_t q = a.nbr[base + 32 * (int64_t)k];
+            const V4 xq = a.x[q];
+            const V4 uq = a.ucur[q];
+            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
+            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
+            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+            const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
+            const R lx = xx2 * rx, ly = yy2 * ry;
+            const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
+            const R dl = (ly + lx) * lx;
+            if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
+            if (!(num < pp.cs * dl)) {
+                if (kBreak) nw &= ~(1u << j);
+                continue;
+            }
+            const R s = Tr<R>::div(num, dl);
+            R t;
+            if (KIND == PD_MAT_BOND_BASED) {
+                t = B.c11 * s;
+            } else {
+                typename Tr<R>::V2 mq = a.mab[q];
+                t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
+            }
+            const R coef = R(0.5) * t * ry * xq.w;
+            fx += coef * Y0;
+            fy += coef * Y1;
+            fz += coef * Y2;
+        }
+        if (kBreak && nw != w) a.words[wb + 32 * (int64_t)(w0 >> 5)] = nw;
+    }
+}
+
+// BC velocity (boundary_conditions.jl:122-126): FixBC v = 0, ToFroBC v = dir*rate.
+template <class R>
+__device__ __forceinline__ void bc_velocity(const StepArgs<R> &a, uint8_t bits, R &v0, R &v1, R &v2) {
+    for (int k = 0; k < a.nbc; ++k) {
+        if (!((bits >> k) & 1)) continue;
+        const FBC &b = a.bc[k];
+        const double dir = ((a.dir_vel >> k) & 1) ? -1.0 : 1.0;
+        R vv[3] = {v0, v1, v2};
+        for (int d = 0; d < 3; ++d)
+            if ((b.dims >> d) & 1) vv[d] = b.kind == PD_BC_FIX ? R(0) : R(dir * b.rate[d]);
+        v0 = vv[0];
+        v1 = vv[1];
+        v2 = vv[2];
+    }
+}
+
+// BC position (boundary_conditions.jl:107-111) on the FP64 displacement.
+template <class R>
+__device__ __forceinline__ void bc_position(const StepArgs<R> &a, int64_t p, uint8_t bits, double &u0, double &u1,
+                                            double &u2) {
+    const double4 x = a.x64[p];
+    double y[3] = {x.x + u0, x.y + u1, x.z + u2};
+    for (int k = 0; k < a.nbc; ++k) {
+        if (!((bits >> k) & 1)) continue;
+        const FBC &b = a.bc[k];
+        const int64_t r = lower_bound_i32(b.idx, b.n, (int32_t)p);
+        double4 last = b.last[r];
+        const double step = a.dt * (((a.dir_pos >> k) & 1) ? -1.0 : 1.0);
+        for (int d = 0; d < 3; ++d) {
+            if (!((b.dims >> d) & 1)) continue;
+            if (b.kind == PD_BC_FIX) {
+                y[d] = cmp(last, d);
+            } else {
+                const double nl = cmp(last, d) + step * b.rate[d];
+                y[d] = nl;
+                cmp(last, d) = nl;
+            }
+        }
+        if (b.kind != PD_BC_FIX) b.last[r] = last;
+    }
+    u0 = y[0] - x.x;
+    u1 = y[1] - x.y;
+    u2 = y[2] - x.z;
+}
+
+template <class R>
+__device__ __forceinline__ void load_u(const StepArgs<R> &a, int64_t p, double &u0, double &u1, double &u2) {
+    if (sizeof(R) == 4) {
+        u0 = a.ax[p];
+        u1 = a.ay[p];
+        u2 = a.az[p];
+    } else {
+        const typename Tr<R>::V4 u = a.ucur[p];
+        u0 = (double)u.x;
+        u1 = (double)u.y;
+        u2 = (double)u.z;
+    }
+}
+
+template <class R>
+__device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double u0, double u1, double u2) {
+    if (sizeof(R) == 4) {
+        a.ax[p] = u0;
+        a.ay[p] = u1;
+        a.az[p] = u2;
+    }
+    typename Tr<R>::V4 o;
+    o.x = (R)u0;
+    o.y = (R)u1;
+    o.z = (R)u2;
+    o.w = R(0);
+    a.unext[p] = o;
+}
+
+// MODE 0: force only (update_acc!): f, p = m v.
+// MODE 1: full step, another step follows: f, kick, BC vel, kick, drift,
+//         BC pos -> next displacement.
+// MODE 2: full step, last of the chunk: f, p, kick, BC vel, store v and f.
+// MODE 3: integration only (forces already in f, e.g. after contacts).
+// MODE 4: integration only, last of the chunk.
+template <class R, int MODE>
+__global__ void __launch_bounds__(kT) k_step(StepArgs<R> a) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
+    if (p >= a.N) return;
+    const int32_t ti = a.tinfo[p];
+    if (ti < 0) {
+        if (MODE == 1 || MODE == 3) a.unext[p] = V4{};
+        return;
+    }
+    R fx = 0, fy = 0, fz = 0;
+    if (MODE <= 2) {
+        const int b = ti >> 8, tp = ti & 255;
+        const FBlock<R> B = a.fb[b];
+        if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
+            const V4 xp = a.x[p], up = a.ucur[p];
+            if (B.kind == PD_MAT_BOND_BASED)
+                bond_gather<R, PD_MAT_BOND_BASED, true>(a, p, B, tp, xp, up, fx, fy, fz);
+            else
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, true>(a, p, B, tp, xp, up, fx, fy, fz);
+            const R ir = a.irho[p];
+            fx *= ir;
+            fy *= ir;
+            fz *= ir;
+        }
+    } else {
+        const V4 ff = a.f[p];
+        fx = ff.x;
+        fy = ff.y;
+        fz = ff.z;
+    }
+    V4 vp = a.v[p];
+    if (MODE == 0) {
+        a.f[p] = V4{fx, fy, fz, R(0)};
+        const R m = a.mass[p];
+        a.p[p] = V4{m * vp.x, m * vp.y, m * vp.z, R(0)};
+        return;
+    }
+    if (MODE == 2 || MODE == 4) {
+        const R m = a.mass[p];
+        if (MODE == 2) a.p[p] = V4{m * vp.x, m * vp.y, m * vp.z, R(0)};
+    }
+    const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
+    R v0 = vp.x + a.c * fx, v1 = vp.y + a.c * fy, v2 = vp.z + a.c * fz;
+    if (bits) bc_velocity(a, bits, v0, v1, v2);
+    if (MODE == 2 || MODE == 4) {
+        a.v[p] = V4{v0, v1, v2, R(0)};
+        a.f[p] = V4{fx, fy, fz, R(0)};
+        return;
+    }
+    v0 += a.c * fx;
+    v1 += a.c * fy;
+    v2 += a.c * fz;
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    u0 += a.dt * (double)v0;
+    u1 += a.dt * (double)v1;
+    u2 += a.dt * (double)v2;
+    if (bits) bc_position(a, p, bits, u0, u1, u2);
+    a.v[p] = V4{v0, v1, v2, R(0)};
+    store_u(a, p, u0, u1, u2);
+}
+
+// First half of a step (velocity_verlet.jl:62-69) from the stored force.
+template <class R>
+__global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
+    if (p >= a.N) return;
+    if (a.tinfo[p] < 0) {
+        a.unext[p] = V4{};
+        return;
+    }
+    const V4 ff = a.f[p], vp = a.v[p];
+    const R v0 = vp.x + a.c * ff.x, v1 = vp.y + a.c * ff.y, v2 = vp.z + a.c * ff.z;
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    u0 += a.dt * (double)v0;
+    u1 += a.dt * (double)v1;
+    u2 += a.dt * (double)v2;
+    const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
+    if (bits) bc_position(a, p, bits, u0, u1, u2);
+    a.v[p] = V4{v0, v1, v2, R(0)};
+    store_u(a, p, u0, u1, u2);
+}
+
+// Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
+// bonds; stores theta_p/m_p for the force pass.
+template <class R>
+__global__ void __launch_bounds__(kT) k_theta(StepArgs<R> a) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
+    if (p >= a.N) return;
+    const int32_t ti = a.tinfo[p];
+    if (ti < 0) return;
+    const FBlock<R> B = a.fb[ti >> 8];
+    if (B.kind != PD_MAT_ORDINARY_STATE_BASED) return;
+    const V4 xp = a.x[p], up = a.ucur[p];
+    const int32_t n = a.cnt[p];
+    const int64_t sp = a.slice_ptr[p >> 5];
+    const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+    R acc = 0;
+    for (int32_t w0 = 0; w0 < n; w0 += 32) {
+        uint32_t m = a.words[wb + 32 * (int64_t)(w0 >> 5)];
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t q = a.nbr[base + 32 * (int64_t)(w0 + j)];
+            const V4 xq = a.x[q], uq = a.ucur[q];
+            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
+            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
+            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+            const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
+            const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
+            acc += Tr<R>::div(num, ly + lx) * xq.w;
+        }
+    }
+    typename Tr<R>::V2 mb = a.mab[p];
+    mb.x = R(3) * acc * mb.y * mb.y;  // theta/m = (3/m) acc / m
+    a.mab[p] = mb;
+}
+
+// Deformed gate on y = x + u (general_material.jl:243-255).
+constexpr int kGB = 148, kGT = 256;
+template <class R>
+__global__ void __launch_bounds__(kGT) k_fgate_partial(StepArgs<R> a, int64_t first, int64_t n, double *part,
+                                                      const int32_t *flag) {
+    if (*flag) return;
+    __shared__ double sh[3][kGT];
+    double u0, u1, u2;
+    load_u(a, first, u0, u1, u2);
+    const double4 x1 = a.x64[first];
+    const double y10 = x1.x + u0, y11 = x1.y + u1, y12 = x1.z + u2;
+    double sd = 0, sa = 0, sx = 0;
+    for (int64_t l = blockIdx.x * (int64_t)kGT + threadIdx.x; l < n; l += (int64_t)kGB * kGT) {
+        const double4 xi = a.x64[first + l];
+        load_u(a, first + l, u0, u1, u2);
+        const double A0 = ((xi.x + u0) - y10) + x1.x, A1 = ((xi.y + u1) - y11) + x1.y, A2 = ((xi.z + u2) - y12) + x1.z;
+        const double d0 = A0 - xi.x, d1 = A1 - xi.y, d2 = A2 - xi.z;
+        sd += d0 * d0 + d1 * d1 + d2 * d2;
+        sa += A0 * A0 + A1 * A1 + A2 * A2;
+        sx += xi.x * xi.x + xi.y * xi.y + xi.z * xi.z;
+    }
+    sh[0][threadIdx.x] = sd;
+    sh[1][threadIdx.x] = sa;
+    sh[2][threadIdx.x] = sx;
+    __syncthreads();
+    for (int s = kGT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int c = 0; c < 3; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; ++c) part[3 * blockIdx.x + c] = sh[c][0];
+}
+
+__global__ void k_fgate_final(const double *part, int32_t *flag) {
+    if (*flag) return;
+    double sd = 0, sa = 0, sx = 0;
+    for (int b = 0; b < kGB; ++b) {
+        sd += part[3 * b];
+        sa += part[3 * b + 1];
+        sx += part[3 * b + 2];
+    }
+    const double d = sqrt(sd);
+    const bool approx = isfinite(d) && d <= fmax(0.0, 0x1p-26 * fmax(sqrt(sa), sqrt(sx)));
+    if (!approx) *flag = 1;
+}
+
+// FP64 state -> fast state.
+template <class R>
+__global__ void k_import(int64_t N, const double4 *x4, const double4 *y, const double4 *v, const double4 *f,
+                         const double4 *pm, const double *mass, const double *dens, const double2 *mth,
+                         const int32_t *tinfo, const DevBlock *blocks, StepArgs<R> a) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const double4 xi = x4[p], yi = y[p], vi = v[p], fi = f[p], pi = pm[p];
+    const double u0 = yi.x - xi.x, u1 = yi.y - xi.y, u2 = yi.z - xi.z;
+    V4 xs;
+    const int32_t ti = tinfo[p];
+    if (sizeof(R) == 4 && ti >= 0) {
+        const double3 c = blocks[ti >> 8].center;
+        xs = V4{(R)(xi.x - c.x), (R)(xi.y - c.y), (R)(xi.z - c.z), (R)xi.w};
+    } else {
+        xs = V4{(R)xi.x, (R)xi.y, (R)xi.z, (R)xi.w};
+    }
+    if (sizeof(R) == 4) {
+        const_cast<V4 *>(a.x)[p] = xs;
+        a.ax[p] = u0;
+        a.ay[p] = u1;
+        a.az[p] = u2;
+    }
+    const_cast<V4 *>(a.ucur)[p] = V4{(R)u0, (R)u1, (R)u2, R(0)};
+    a.v[p] = V4{(R)vi.x, (R)vi.y, (R)vi.z, R(0)};
+    a.f[p] = V4{(R)fi.x, (R)fi.y, (R)fi.z, R(0)};
+    a.p[p] = V4{(R)pi.x, (R)pi.y, (R)pi.z, R(0)};
+    const_cast<R *>(a.irho)[p] = ti >= 0 ? (R)(1.0 / dens[p]) : R(0);
+    const_cast<R *>(a.mass)[p] = (R)mass[p];
+    const double m = mth[p].x;
+    a.mab[p] = typename Tr<R>::V2{(R)(m > 0 ? mth[p].y / m : 0.0), (R)(m > 0 ? 1.0 / m : 0.0)};
+}
+
+// fast state -> FP64 state (y = x + u, v, f, p, theta).
+template <class R>
+__global__ void k_export(int64_t N, const double4 *x4, double4 *y, double4 *v, double4 *f, double4 *pm, double2 *mth,
+                         StepArgs<R> a) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    const double4 xi = x4[p];
+    y[p] = make_double4(xi.x + u0, xi.y + u1, xi.z + u2, 0.0);
+    const typename Tr<R>::V4 vi = a.v[p], fi = a.f[p], pi = a.p[p];
+    v[p] = make_double4(vi.x, vi.y, vi.z, 0.0);
+    f[p] = make_double4(fi.x, fi.y, fi.z, 0.0);
+    pm[p] = make_double4(pi.x, pi.y, pi.z, 0.0);
+    const typename Tr<R>::V2 mb = a.mab[p];
+    if (mb.y != R(0)) mth[p].y = (double)mb.x / (double)mb.y;
+}
+
+// Contact accelerations added to the fast force (nonlinearspring.jl:124-145,
+// contacts.jl:210-247 / 357-381), evaluated in FP64 on y = x + u.
+struct CLawF {
+    double equi, expo, K;
+};
+__device__ __forceinline__ void cfn(const CLawF &c, double d0, double d1, double d2, double &F0, double &F1,
+                                    double &F2) {
+    const double mag = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    const double del = c.equi - mag;
+    if (del < 0.0) {
+        F0 = F1 = F2 = 0.0;
+        return;
+    }
+    const double strain = del / c.equi;
+    double pw;
+    if (c.expo == 1.0) pw = strain;
+    else if (c.expo == 2.0) pw = strain * strain;
+    else pw = pow(strain, c.expo);
+    const double s = c.K * pw / (mag + 1e-10);
+    F0 = s * d0;
+    F1 = s * d1;
+    F2 = s * d2;
+}
+
+template <class R>
+__device__ __forceinline__ void ypos(const StepArgs<R> &a, int64_t p, double &y0, double &y1, double &y2) {
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    const double4 x = a.x64[p];
+    y0 = x.x + u0;
+    y1 = x.y + u1;
+    y2 = x.z + u2;
+}
+
+template <class R>
+__global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows, const int32_t *nb,
+                         const double *dens, CLawF law) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n1) return;
+    const int64_t p = first1 + i;
+    double yi0, yi1, yi2, a0 = 0, a1 = 0, a2 = 0;
+    ypos(a, p, yi0, yi1, yi2);
+    const double inv = 1.0 / dens[p];
+    for (int64_t r = 0; r < rows; ++r) {
+        const int32_t j = nb[r * n1 + i];
+        if (j < 0) break;
+        double yj0, yj1, yj2, F0, F1, F2;
+        ypos(a, j, yj0, yj1, yj2);
+        cfn(law, yi0 - yj0, yi1 - yj1, yi2 - yj2, F0, F1, F2);
+        const double s = a.x64[j].w * inv;
+        a0 += F0 * s;
+        a1 += F1 * s;
+        a2 += F2 * s;
+    }
+    typename Tr<R>::V4 f = a.f[p];
+    f.x += (R)a0;
+    f.y += (R)a1;
+    f.z += (R)a2;
+    a.f[p] = f;
+}
+
+template <class R>
+__global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_t *roff, const int32_t *rev,
+                         const double *dens, CLawF law) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n2) return;
+    const int32_t o = roff[j], e = roff[j + 1];
+    if (o == e) return;
+    const int64_t q = first2 + j;
+    double yj0, yj1, yj2, a0 = 0, a1 = 0, a2 = 0;
+    ypos(a, q, yj0, yj1, yj2);
+    const double inv = 1.0 / dens[q];
+    for (int32_t r = o; r < e; ++r) {
+        const int32_t i = rev[r];
+        double yi0, yi1, yi2, F0, F1, F2;
+        ypos(a, i, yi0, yi1, yi2);
+        cfn(law, yi0 - yj0, yi1 - yj1, yi2 - yj2, F0, F1, F2);
+        const double s = a.x64[i].w * inv;
+        a0 -= F0 * s;
+        a1 -= F1 * s;
+        a2 -= F2 * s;
+    }
+    typename Tr<R>::V4 f = a.f[q];
+    f.x += (R)a0;
+    f.y += (R)a1;
+    f.z += (R)a2;
+    a.f[q] = f;
+}
+
+template <class R>
+__global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, const int32_t *nb11, const int32_t *roff,
+                       const int32_t *rev, const double *dens, CLawF law) {
+    const int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (li >= n) return;
+    const int64_t p = first + li;
+    const int32_t o = roff[li], e = roff[li + 1], q = nb11[li];
+    if (o == e && q < 0) return;
+    double yp0, yp1, yp2, a0 = 0, a1 = 0, a2 = 0, F0, F1, F2;
+    ypos(a, p, yp0, yp1, yp2);
+    const double den = dens[p], vol = a.x64[p].w;
+    for (int32_t r = o; r < e; ++r) {
+        double yi0, yi1, yi2;
+        ypos(a, rev[r], yi0, yi1, yi2);
+        cfn(law, yi0 - yp0, yi1 - yp1, yi2 - yp2, F0, F1, F2);
+        a0 -= F0 * (vol / den);
+        a1 -= F1 * (vol / den);
+        a2 -= F2 * (vol / den);
+    }
+    if (q >= 0) {
+        double yq0, yq1, yq2;
+        ypos(a, q, yq0, yq1, yq2);
+        cfn(law, yp0 - yq0, yp1 - yq1, yp2 - yq2, F0, F1, F2);
+        const double s = a.x64[q].w / den;
+        a0 += F0 * s;
+        a1 += F1 * s;
+        a2 += F2 * s;
+    }
+    typename Tr<R>::V4 f = a.f[p];
+    f.x += (R)a0;
+    f.y += (R)a1;
+    f.z += (R)a2;
+    a.f[p] = f;
+}
+
+// ----------------------------------------------------------------------
+// host-side state
+// ----------------------------------------------------------------------
+template <class R>
+struct Fast {
+    using V4 = typename Tr<R>::V4;
+    using V2 = typename Tr<R>::V2;
+    DBuf<V4> x, u[2], v, f, p;
+    DBuf<double> ax, ay, az;
+    DBuf<R> irho, mass;
+    DBuf<V2> mab;
+    DBuf<FBlock<R>> fb;
+    DBuf<FPair<R>> fp;
+    DBuf<uint8_t> bcbits;
+    DBuf<double> gpart;
+    int cur = 0;
+};
+
+struct FastHolder {
+    int prec = 0;
+    Fast<float> f32;
+    Fast<double> f64;
+    bool dirty = false;  // fast state newer than the FP64 arrays
+};
+
+FastHolder *holder(pd_env *env) { return (FastHolder *)env->fast; }
+
+template <class R>
+StepArgs<R> args(pd_env *env, Fast<R> &F) {
+    StepArgs<R> a{};
+    a.N = env->N;
+    a.x = sizeof(R) == 4 ? F.x.p : (const typename Tr<R>::V4 *)(void *)env->x4.p;
+    a.ucur = F.u[F.cur].p;
+    a.unext = F.u[1 - F.cur].p;
+    a.ax = F.ax.p;
+    a.ay = F.ay.p;
+    a.az = F.az.p;
+    a.v = F.v.p;
+    a.f = F.f.p;
+    a.p = F.p.p;
+    a.irho = F.irho.p;
+    a.mass = F.mass.p;
+    a.mab = F.mab.p;
+    a.tinfo = env->tinfo.p;
+    a.cnt = env->cnt.p;
+    a.nbr = env->nbr.p;
+    a.slice_ptr = env->slice_ptr.p;
+    a.words = env->words[env->cur].p;
+    a.fb = F.fb.p;
+    a.fp = F.fp.p;
+    a.deformed = env->deformed.p;
+    a.x64 = env->x4.p;
+    a.bcbits = F.bcbits.p;
+    a.c = (R)(env->dt / 2);
+    a.dt = env->dt;
+    a.nbc = (int)env->hbc.size();
+    for (size_t k = 0; k < env->hbc.size() && k < (size_t)kMaxFastBC; ++k) {
+        const HostBC &h = env->hbc[k];
+        FBC &b = a.bc[k];
+        b.kind = h.kind;
+        b.dims = h.dims;
+        for (int d = 0; d < 3; ++d) b.rate[d] = h.rate[d];
+        b.n = env->bcs[k].n;
+        b.idx = env->bcs[k].idx.p;
+        b.last = env->bcs[k].last.p;
+    }
+    return a;
+}
+
+uint32_t dir_bits(const pd_env *env) {
+    uint32_t m = 0;
+    for (size_t k = 0; k < env->hbc.size(); ++k)
+        if (env->hbc[k].dir < 0) m |= 1u << k;
+    return m;
+}
+
+template <class R>
+pd_status init_fast(pd_env *env, Fast<R> &F) {
+    const int64_t N = env->N;
+    if (!F.u[0].p) {
+        if (sizeof(R) == 4) {
+            PD_TRY(F.x.alloc(N));
+            PD_TRY(F.ax.alloc(N));
+            PD_TRY(F.ay.alloc(N));
+            PD_TRY(F.az.alloc(N));
+        }
+        PD_TRY(F.u[0].alloc(N));
+        PD_TRY(F.u[1].alloc(N));
+        PD_TRY(F.v.alloc(N));
+        PD_TRY(F.f.alloc(N));
+        PD_TRY(F.p.alloc(N));
+        PD_TRY(F.irho.alloc(N));
+        PD_TRY(F.mass.alloc(N));
+        PD_TRY(F.mab.alloc(N));
+        PD_TRY(F.bcbits.alloc(N));
+        PD_TRY(F.gpart.alloc(3 * kGB));
+        // parameters in the working precision
+        std::vector<FBlock<R>> fb;
+        std::vector<FPair<R>> fp;
+        for (const auto &b : env->hb) {
+            FBlock<R> d{};
+            d.kind = b.kind;
+            d.nt = b.nt;
+            d.pair_base = (int32_t)fp.size();
+            d.c11 = (R)b.c[0];
+            fb.push_back(d);
+            for (int j = 0; j < b.nt; ++j)
+                for (int i = 0; i < b.nt; ++i) {
+                    size_t e = (size_t)i + (size_t)j * b.nt;
+                    FPair<R> pp{};
+                    pp.cs = (R)b.cs[e];
+                    pp.k35 = (R)(3 * b.K[e] - 5 * b.G[e]);
+                    pp.g15 = (R)(15 * b.G[e]);
+                    fp.push_back(pp);
+                }
+        }
+        PD_TRY(F.fb.alloc(fb.size()));
+        PD_TRY(F.fp.alloc(fp.size()));
+        CK(cudaMemcpyAsync(F.fb.p, fb.data(), fb.size() * sizeof(FBlock<R>), cudaMemcpyHostToDevice, env->st));
+        CK(cudaMemcpyAsync(F.fp.p, fp.data(), fp.size() * sizeof(FPair<R>), cudaMemcpyHostToDevice, env->st));
+        std::vector<uint8_t> bits(N, 0);
+        for (size_t k = 0; k < env->hbc.size(); ++k)
+            for (int64_t e : env->hbc[k].env_idx) bits[env->map_h[e]] |= (uint8_t)(1u << k);
+        CK(cudaMemcpyAsync(F.bcbits.p, bits.data(), N, cudaMemcpyHostToDevice, env->st));
+        CK(cudaStreamSynchronize(env->st));
+    }
+    F.cur = 0;
+    StepArgs<R> ai = args(env, F);  // FP64 reads x4 in place; FP32C fills F.x
+    k_import<R><<<gridn(env->N, 256), 256, 0, env->st>>>(env->N, env->x4.p, env->y.p, env->v.p, env->f.p, env->p.p,
+                                                         env->mass.p, env->dens.p, env->mth.p, env->tinfo.p,
+                                                         env->blocks_d.p, ai);
+    note_launch();
+    CK(cudaGetLastError());
     return PD_OK;
 }
 
-void fast_release(pd_env *env) { (void)env; }
+template <class R>
+pd_status gate_if_needed(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
+    for (size_t b = 0; b < env->hb.size(); ++b) {
+        const HostBlock &hb = env->hb[b];
+        if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
+        k_fgate_partial<R><<<kGB, kGT, 0, env->st>>>(a, hb.first_int, hb.n, F.gpart.p, env->deformed.p + b);
+        k_fgate_final<<<1, 1, 0, env->st>>>(F.gpart.p, env->deformed.p + b);
+        note_launch();
+        note_launch();
+    }
+    return PD_OK;
+}
+
+template <class R>
+pd_status contacts_fast(pd_env *env, StepArgs<R> &a) {
+    for (size_t k = 0; k < env->hc.size(); ++k) {
+        const HostContact &hc = env->hc[k];
+        DevContact &dc = env->contacts[k];
+        if (!dc.has_neighs) continue;
+        CLawF law{hc.equi_dist, hc.exponent, hc.stiffness};
+        if (hc.kind == PD_CONTACT_12) {
+            k_fc12_1<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.rows, dc.nb.p, env->dens.p, law);
+            k_fc12_2<R><<<gridn(dc.n2, 256), 256, 0, env->st>>>(a, dc.first2, dc.n2, dc.rev_off.p, dc.rev.p,
+                                                                env->dens.p, law);
+            note_launch();
+            note_launch();
+        } else {
+            k_fc11<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nb.p, dc.rev_off.p, dc.rev.p,
+                                                             env->dens.p, law);
+            note_launch();
+        }
+    }
+    CK(cudaGetLastError());
+    return PD_OK;
+}
+
+bool any_lps(const pd_env *env) {
+    for (const auto &b : env->hb)
+        if (b.kind == PD_MAT_ORDINARY_STATE_BASED) return true;
+    return false;
+}
+
+template <class R>
+pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
+    cudaStream_t st = env->st;
+    const unsigned grid = gridn(env->N);
+    const bool lps = any_lps(env);
+    const bool contacts = !env->hc.empty();
+    {
+        StepArgs<R> a = args(env, F);
+        a.dir_pos = dir_bits(env);
+        k_prologue<R><<<grid, kT, 0, st>>>(a);
+        note_launch();
+        F.cur = 1 - F.cur;
+    }
+    for (int64_t s = 0; s < nsteps; ++s) {
+        const bool last = s == nsteps - 1;
+        StepArgs<R> a = args(env, F);
+        a.dir_vel = dir_bits(env);
+        // check!(env) then time_step += 1 (velocity_verlet.jl:81-85)
+        for (auto &h : env->hbc) {
+            if (h.kind != PD_BC_TOFRO) continue;
+            const double r = std::fmod((double)env->ts, h.freq);
+            if ((env->ts > h.applyafter) && (r == 0.0)) h.dir = -h.dir;
+        }
+        env->ts += 1;
+        a.dir_pos = dir_bits(env);
+        PD_TRY(gate_if_needed(env, a, F));
+        if (lps) {
+            k_theta<R><<<grid, kT, 0, st>>>(a);
+            note_launch();
+        }
+        prof_begin(env, st);
+        if (!contacts) {
+            if (last) k_step<R, 2><<<grid, kT, 0, st>>>(a);
+            else k_step<R, 1><<<grid, kT, 0, st>>>(a);
+            note_launch();
+            prof_end(env, st);
+        } else {
+            k_step<R, 0><<<grid, kT, 0, st>>>(a);
+            note_launch();
+            prof_end(env, st);
+            PD_TRY(contacts_fast(env, a));
+            if (last) k_step<R, 4><<<grid, kT, 0, st>>>(a);
+            else k_step<R, 3><<<grid, kT, 0, st>>>(a);
+            note_launch();
+        }
+        if (!last) F.cur = 1 - F.cur;
+        if ((s & 63) == 63) CK(cudaGetLastError());
+    }
+    CK(cudaGetLastError());
+    return PD_OK;
+}
+
+template <class R>
+pd_status update_acc_fast(pd_env *env, Fast<R> &F) {
+    StepArgs<R> a = args(env, F);
+    PD_TRY(gate_if_needed(env, a, F));
+    if (any_lps(env)) {
+        k_theta<R><<<gridn(env->N), kT, 0, env->st>>>(a);
+        note_launch();
+    }
+    prof_begin(env, env->st);
+    k_step<R, 0><<<gridn(env->N), kT, 0, env->st>>>(a);
+    note_launch();
+    prof_end(env, env->st);
+    PD_TRY(contacts_fast(env, a));
+    return PD_OK;
+}
+
+template <class R>
+pd_status export_fast(pd_env *env, Fast<R> &F) {
+    StepArgs<R> a = args(env, F);
+    k_export<R><<<gridn(env->N, 256), 256, 0, env->st>>>(env->N, env->x4.p, env->y.p, env->v.p, env->f.p, env->p.p,
+                                                         env->mth.p, a);
+    note_launch();
+    CK(cudaGetLastError());
+    return PD_OK;
+}
+
+pd_status ensure_fast(pd_env *env) {
+    if (env->hbc.size() > (size_t)kMaxFastBC)
+        return fail(PD_ERR_UNSUPPORTED, "the throughput modes support at most %d boundary conditions", kMaxFastBC);
+    if (!env->fast) {
+        FastHolder *h = new (std::nothrow) FastHolder();
+        if (!h) return fail(PD_ERR_OOM, "host allocation failed");
+        h->prec = env->precision;
+        env->fast = h;
+    }
+    FastHolder *h = holder(env);
+    if (!env->fast_valid) {
+        if (h->prec == PD_PREC_FP32C) PD_TRY(init_fast(env, h->f32));
+        else PD_TRY(init_fast(env, h->f64));
+        env->fast_valid = true;
+        h->dirty = false;
+    }
+    return PD_OK;
+}
+
+pd_status refresh_deformed_flags(pd_env *env) {
+    bool all = true;
+    for (size_t b = 0; b < env->hb.size(); ++b)
+        if (env->hb[b].kind != PD_MAT_SKIP && !env->deformed_h[b]) all = false;
+    if (all) return PD_OK;
+    std::vector<int32_t> h(env->hb.size());
+    CK(cudaMemcpyAsync(h.data(), env->deformed.p, h.size() * 4, cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    for (size_t b = 0; b < h.size(); ++b) env->deformed_h[b] = h[b];
+    return PD_OK;
+}
+
+}  // namespace
+
+pd_status sync_state_to_fp64(pd_env *env, bool invalidate) {
+    FastHolder *h = holder(env);
+    if (h && env->fast_valid && h->dirty) {
+        if (h->prec == PD_PREC_FP32C) PD_TRY(export_fast(env, h->f32));
+        else PD_TRY(export_fast(env, h->f64));
+        CK(cudaStreamSynchronize(env->st));
+        h->dirty = false;
+    }
+    if (invalidate) env->fast_valid = false;
+    return PD_OK;
+}
+
+void fast_release(pd_env *env) {
+    delete holder(env);
+    env->fast = nullptr;
+    env->fast_valid = false;
+}
 
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps) {
-    (void)env;
-    (void)nsteps;
-    return fail(PD_ERR_UNSUPPORTED, "throughput modes are not built yet");
+    if (nsteps == 0) return PD_OK;
+    PD_TRY(ensure_fast(env));
+    FastHolder *h = holder(env);
+    if (h->prec == PD_PREC_FP32C) PD_TRY(vv_chunk(env, h->f32, nsteps));
+    else PD_TRY(vv_chunk(env, h->f64, nsteps));
+    h->dirty = true;
+    PD_TRY(refresh_deformed_flags(env));
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
+}
+
+pd_status fast_update_acc(pd_env *env) {
+    PD_TRY(ensure_fast(env));
+    FastHolder *h = holder(env);
+    if (h->prec == PD_PREC_FP32C) PD_TRY(update_acc_fast(env, h->f32));
+    else PD_TRY(update_acc_fast(env, h->f64));
+    h->dirty = true;
+    PD_TRY(refresh_deformed_flags(env));
+    CK(cudaStreamSynchronize(env->st));
+    return PD_OK;
 }
 
 }  // namespace pd

@@ -209,6 +209,7 @@ pd_status refresh_deformed(pd_env *env) {
 extern "C" pd_status pd_env_update_acc(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
+    if (env->precision != PD_PREC_FP64_SERIAL) return fast_update_acc(env);
     PD_TRY(sync_state_to_fp64(env));
     PD_TRY(update_acc_serial(env));
     PD_TRY(refresh_deformed(env));
@@ -219,7 +220,7 @@ extern "C" pd_status pd_env_update_acc(pd_env *env) {
 extern "C" pd_status pd_env_apply_bc_at0(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
-    PD_TRY(sync_state_to_fp64(env));
+    PD_TRY(sync_state_to_fp64(env, false));
     for (size_t k = 0; k < env->hbc.size(); ++k) launch_bc_snapshot(env->st, bc_view(env, k), env->y.p);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(env->st));
@@ -306,7 +307,7 @@ extern "C" pd_status pd_env_qsdrag(pd_env *env, double step_size, double drag, i
 extern "C" pd_status pd_env_update_neighs(pd_env *env, int64_t max_part) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
-    PD_TRY(sync_state_to_fp64(env));
+    PD_TRY(sync_state_to_fp64(env, false));
     PD_TRY(contacts_update_neighs(env, max_part));
     CK(cudaStreamSynchronize(env->st));
     return PD_OK;

@@ -1,0 +1,151 @@
+"""Throughput modes (one-pass FP64, FP32-compensated) against the FP64
+oracle: relative-L2 error of displacement and velocity after N steps and the
+broken-bond mismatch.  Tolerances (stated per test):
+  FP64 one-pass: rel-L2 <= 1e-10 (summation order differs from the serial loop)
+  FP32C:         rel-L2 <= 1e-4  (the acceptance bound for the FP32 path)
+"""
+import numpy as np
+import pytest
+
+import peridyn_b200 as pb
+from peridyn_b200 import configs, lattice
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32c": 1e-4}
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _run_pair(oracle, w, precision, nsteps, bc0=True):
+    env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    if bc0:
+        ora.apply_bc_at0()
+        pb.apply_bc_at0(env, 0)
+    for _ in range(nsteps):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=nsteps)
+    return env, ora
+
+
+def _errors(env, ora):
+    y, v, f, p = env.get_state()
+    x = np.hstack([B.x for B in ora.blocks])
+    eu = rel_l2(y - x, ora.y - x)
+    ev = rel_l2(v, ora.v)
+    mism = 0
+    for b, B in enumerate(ora.blocks):
+        _, intact = env._family(b)
+        mism += int((intact != B.intact.astype(bool)).sum())
+    return eu, ev, mism
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("builder,nsteps", [
+    (lambda: configs.pmb_cube(n=12, peak=20.0), 200),
+    (lambda: configs.lps_bar(nx=40, ny=10, nz=10), 300),
+])
+def test_trajectory_error_bound(oracle, precision, builder, nsteps):
+    w = builder()
+    env, ora = _run_pair(oracle, w, precision, nsteps)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= TOL[precision], f"displacement rel-L2 {eu:.3e}"
+    assert ev <= TOL[precision], f"velocity rel-L2 {ev:.3e}"
+    assert mism == 0
+    assert env.time_step == nsteps
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_breaking_mismatch_is_small(oracle, precision):
+    w = configs.pmb_cube(n=12, peak=400.0, cs=0.002)
+    env, ora = _run_pair(oracle, w, precision, 80, bc0=False)
+    eu, ev, mism = _errors(env, ora)
+    nbroken = int((ora.blocks[0].family > 0).sum() - ora.blocks[0].intact.sum())
+    assert nbroken > 100
+    # bonds whose stretch sits within rounding of cs may differ
+    assert mism <= max(2, nbroken // 200), f"{mism} of {nbroken} broken bonds differ"
+    assert eu <= (1e-8 if precision == "fp64" else 1e-3)
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_multitype_and_tofro(oracle, precision):
+    x, vol = lattice.cuboid(14, 6, 6, 1e-3, jitter=1e-5, seed=4)
+    t = np.where(x[0] < x[0].mean(), 1, 2).astype(np.int64)
+    gen = pb.GeneralMaterial(x.copy(order="F"), np.zeros_like(x, order="F"), x, vol, t, 3.015e-3, max_neigh=200)
+    spc = pb.OrdinaryStateBasedSpecific([20e9, 25e9, 30e9], [9e9, 10e9, 12e9], [0.05, 0.05, 0.05], [2000.0, 2500.0])
+    mat = pb.PeridynamicsMaterial(gen, spc)
+    bcs = [pb.FixBC(x[0] < 2e-3), pb.ToFroBC(x[0] > 12e-3, [2.0, 0.3, 0.0], 40, applyafter=10)]
+    w = {"materials": [mat], "contacts": [], "bcs": bcs, "dt": 2e-8}
+    env, ora = _run_pair(oracle, w, precision, 150)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= TOL[precision] and ev <= TOL[precision] and mism == 0
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_chunked_equals_single_run(precision):
+    w = configs.lps_bar(nx=30, ny=8, nz=8)
+    e1 = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+    e2 = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+    for e in (e1, e2):
+        pb.apply_bc_at0(e, 0)
+    pb.velocity_verlet_step(e1, nsteps=60)
+    for _ in range(6):
+        pb.velocity_verlet_step(e2, nsteps=10)
+        e2.get_state()  # reads do not perturb the device state
+    s1, s2 = e1.get_state(), e2.get_state()
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    e1.close()
+    e2.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_contact_impact_fast(oracle, precision):
+    w = configs.disk_impact(radius=2.0e-3, thickness=1.0e-3, spacing=2.5e-4, sphere_radius=0.75e-3, speed=150.0,
+                            cs=0.003)
+    env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    ora.update_acc()
+    pb.update_acc(env)
+    for _ in range(60):
+        ora.update_neighs()
+        pb.update_neighs(env)
+        ora.vv_step()
+        pb.velocity_verlet_step(env)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= (1e-9 if precision == "fp64" else 2e-4), eu
+    assert mism == 0
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_rigid_gate_fast(precision):
+    w = configs.pmb_cube(n=8, peak=0.0)
+    w["materials"][0].general.velocity[0] = 3.0
+    env = pb.Env(1, w["materials"], [], [], w["dt"], precision=precision)
+    pb.velocity_verlet_step(env, nsteps=10)
+    assert not env.deformed()[0]
+    assert np.all(env.f == 0.0)
+    env.close()
+
+
+def test_update_acc_fast_matches_oracle(oracle):
+    w = configs.lps_bar(nx=24, ny=7, nz=6)
+    for precision, tol in (("fp64", 1e-12), ("fp32c", 2e-4)):
+        env = pb.Env(1, w["materials"], [], [], w["dt"], precision=precision)
+        ora = oracle.OracleEnv(w["materials"], [], [], w["dt"])
+        rng = np.random.default_rng(2)
+        y = ora.y + rng.normal(0.0, 1e-6, size=ora.y.shape)
+        ora.y[:] = y
+        env.set_state(y=y)
+        ora.update_acc()
+        pb.update_acc(env)
+        assert rel_l2(env.f, ora.f) <= tol
+        assert np.allclose(env.theta(0), ora.blocks[0].theta, rtol=tol, atol=tol * np.abs(ora.blocks[0].theta).max())
+        env.close()
