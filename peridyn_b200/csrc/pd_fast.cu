@@ -22,6 +22,10 @@
 //   f_p += (t / (2|Y|)) V_q Y  ... scaled by 1/rho_p once per particle.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "pd_env_impl.h"
@@ -105,12 +109,29 @@ __device__ __forceinline__ int64_t lower_bound_i32(const int32_t *a, int64_t n, 
 
 __device__ __forceinline__ double &cmp(double4 &a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 
-// Gather of p's bonds.  Returns the acceleration before the 1/rho scaling.
-template <class R, int KIND, bool kBreak>
-__device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, const FBlock<R> &B, int tp,
+// Work split of a 32-particle slice over WPS warps: warp w handles the
+// chunks c = w, w + WPS, ... of CS consecutive bonds of every particle of
+// the slice (CS = 32 -- one intact word -- for WPS <= 4, 16 for WPS = 8).
+// Partial sums are combined in a fixed order, so results do not depend on
+// scheduling.
+template <int WPS>
+struct Split {
+    static constexpr int CS = WPS <= 4 ? 32 : 16;
+    static constexpr int BT = WPS <= 4 ? 128 : 256;  // threads per block
+    static constexpr int NW = BT / 32;                // warps per block
+    static constexpr int SPB = NW / WPS;              // slices per block
+};
+
+// Gather of p's bonds in the chunks owned by warp w.  Returns the
+// acceleration before the 1/rho scaling.  Every bond appears in both
+// endpoint families and the serial loop adds its term to f_p from both
+// visits, hence the factor 2 (t/|Y| rather than t/(2|Y|)).
+template <class R, int KIND, bool kBreak, int WPS>
+__device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
                                             typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
                                             R &fz) {
     using V4 = typename Tr<R>::V4;
+    constexpr int CS = Split<WPS>::CS;
     const int32_t n = a.cnt[p];
     const int64_t sp = a.slice_ptr[p >> 5];
     const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
@@ -121,9 +142,11 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, con
         Bp = m.y;
     }
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
-    for (int32_t w0 = 0; w0 < n; w0 += 32) {
-        const uint32_t w = a.words[wb + 32 * (int64_t)(w0 >> 5)];
-        uint32_t m = w, nw = w;
+    for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
+        const int64_t widx = wb + 32 * (int64_t)(w0 >> 5);
+        const uint32_t word = a.words[widx];
+        uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+        uint32_t brk = 0;
         while (m) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
@@ -142,7 +165,7 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, con
             const R dl = (ly + lx) * lx;
             if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             if (!(num < pp.cs * dl)) {
-                if (kBreak) nw &= ~(1u << j);
+                if (kBreak) brk |= 1u << j;
                 continue;
             }
             const R s = Tr<R>::div(num, dl);
@@ -153,12 +176,13 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, con
                 typename Tr<R>::V2 mq = a.mab[q];
                 t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
             }
-            const R coef = R(0.5) * t * ry * xq.w;
+            const R coef = t * ry * xq.w;
             fx += coef * Y0;
             fy += coef * Y1;
             fz += coef * Y2;
         }
-        if (kBreak && nw != w) a.words[wb + 32 * (int64_t)(w0 >> 5)] = nw;
+        // bonds break rarely; two warps may own the halves of one word
+        if (kBreak && brk) atomicAnd(&a.words[widx], ~(CS == 32 ? brk : (brk << (w0 & 31))));
     }
 }
 
@@ -242,36 +266,73 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 // MODE 2: full step, last of the chunk: f, p, kick, BC vel, store v and f.
 // MODE 3: integration only (forces already in f, e.g. after contacts).
 // MODE 4: integration only, last of the chunk.
+// MODE 5: force only into a scratch array, no bond breaking (autotuning).
 template <class R, int MODE>
-__global__ void __launch_bounds__(kT) k_step(StepArgs<R> a) {
+__device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
+
+template <class R, int WPS, int MODE>
+__global__ void __launch_bounds__(Split<WPS>::BT) k_step(StepArgs<R> a) {
     using V4 = typename Tr<R>::V4;
-    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
-    if (p >= a.N) return;
-    const int32_t ti = a.tinfo[p];
-    if (ti < 0) {
-        if (MODE == 1 || MODE == 3) a.unext[p] = V4{};
-        return;
-    }
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][3][32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = wid % WPS;
+    const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     R fx = 0, fy = 0, fz = 0;
-    if (MODE <= 2) {
+    if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
         const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             const V4 xp = a.x[p], up = a.ucur[p];
             if (B.kind == PD_MAT_BOND_BASED)
-                bond_gather<R, PD_MAT_BOND_BASED, true>(a, p, B, tp, xp, up, fx, fy, fz);
+                bond_gather<R, PD_MAT_BOND_BASED, MODE != 5, WPS>(a, p, w, B, tp, xp, up, fx, fy, fz);
             else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, true>(a, p, B, tp, xp, up, fx, fy, fz);
-            const R ir = a.irho[p];
-            fx *= ir;
-            fy *= ir;
-            fz *= ir;
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, MODE != 5, WPS>(a, p, w, B, tp, xp, up, fx, fy, fz);
         }
-    } else {
-        const V4 ff = a.f[p];
-        fx = ff.x;
-        fy = ff.y;
-        fz = ff.z;
+    }
+    if (WPS > 1) {
+        sh[wid][0][lane] = fx;
+        sh[wid][1][lane] = fy;
+        sh[wid][2][lane] = fz;
+        __syncthreads();
+        if (w != 0) return;
+        fx = fy = fz = 0;
+        for (int k = 0; k < WPS; ++k) {
+            fx += sh[wid + k][0][lane];
+            fy += sh[wid + k][1][lane];
+            fz += sh[wid + k][2][lane];
+        }
+    }
+    if (p >= a.N) return;
+    if (ti < 0) {
+        if (MODE == 1) a.unext[p] = V4{};
+        return;
+    }
+    const R ir = a.irho[p];
+    integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
+}
+
+// MODE 3/4: integration of forces already in f (after contact forces).
+template <class R, int MODE>
+__global__ void __launch_bounds__(kT) k_integrate(StepArgs<R> a) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
+    if (p >= a.N) return;
+    if (a.tinfo[p] < 0) {
+        if (MODE == 3) a.unext[p] = V4{};
+        return;
+    }
+    const V4 ff = a.f[p];
+    integrate<R, MODE>(a, p, ff.x, ff.y, ff.z);
+}
+
+template <class R, int MODE>
+__device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz) {
+    using V4 = typename Tr<R>::V4;
+    if (MODE == 5) {
+        a.f[p] = V4{fx, fy, fz, R(0)};
+        return;
     }
     V4 vp = a.v[p];
     if (MODE == 0) {
@@ -329,27 +390,30 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
 }
 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
-// bonds; stores theta_p/m_p for the force pass.
-template <class R>
-__global__ void __launch_bounds__(kT) k_theta(StepArgs<R> a) {
+// bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
+template <class R, int WPS>
+__global__ void __launch_bounds__(Split<WPS>::BT) k_theta(StepArgs<R> a) {
     using V4 = typename Tr<R>::V4;
-    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
-    if (p >= a.N) return;
-    const int32_t ti = a.tinfo[p];
-    if (ti < 0) return;
-    const FBlock<R> B = a.fb[ti >> 8];
-    if (B.kind != PD_MAT_ORDINARY_STATE_BASED) return;
-    const V4 xp = a.x[p], up = a.ucur[p];
-    const int32_t n = a.cnt[p];
-    const int64_t sp = a.slice_ptr[p >> 5];
-    const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB, CS = Split<WPS>::CS;
+    __shared__ R sh[WPS > 1 ? NW : 1][32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = wid % WPS;
+    const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    const int32_t ti = p < a.N ? a.tinfo[p] : -1;
+    const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
-    for (int32_t w0 = 0; w0 < n; w0 += 32) {
-        uint32_t m = a.words[wb + 32 * (int64_t)(w0 >> 5)];
-        while (m) {
-            const int j = __ffs(m) - 1;
-            m &= m - 1;
-            const int32_t q = a.nbr[base + 32 * (int64_t)(w0 + j)];
+    if (lps) {
+        const V4 xp = a.x[p], up = a.ucur[p];
+        const int32_t n = a.cnt[p];
+        const int64_t sp = a.slice_ptr[p >> 5];
+        const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+        for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
+            const uint32_t word = a.words[wb + 32 * (int64_t)(w0 >> 5)];
+            uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+            while (m) {
+                const int j = __ffs(m) - 1;
+                m &= m - 1;
+                const int32_t q = a.nbr[base + 32 * (int64_t)(w0 + j)];
             const V4 xq = a.x[q], uq = a.ucur[q];
             const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
             const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
@@ -358,9 +422,18 @@ __global__ void __launch_bounds__(kT) k_theta(StepArgs<R> a) {
             const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
             const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
             const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
-            acc += Tr<R>::div(num, ly + lx) * xq.w;
+                acc += Tr<R>::div(num, ly + lx) * xq.w;
+            }
         }
     }
+    if (WPS > 1) {
+        sh[wid][lane] = acc;
+        __syncthreads();
+        if (w != 0) return;
+        acc = 0;
+        for (int k = 0; k < WPS; ++k) acc += sh[wid + k][lane];
+    }
+    if (!lps) return;
     typename Tr<R>::V2 mb = a.mab[p];
     mb.x = R(3) * acc * mb.y * mb.y;  // theta/m = (3/m) acc / m
     a.mab[p] = mb;
@@ -604,8 +677,35 @@ struct Fast {
     DBuf<FPair<R>> fp;
     DBuf<uint8_t> bcbits;
     DBuf<double> gpart;
+    DBuf<V4> tune;        // autotuner output scratch
+    DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     int cur = 0;
+    int wps = 0;          // warps per 32-particle slice (autotuned)
 };
+
+template <class R, int MODE>
+void launch_step(cudaStream_t st, int wps, const StepArgs<R> &a) {
+    const int64_t slices = (a.N + 31) / 32;
+    switch (wps) {
+        case 1: k_step<R, 1, MODE><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_step<R, 2, MODE><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_step<R, 4, MODE><<<(unsigned)slices, 128, 0, st>>>(a); break;
+        default: k_step<R, 8, MODE><<<(unsigned)slices, 256, 0, st>>>(a); break;
+    }
+    note_launch();
+}
+
+template <class R>
+void launch_theta(cudaStream_t st, int wps, const StepArgs<R> &a) {
+    const int64_t slices = (a.N + 31) / 32;
+    switch (wps) {
+        case 1: k_theta<R, 1><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_theta<R, 2><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_theta<R, 4><<<(unsigned)slices, 128, 0, st>>>(a); break;
+        default: k_theta<R, 8><<<(unsigned)slices, 256, 0, st>>>(a); break;
+    }
+    note_launch();
+}
 
 struct FastHolder {
     int prec = 0;
@@ -767,12 +867,87 @@ bool any_lps(const pd_env *env) {
     return false;
 }
 
+// Project autotuner: times the force (and dilatation) kernels for every
+// warps-per-slice split on the environment itself -- force written to a
+// scratch array, no bond breaking, every block treated as deformed -- and
+// keeps the fastest.  Results are cached per (particles, bonds, precision,
+// state-based) for the life of the process.
+std::mutex g_tune_mutex;
+std::map<std::tuple<int64_t, int64_t, int, bool>, int> g_tune_cache;
+
+template <class R>
+pd_status autotune(pd_env *env, Fast<R> &F) {
+    if (F.wps) return PD_OK;
+    const bool lps = any_lps(env);
+    const auto key = std::make_tuple(env->N, env->nnz, env->precision, lps);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            F.wps = it->second;
+            return PD_OK;
+        }
+    }
+    if (const char *fixed = std::getenv("PD_WPS")) {
+        const int w = std::atoi(fixed);
+        if (w == 1 || w == 2 || w == 4 || w == 8) {
+            F.wps = w;
+            return PD_OK;
+        }
+    }
+    PD_TRY(F.tune.alloc(env->N));
+    std::vector<int32_t> ones(env->hb.size(), 1);
+    PD_TRY(F.ones.alloc(ones.size()));
+    CK(cudaMemcpyAsync(F.ones.p, ones.data(), ones.size() * 4, cudaMemcpyHostToDevice, env->st));
+    StepArgs<R> a = args(env, F);
+    a.f = F.tune.p;
+    a.p = F.tune.p;
+    a.deformed = F.ones.p;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_w = 4;
+    for (int w : {1, 2, 4, 8}) {
+        if (lps) launch_theta(env->st, w, a);
+        launch_step<R, 5>(env->st, w, a);
+        cudaEventRecord(e0, env->st);
+        for (int r = 0; r < 3; ++r) {
+            if (lps) launch_theta(env->st, w, a);
+            launch_step<R, 5>(env->st, w, a);
+        }
+        cudaEventRecord(e1, env->st);
+        cudaError_t err = cudaEventSynchronize(e1);
+        if (err != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return cuda_fail(err, "autotune", __FILE__, __LINE__);
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_w = w;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    F.tune.reset();
+    F.wps = best_w;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best_w;
+    return PD_OK;
+}
+
 template <class R>
 pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
     cudaStream_t st = env->st;
     const unsigned grid = gridn(env->N);
     const bool lps = any_lps(env);
     const bool contacts = !env->hc.empty();
+    PD_TRY(autotune(env, F));
+    const int wps = F.wps;
     {
         StepArgs<R> a = args(env, F);
         a.dir_pos = dir_bits(env);
@@ -793,23 +968,18 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
         env->ts += 1;
         a.dir_pos = dir_bits(env);
         PD_TRY(gate_if_needed(env, a, F));
-        if (lps) {
-            k_theta<R><<<grid, kT, 0, st>>>(a);
-            note_launch();
-        }
+        if (lps) launch_theta(st, wps, a);
         prof_begin(env, st);
         if (!contacts) {
-            if (last) k_step<R, 2><<<grid, kT, 0, st>>>(a);
-            else k_step<R, 1><<<grid, kT, 0, st>>>(a);
-            note_launch();
+            if (last) launch_step<R, 2>(st, wps, a);
+            else launch_step<R, 1>(st, wps, a);
             prof_end(env, st);
         } else {
-            k_step<R, 0><<<grid, kT, 0, st>>>(a);
-            note_launch();
+            launch_step<R, 0>(st, wps, a);
             prof_end(env, st);
             PD_TRY(contacts_fast(env, a));
-            if (last) k_step<R, 4><<<grid, kT, 0, st>>>(a);
-            else k_step<R, 3><<<grid, kT, 0, st>>>(a);
+            if (last) k_integrate<R, 4><<<grid, kT, 0, st>>>(a);
+            else k_integrate<R, 3><<<grid, kT, 0, st>>>(a);
             note_launch();
         }
         if (!last) F.cur = 1 - F.cur;
@@ -821,15 +991,12 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
 
 template <class R>
 pd_status update_acc_fast(pd_env *env, Fast<R> &F) {
+    PD_TRY(autotune(env, F));
     StepArgs<R> a = args(env, F);
     PD_TRY(gate_if_needed(env, a, F));
-    if (any_lps(env)) {
-        k_theta<R><<<gridn(env->N), kT, 0, env->st>>>(a);
-        note_launch();
-    }
+    if (any_lps(env)) launch_theta(env->st, F.wps, a);
     prof_begin(env, env->st);
-    k_step<R, 0><<<gridn(env->N), kT, 0, env->st>>>(a);
-    note_launch();
+    launch_step<R, 0>(env->st, F.wps, a);
     prof_end(env, env->st);
     PD_TRY(contacts_fast(env, a));
     return PD_OK;
