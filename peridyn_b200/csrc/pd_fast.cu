@@ -147,39 +147,55 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         const uint32_t word = a.words[widx];
         uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
         uint32_t brk = 0;
+        // U bonds in flight per thread: their index and neighbour loads are
+        // issued before any of them is used (memory-level parallelism).
+        constexpr int U = sizeof(R) == 4 ? 4 : 2;
         while (m) {
-            const int j = __ffs(m) - 1;
-            m &= m - 1;
-            const int32_t k = w0 + j;
-            const int32_t q = a.nbr[base + 32 * (int64_t)k];
-            const V4 xq = a.x[q];
-            const V4 uq = a.ucur[q];
-            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
-            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
-            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
-            const R lx = xx2 * rx, ly = yy2 * ry;
-            const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
-            const R dl = (ly + lx) * lx;
-            if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
-            if (!(num < pp.cs * dl)) {
-                if (kBreak) brk |= 1u << j;
-                continue;
+            int j[U];
+            int32_t q[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                j[u] = m ? __ffs(m) - 1 : -1;
+                m &= m - 1;
             }
-            const R s = Tr<R>::div(num, dl);
-            R t;
-            if (KIND == PD_MAT_BOND_BASED) {
-                t = B.c11 * s;
-            } else {
-                typename Tr<R>::V2 mq = a.mab[q];
-                t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
+#pragma unroll
+            for (int u = 0; u < U; ++u) q[u] = j[u] >= 0 ? a.nbr[base + 32 * (int64_t)(w0 + j[u])] : (int32_t)p;
+            V4 xq[U], uq[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                xq[u] = a.x[q[u]];
+                uq[u] = a.ucur[q[u]];
             }
-            const R coef = t * ry * xq.w;
-            fx += coef * Y0;
-            fy += coef * Y1;
-            fz += coef * Y2;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (j[u] < 0) continue;
+                const R x0 = xq[u].x - xp.x, x1 = xq[u].y - xp.y, x2 = xq[u].z - xp.z;
+                const R e0 = uq[u].x - up.x, e1 = uq[u].y - up.y, e2 = uq[u].z - up.z;
+                const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+                const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+                const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+                const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
+                const R lx = xx2 * rx, ly = yy2 * ry;
+                const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
+                const R dl = (ly + lx) * lx;
+                if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q[u]] & 255) * B.nt];
+                if (!(num < pp.cs * dl)) {
+                    if (kBreak) brk |= 1u << j[u];
+                    continue;
+                }
+                const R s = Tr<R>::div(num, dl);
+                R t;
+                if (KIND == PD_MAT_BOND_BASED) {
+                    t = B.c11 * s;
+                } else {
+                    typename Tr<R>::V2 mq = a.mab[q[u]];
+                    t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
+                }
+                const R coef = t * ry * xq[u].w;
+                fx += coef * Y0;
+                fy += coef * Y1;
+                fz += coef * Y2;
+            }
         }
         // bonds break rarely; two warps may own the halves of one word
         if (kBreak && brk) atomicAnd(&a.words[widx], ~(CS == 32 ? brk : (brk << (w0 & 31))));
@@ -410,19 +426,35 @@ __global__ void __launch_bounds__(Split<WPS>::BT) k_theta(StepArgs<R> a) {
         for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
             const uint32_t word = a.words[wb + 32 * (int64_t)(w0 >> 5)];
             uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+            constexpr int U = sizeof(R) == 4 ? 4 : 2;
             while (m) {
-                const int j = __ffs(m) - 1;
-                m &= m - 1;
-                const int32_t q = a.nbr[base + 32 * (int64_t)(w0 + j)];
-            const V4 xq = a.x[q], uq = a.ucur[q];
-            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
-            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
-            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
-            const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
-                acc += Tr<R>::div(num, ly + lx) * xq.w;
+                int j[U];
+                int32_t q[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    j[u] = m ? __ffs(m) - 1 : -1;
+                    m &= m - 1;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) q[u] = j[u] >= 0 ? a.nbr[base + 32 * (int64_t)(w0 + j[u])] : (int32_t)p;
+                V4 xq[U], uq[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    xq[u] = a.x[q[u]];
+                    uq[u] = a.ucur[q[u]];
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (j[u] < 0) continue;
+                    const R x0 = xq[u].x - xp.x, x1 = xq[u].y - xp.y, x2 = xq[u].z - xp.z;
+                    const R e0 = uq[u].x - up.x, e1 = uq[u].y - up.y, e2 = uq[u].z - up.z;
+                    const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+                    const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+                    const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+                    const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
+                    const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
+                    acc += Tr<R>::div(num, ly + lx) * xq[u].w;
+                }
             }
         }
     }
