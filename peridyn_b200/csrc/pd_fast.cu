@@ -22,6 +22,7 @@
 //   f_p += (t / (2|Y|)) V_q Y  ... scaled by 1/rho_p once per particle.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -120,13 +121,43 @@ struct Split {
     static constexpr int BT = WPS <= 4 ? 128 : 256;  // threads per block
     static constexpr int NW = BT / 32;                // warps per block
     static constexpr int SPB = NW / WPS;              // slices per block
+    static constexpr int MINB = 1024 / BT;            // resident blocks per SM aimed for (<= 64 registers)
 };
+
+// Combine the WPS partial sums of one slice without a block barrier: each
+// warp publishes its partials, and the last warp of the slice to arrive
+// adds them in warp order (fixed, so the result does not depend on which
+// warp arrives last) and continues with the particle update.  Returns
+// true in the lanes of that warp.
+template <int WPS, int NC, class R>
+__device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, int wid, int lane, R *v) {
+    const int w = wid % WPS, sl = wid / WPS;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) sh[wid][c][lane] = v[c];
+    __syncwarp();
+    int old = 0;
+    if (lane == 0) {
+        __threadfence_block();
+        old = atomicAdd(&arrive[sl], 1);
+    }
+    old = __shfl_sync(0xffffffffu, old, 0);
+    if (old != WPS - 1) return false;
+    __threadfence_block();
+    const int w0 = wid - w;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        R s = 0;
+        for (int k = 0; k < WPS; ++k) s += sh[w0 + k][c][lane];
+        v[c] = s;
+    }
+    return true;
+}
 
 // Gather of p's bonds in the chunks owned by warp w.  Returns the
 // acceleration before the 1/rho scaling.  Every bond appears in both
 // endpoint families and the serial loop adds its term to f_p from both
 // visits, hence the factor 2 (t/|Y| rather than t/(2|Y|)).
-template <class R, int KIND, bool kBreak, int WPS>
+template <class R, int KIND, bool kBreak, int WPS, int U>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
                                             typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
                                             R &fz) {
@@ -149,7 +180,6 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         uint32_t brk = 0;
         // U bonds in flight per thread: their index and neighbour loads are
         // issued before any of them is used (memory-level parallelism).
-        constexpr int U = sizeof(R) == 4 ? 4 : 2;
         while (m) {
             int j[U];
             int32_t q[U];
@@ -286,40 +316,35 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 template <class R, int MODE>
 __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
 
-template <class R, int WPS, int MODE>
-__global__ void __launch_bounds__(Split<WPS>::BT) k_step(StepArgs<R> a) {
+template <class R, int WPS, int U, int MODE>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_step(StepArgs<R> a) {
     using V4 = typename Tr<R>::V4;
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
+    __shared__ int arrive[SPB];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
-    R fx = 0, fy = 0, fz = 0;
+    R f[3] = {0, 0, 0};
     if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
         const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             const V4 xp = a.x[p], up = a.ucur[p];
             if (B.kind == PD_MAT_BOND_BASED)
-                bond_gather<R, PD_MAT_BOND_BASED, MODE != 5, WPS>(a, p, w, B, tp, xp, up, fx, fy, fz);
+                bond_gather<R, PD_MAT_BOND_BASED, MODE != 5, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
             else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, MODE != 5, WPS>(a, p, w, B, tp, xp, up, fx, fy, fz);
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, MODE != 5, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1],
+                                                                             f[2]);
         }
     }
-    if (WPS > 1) {
-        sh[wid][0][lane] = fx;
-        sh[wid][1][lane] = fy;
-        sh[wid][2][lane] = fz;
-        __syncthreads();
-        if (w != 0) return;
-        fx = fy = fz = 0;
-        for (int k = 0; k < WPS; ++k) {
-            fx += sh[wid + k][0][lane];
-            fy += sh[wid + k][1][lane];
-            fz += sh[wid + k][2][lane];
-        }
-    }
+    if (WPS > 1 && !last_arrival_sum<WPS, 3>(sh, arrive, wid, lane, f)) return;
+    const R fx = f[0], fy = f[1], fz = f[2];
     if (p >= a.N) return;
     if (ti < 0) {
         if (MODE == 1) a.unext[p] = V4{};
@@ -407,13 +432,18 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
-template <class R, int WPS>
-__global__ void __launch_bounds__(Split<WPS>::BT) k_theta(StepArgs<R> a) {
+template <class R, int WPS, int U>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_theta(StepArgs<R> a) {
     using V4 = typename Tr<R>::V4;
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB, CS = Split<WPS>::CS;
-    __shared__ R sh[WPS > 1 ? NW : 1][32];
+    __shared__ R sh[WPS > 1 ? NW : 1][1][32];
+    __shared__ int arrive[SPB];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
@@ -426,7 +456,6 @@ __global__ void __launch_bounds__(Split<WPS>::BT) k_theta(StepArgs<R> a) {
         for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
             const uint32_t word = a.words[wb + 32 * (int64_t)(w0 >> 5)];
             uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
-            constexpr int U = sizeof(R) == 4 ? 4 : 2;
             while (m) {
                 int j[U];
                 int32_t q[U];
@@ -458,13 +487,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT) k_theta(StepArgs<R> a) {
             }
         }
     }
-    if (WPS > 1) {
-        sh[wid][lane] = acc;
-        __syncthreads();
-        if (w != 0) return;
-        acc = 0;
-        for (int k = 0; k < WPS; ++k) acc += sh[wid + k][lane];
-    }
+    if (WPS > 1 && !last_arrival_sum<WPS, 1>(sh, arrive, wid, lane, &acc)) return;
     if (!lps) return;
     typename Tr<R>::V2 mb = a.mab[p];
     mb.x = R(3) * acc * mb.y * mb.y;  // theta/m = (3/m) acc / m
@@ -715,28 +738,48 @@ struct Fast {
     int wps = 0;          // warps per 32-particle slice (autotuned)
 };
 
-template <class R, int MODE>
-void launch_step(cudaStream_t st, int wps, const StepArgs<R> &a) {
+// Kernel shape, chosen by the autotuner: cfg = 10 * WPS + U (warps per
+// slice, bonds in flight per thread).  FP32 tries U in {2, 4}, FP64 {1, 2}.
+template <class R>
+struct Unroll {
+    static constexpr int LO = sizeof(R) == 4 ? 2 : 1;
+    static constexpr int HI = sizeof(R) == 4 ? 4 : 2;
+};
+
+template <class R, int MODE, int U>
+void launch_step_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
     switch (wps) {
-        case 1: k_step<R, 1, MODE><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_step<R, 2, MODE><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_step<R, 4, MODE><<<(unsigned)slices, 128, 0, st>>>(a); break;
-        default: k_step<R, 8, MODE><<<(unsigned)slices, 256, 0, st>>>(a); break;
+        case 1: k_step<R, 1, U, MODE><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_step<R, 2, U, MODE><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_step<R, 4, U, MODE><<<(unsigned)slices, 128, 0, st>>>(a); break;
+        default: k_step<R, 8, U, MODE><<<(unsigned)slices, 256, 0, st>>>(a); break;
+    }
+    note_launch();
+}
+
+template <class R, int MODE>
+void launch_step(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    if (cfg % 10 == Unroll<R>::LO) launch_step_u<R, MODE, Unroll<R>::LO>(st, cfg / 10, a);
+    else launch_step_u<R, MODE, Unroll<R>::HI>(st, cfg / 10, a);
+}
+
+template <class R, int U>
+void launch_theta_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
+    const int64_t slices = (a.N + 31) / 32;
+    switch (wps) {
+        case 1: k_theta<R, 1, U><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_theta<R, 2, U><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_theta<R, 4, U><<<(unsigned)slices, 128, 0, st>>>(a); break;
+        default: k_theta<R, 8, U><<<(unsigned)slices, 256, 0, st>>>(a); break;
     }
     note_launch();
 }
 
 template <class R>
-void launch_theta(cudaStream_t st, int wps, const StepArgs<R> &a) {
-    const int64_t slices = (a.N + 31) / 32;
-    switch (wps) {
-        case 1: k_theta<R, 1><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_theta<R, 2><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_theta<R, 4><<<(unsigned)slices, 128, 0, st>>>(a); break;
-        default: k_theta<R, 8><<<(unsigned)slices, 256, 0, st>>>(a); break;
-    }
-    note_launch();
+void launch_theta(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    if (cfg % 10 == Unroll<R>::LO) launch_theta_u<R, Unroll<R>::LO>(st, cfg / 10, a);
+    else launch_theta_u<R, Unroll<R>::HI>(st, cfg / 10, a);
 }
 
 struct FastHolder {
@@ -920,10 +963,11 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
             return PD_OK;
         }
     }
-    if (const char *fixed = std::getenv("PD_WPS")) {
-        const int w = std::atoi(fixed);
-        if (w == 1 || w == 2 || w == 4 || w == 8) {
-            F.wps = w;
+    if (const char *fixed = std::getenv("PD_KERNEL_SHAPE")) {  // "WPS,U" overrides the tuner
+        int w = 0, u = 0;
+        if (std::sscanf(fixed, "%d,%d", &w, &u) == 2 && (w == 1 || w == 2 || w == 4 || w == 8) &&
+            (u == Unroll<R>::LO || u == Unroll<R>::HI)) {
+            F.wps = 10 * w + u;
             return PD_OK;
         }
     }
@@ -939,8 +983,11 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_w = 4;
-    for (int w : {1, 2, 4, 8}) {
+    int best_w = 40 + Unroll<R>::LO;
+    std::vector<int> shapes;
+    for (int wps : {1, 2, 4, 8})
+        for (int u : {Unroll<R>::LO, Unroll<R>::HI}) shapes.push_back(10 * wps + u);
+    for (int w : shapes) {
         if (lps) launch_theta(env->st, w, a);
         launch_step<R, 5>(env->st, w, a);
         cudaEventRecord(e0, env->st);
