@@ -259,6 +259,7 @@ def main():
     def reset():
         env.set_state(y=y0, v=v0, f=np.zeros_like(y0))
         _abi.check(L.pd_env_reset_bonds(env._h))
+        _abi.check(L.pd_env_reset_deformed(env._h))
         env.time_step = 0
         if work["bcs"]:
             pb.apply_bc_at0(env, 0)
@@ -318,6 +319,7 @@ def main():
     e2e_times = []
     for _ in range(args.steps):
         _abi.check(L.pd_env_reset_bonds(env._h))
+        _abi.check(L.pd_env_reset_deformed(env._h))
         env.time_step = 0
         flush.zero_()
         torch.cuda.synchronize()

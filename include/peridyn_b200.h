@@ -177,6 +177,9 @@ PD_API pd_status pd_env_get_time_step(const pd_env *env, int64_t *time_step);
 PD_API pd_status pd_env_set_time_step(pd_env *env, int64_t time_step);
 /* Reset every intact flag to the state right after finalize. */
 PD_API pd_status pd_env_reset_bonds(pd_env *env);
+/* Reset the per-block "deformed" flags (general_material.jl:54, set when a
+ * block first leaves rigid motion) to their state right after finalize. */
+PD_API pd_status pd_env_reset_deformed(pd_env *env);
 
 /* ---------------------------------------------------------------------- */
 /* Solver entry points                                                     */

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "pd_env_get_time_step": (ctypes.c_int32, [c_vp, c_i64p]),
     "pd_env_set_time_step": (ctypes.c_int32, [c_vp, ctypes.c_int64]),
     "pd_env_reset_bonds": (ctypes.c_int32, [c_vp]),
+    "pd_env_reset_deformed": (ctypes.c_int32, [c_vp]),
     "pd_env_apply_bc_at0": (ctypes.c_int32, [c_vp]),
     "pd_env_update_acc": (ctypes.c_int32, [c_vp]),
     "pd_env_vv_steps": (ctypes.c_int32, [c_vp, ctypes.c_int64]),

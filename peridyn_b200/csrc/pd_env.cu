@@ -448,6 +448,7 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         // general_material.jl:92-96: deformed = (y0 != x)
         env->deformed_h[bi] = deformed ? 1 : 0;
     }
+    env->deformed0 = env->deformed_h;
     env->blocks_h = blocks;
 
     PD_TRY(env->x4.alloc(N));
@@ -853,6 +854,16 @@ extern "C" pd_status pd_env_get_time_step(const pd_env *env, int64_t *ts) {
 extern "C" pd_status pd_env_set_time_step(pd_env *env, int64_t ts) {
     PD_TRY(check_env(env));
     env->ts = ts;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_reset_deformed(pd_env *env) {
+    PD_TRY(need_final(env));
+    CK(cudaSetDevice(env->device));
+    std::vector<int32_t> h(env->deformed0.begin(), env->deformed0.end());
+    CK(cudaMemcpyAsync(env->deformed.p, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    env->deformed_h = env->deformed0;
     return PD_OK;
 }
 

@@ -155,6 +155,10 @@ struct pd_env {
     pd::DBuf<pd::DevBlock> blocks_d;
     pd::DBuf<pd::PairParam> pairs;
     pd::DBuf<double> partials, out3, stage;
+    pd::DBuf<pd::GateItem> gate_items;  // undeformed blocks for the gate kernels
+    pd::DBuf<double> gate_part;
+    std::vector<pd::GateItem> gate_items_h;
+    std::vector<int> deformed0;  // gate flags right after finalize
     pd::DBuf<int32_t> flag;
     std::vector<pd::DevBC> bcs;
     std::vector<pd::DevContact> contacts;

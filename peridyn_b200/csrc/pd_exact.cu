@@ -421,19 +421,21 @@ __global__ void k_zero4(int64_t N, double4 *__restrict__ a) {
 // Deformed gate: isapprox(y .- y[:,1] .+ x[:,1], x) with rtol = sqrt(eps)
 // (general_material.jl:249).  Deterministic two-stage reduction.
 // ---------------------------------------------------------------------
-constexpr int kGateBlocks = 148;
 constexpr int kGateThreads = 256;
 
 __global__ void __launch_bounds__(kGateThreads)
-    k_gate_partial(int64_t first, int64_t n, const double4 *__restrict__ x4,
-                   const double4 *__restrict__ y, double *__restrict__ partials,
-                   const int32_t *__restrict__ flag) {
-    if (*flag) return;
+    k_gate_partial(const GateItem *__restrict__ items, int gx, const double4 *__restrict__ x4,
+                   const double4 *__restrict__ y, double *__restrict__ part,
+                   const int32_t *__restrict__ deformed) {
+    const GateItem it = items[blockIdx.y];
+    double *partials = part + 3 * ((int64_t)blockIdx.y * gx);
+    if (deformed[it.block]) return;
+    const int64_t first = it.first, n = it.n;
     __shared__ double sh[3][kGateThreads];
     double4 y1 = y[first], x1 = x4[first];
     double sd = 0.0, sa = 0.0, sx = 0.0;
     for (int64_t l = blockIdx.x * (int64_t)kGateThreads + threadIdx.x; l < n;
-         l += (int64_t)kGateBlocks * kGateThreads) {
+         l += (int64_t)gx * kGateThreads) {
         double4 yi = y[first + l], xi = x4[first + l];
         double a0 = (yi.x - y1.x) + x1.x, a1 = (yi.y - y1.y) + x1.y, a2 = (yi.z - y1.z) + x1.z;
         double d0 = a0 - xi.x, d1 = a1 - xi.y, d2 = a2 - xi.z;
@@ -454,10 +456,15 @@ __global__ void __launch_bounds__(kGateThreads)
         for (int c = 0; c < 3; ++c) partials[3 * blockIdx.x + c] = sh[c][0];
 }
 
-__global__ void k_gate_final(const double *__restrict__ partials, int32_t *__restrict__ flag) {
+__global__ void k_gate_final(const GateItem *__restrict__ items, int nitems, int gx,
+                             const double *__restrict__ part, int32_t *__restrict__ deformed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    int32_t *flag = deformed + items[i].block;
     if (*flag) return;
+    const double *partials = part + 3 * ((int64_t)i * gx);
     double sd = 0.0, sa = 0.0, sx = 0.0;
-    for (int b = 0; b < kGateBlocks; ++b) {
+    for (int b = 0; b < gx; ++b) {
         sd = sd + partials[3 * b];
         sa = sa + partials[3 * b + 1];
         sx = sx + partials[3 * b + 2];
@@ -636,12 +643,13 @@ void launch_zero4(cudaStream_t st, int64_t N, double4 *a) {
     k_zero4<<<grid_for(N, 256), 256, 0, st>>>(N, a); pd::note_launch();
 }
 
-void launch_gate(cudaStream_t st, int64_t first, int64_t n, const double4 *x4,
-                 const double4 *y, double *partials, int32_t *deformed_flag) {
-    if (n <= 0) return;
-    k_gate_partial<<<kGateBlocks, kGateThreads, 0, st>>>(first, n, x4, y, partials,
-                                                          deformed_flag); pd::note_launch();
-    k_gate_final<<<1, 1, 0, st>>>(partials, deformed_flag); pd::note_launch();
+void launch_gate_multi(cudaStream_t st, const GateItem *items, int nitems, int gx, const double4 *x4,
+                       const double4 *y, double *partials, int32_t *deformed) {
+    if (nitems <= 0) return;
+    k_gate_partial<<<dim3(gx, nitems), kGateThreads, 0, st>>>(items, gx, x4, y, partials, deformed);
+    pd::note_launch();
+    k_gate_final<<<(nitems + 127) / 128, 128, 0, st>>>(items, nitems, gx, partials, deformed);
+    pd::note_launch();
 }
 
 void launch_damage(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -76,10 +77,13 @@ struct FBC {
 template <class R>
 struct StepArgs {
     int64_t N;
-    const typename Tr<R>::V4 *x;  // (x, vol): FP32C relative to the block centre
-    const typename Tr<R>::V4 *ucur;
-    typename Tr<R>::V4 *unext;
-    double *ax, *ay, *az;  // FP64 displacement accumulator (FP32C)
+    // Interleaved particle records, double-buffered by step parity:
+    // xu[2i] = (x, volume) (FP32C: relative to the block centre; identical
+    // in both buffers), xu[2i+1] = (u, -) displacement.  One address per
+    // neighbour fetches both.
+    const typename Tr<R>::V4 *xu;
+    typename Tr<R>::V4 *xn;  // next-step buffer (only the u records are written)
+    double *ax, *ay, *az;    // FP64 displacement accumulator (FP32C)
     typename Tr<R>::V4 *v, *f, *p;
     const R *irho, *mass;
     typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
@@ -165,7 +169,8 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
     constexpr int CS = Split<WPS>::CS;
     const int32_t n = a.cnt[p];
     const int64_t sp = a.slice_ptr[p >> 5];
-    const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+    const int32_t *nb = a.nbr + sp + (p & 31);
+    uint32_t *wp = a.words + (sp >> 5) + (p & 31);
     R Ap = 0, Bp = 0;
     if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
         typename Tr<R>::V2 m = a.mab[p];
@@ -174,61 +179,54 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
     }
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
-        const int64_t widx = wb + 32 * (int64_t)(w0 >> 5);
-        const uint32_t word = a.words[widx];
-        uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+        uint32_t *wptr = wp + 32 * (w0 >> 5);
+        const uint32_t word = *wptr;
+        const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+        if (!bits) continue;
+        // Dense walk over the chunk: intact bonds dominate, so testing the
+        // bit per bond is cheaper than extracting set bits; the unrolled
+        // iterations' index and neighbour loads overlap.
+        const int32_t kend = min(CS, n - w0);
+        const int32_t *np = nb + 32 * w0;
         uint32_t brk = 0;
-        // U bonds in flight per thread: their index and neighbour loads are
-        // issued before any of them is used (memory-level parallelism).
-        while (m) {
-            int j[U];
-            int32_t q[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                j[u] = m ? __ffs(m) - 1 : -1;
-                m &= m - 1;
+#pragma unroll U
+        for (int32_t j = 0; j < kend; ++j) {
+            const int32_t q = __ldg(np + 32 * j);
+            const V4 *r = a.xu + 2 * (int64_t)q;
+            const V4 xq = r[0];
+            const V4 uq = r[1];
+            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
+            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
+            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+            const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
+            const R lx = xx2 * rx, ly = yy2 * ry;
+            // 2 xi.eta + eta.eta = eta . (xi + Y)
+            const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+            const R dl = (ly + lx) * lx;
+            if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
+            const bool live = (bits >> j) & 1u;
+            if (!(num < pp.cs * dl)) {
+                if (kBreak && live) brk |= 1u << j;
+                continue;
             }
-#pragma unroll
-            for (int u = 0; u < U; ++u) q[u] = j[u] >= 0 ? a.nbr[base + 32 * (int64_t)(w0 + j[u])] : (int32_t)p;
-            V4 xq[U], uq[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                xq[u] = a.x[q[u]];
-                uq[u] = a.ucur[q[u]];
+            if (!live) continue;
+            const R s = Tr<R>::div(num, dl);
+            R t;
+            if (KIND == PD_MAT_BOND_BASED) {
+                t = B.c11 * s;
+            } else {
+                typename Tr<R>::V2 mq = a.mab[q];
+                t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
             }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (j[u] < 0) continue;
-                const R x0 = xq[u].x - xp.x, x1 = xq[u].y - xp.y, x2 = xq[u].z - xp.z;
-                const R e0 = uq[u].x - up.x, e1 = uq[u].y - up.y, e2 = uq[u].z - up.z;
-                const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-                const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-                const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-                const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
-                const R lx = xx2 * rx, ly = yy2 * ry;
-                const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
-                const R dl = (ly + lx) * lx;
-                if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q[u]] & 255) * B.nt];
-                if (!(num < pp.cs * dl)) {
-                    if (kBreak) brk |= 1u << j[u];
-                    continue;
-                }
-                const R s = Tr<R>::div(num, dl);
-                R t;
-                if (KIND == PD_MAT_BOND_BASED) {
-                    t = B.c11 * s;
-                } else {
-                    typename Tr<R>::V2 mq = a.mab[q[u]];
-                    t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
-                }
-                const R coef = t * ry * xq[u].w;
-                fx += coef * Y0;
-                fy += coef * Y1;
-                fz += coef * Y2;
-            }
+            const R coef = t * ry * xq.w;
+            fx += coef * Y0;
+            fy += coef * Y1;
+            fz += coef * Y2;
         }
         // bonds break rarely; two warps may own the halves of one word
-        if (kBreak && brk) atomicAnd(&a.words[widx], ~(CS == 32 ? brk : (brk << (w0 & 31))));
+        if (kBreak && brk) atomicAnd(wptr, ~(CS == 32 ? brk : (brk << (w0 & 31))));
     }
 }
 
@@ -284,7 +282,7 @@ __device__ __forceinline__ void load_u(const StepArgs<R> &a, int64_t p, double &
         u1 = a.ay[p];
         u2 = a.az[p];
     } else {
-        const typename Tr<R>::V4 u = a.ucur[p];
+        const typename Tr<R>::V4 u = a.xu[2 * p + 1];
         u0 = (double)u.x;
         u1 = (double)u.y;
         u2 = (double)u.z;
@@ -303,7 +301,7 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
     o.y = (R)u1;
     o.z = (R)u2;
     o.w = R(0);
-    a.unext[p] = o;
+    a.xn[2 * p + 1] = o;
 }
 
 // MODE 0: force only (update_acc!): f, p = m v.
@@ -335,7 +333,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         const int b = ti >> 8, tp = ti & 255;
         const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
-            const V4 xp = a.x[p], up = a.ucur[p];
+            const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
             if (B.kind == PD_MAT_BOND_BASED)
                 bond_gather<R, PD_MAT_BOND_BASED, MODE != 5, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
             else
@@ -347,7 +345,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     const R fx = f[0], fy = f[1], fz = f[2];
     if (p >= a.N) return;
     if (ti < 0) {
-        if (MODE == 1) a.unext[p] = V4{};
+        if (MODE == 1) a.xn[2 * p + 1] = V4{};
         return;
     }
     const R ir = a.irho[p];
@@ -361,7 +359,7 @@ __global__ void __launch_bounds__(kT) k_integrate(StepArgs<R> a) {
     const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
     if (p >= a.N) return;
     if (a.tinfo[p] < 0) {
-        if (MODE == 3) a.unext[p] = V4{};
+        if (MODE == 3) a.xn[2 * p + 1] = V4{};
         return;
     }
     const V4 ff = a.f[p];
@@ -414,7 +412,7 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
     if (p >= a.N) return;
     if (a.tinfo[p] < 0) {
-        a.unext[p] = V4{};
+        a.xn[2 * p + 1] = V4{};
         return;
     }
     const V4 ff = a.f[p], vp = a.v[p];
@@ -449,41 +447,31 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
     if (lps) {
-        const V4 xp = a.x[p], up = a.ucur[p];
+        const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
         const int32_t n = a.cnt[p];
         const int64_t sp = a.slice_ptr[p >> 5];
-        const int64_t base = sp + (p & 31), wb = (sp >> 5) + (p & 31);
+        const int32_t *nb = a.nbr + sp + (p & 31);
+        const uint32_t *wp = a.words + (sp >> 5) + (p & 31);
         for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
-            const uint32_t word = a.words[wb + 32 * (int64_t)(w0 >> 5)];
-            uint32_t m = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
-            while (m) {
-                int j[U];
-                int32_t q[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    j[u] = m ? __ffs(m) - 1 : -1;
-                    m &= m - 1;
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) q[u] = j[u] >= 0 ? a.nbr[base + 32 * (int64_t)(w0 + j[u])] : (int32_t)p;
-                V4 xq[U], uq[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    xq[u] = a.x[q[u]];
-                    uq[u] = a.ucur[q[u]];
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    if (j[u] < 0) continue;
-                    const R x0 = xq[u].x - xp.x, x1 = xq[u].y - xp.y, x2 = xq[u].z - xp.z;
-                    const R e0 = uq[u].x - up.x, e1 = uq[u].y - up.y, e2 = uq[u].z - up.z;
-                    const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-                    const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-                    const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-                    const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
-                    const R num = R(2) * (x0 * e0 + x1 * e1 + x2 * e2) + (e0 * e0 + e1 * e1 + e2 * e2);
-                    acc += Tr<R>::div(num, ly + lx) * xq[u].w;
-                }
+            const uint32_t word = wp[32 * (w0 >> 5)];
+            const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+            if (!bits) continue;
+            const int32_t kend = min(CS, n - w0);
+            const int32_t *np = nb + 32 * w0;
+#pragma unroll U
+            for (int32_t j = 0; j < kend; ++j) {
+                const int32_t q = __ldg(np + 32 * j);
+                const V4 *r = a.xu + 2 * (int64_t)q;
+                const V4 xq = r[0];
+                const V4 uq = r[1];
+                const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
+                const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
+                const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+                const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+                const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+                const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
+                const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+                if ((bits >> j) & 1u) acc += Tr<R>::div(num, ly + lx) * xq.w;
             }
         }
     }
@@ -496,17 +484,22 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
 
 // Deformed gate on y = x + u (general_material.jl:243-255).
 constexpr int kGB = 148, kGT = 256;
+// One GateItem per block still undeformed; grid.y walks the list and
+// grid.x = gx CTAs share each block, so any number of blocks is tested in
+// two launches.
 template <class R>
-__global__ void __launch_bounds__(kGT) k_fgate_partial(StepArgs<R> a, int64_t first, int64_t n, double *part,
-                                                      const int32_t *flag) {
-    if (*flag) return;
+__global__ void __launch_bounds__(kGT) k_fgate_partial(StepArgs<R> a, const GateItem *items, int gx, double *part) {
+    const GateItem it = items[blockIdx.y];
+    double *out = part + 3 * ((int64_t)blockIdx.y * gx + blockIdx.x);
+    if (a.deformed[it.block]) return;
+    const int64_t first = it.first, n = it.n;
     __shared__ double sh[3][kGT];
     double u0, u1, u2;
     load_u(a, first, u0, u1, u2);
     const double4 x1 = a.x64[first];
     const double y10 = x1.x + u0, y11 = x1.y + u1, y12 = x1.z + u2;
     double sd = 0, sa = 0, sx = 0;
-    for (int64_t l = blockIdx.x * (int64_t)kGT + threadIdx.x; l < n; l += (int64_t)kGB * kGT) {
+    for (int64_t l = blockIdx.x * (int64_t)kGT + threadIdx.x; l < n; l += (int64_t)gx * kGT) {
         const double4 xi = a.x64[first + l];
         load_u(a, first + l, u0, u1, u2);
         const double A0 = ((xi.x + u0) - y10) + x1.x, A1 = ((xi.y + u1) - y11) + x1.y, A2 = ((xi.z + u2) - y12) + x1.z;
@@ -525,16 +518,20 @@ __global__ void __launch_bounds__(kGT) k_fgate_partial(StepArgs<R> a, int64_t fi
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int c = 0; c < 3; ++c) part[3 * blockIdx.x + c] = sh[c][0];
+        for (int c = 0; c < 3; ++c) out[c] = sh[c][0];
 }
 
-__global__ void k_fgate_final(const double *part, int32_t *flag) {
+__global__ void k_fgate_final(const GateItem *items, int nitems, int gx, const double *part, int32_t *deformed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    int32_t *flag = deformed + items[i].block;
     if (*flag) return;
     double sd = 0, sa = 0, sx = 0;
-    for (int b = 0; b < kGB; ++b) {
-        sd += part[3 * b];
-        sa += part[3 * b + 1];
-        sx += part[3 * b + 2];
+    for (int b = 0; b < gx; ++b) {
+        const double *q = part + 3 * ((int64_t)i * gx + b);
+        sd += q[0];
+        sa += q[1];
+        sx += q[2];
     }
     const double d = sqrt(sd);
     const bool approx = isfinite(d) && d <= fmax(0.0, 0x1p-26 * fmax(sqrt(sa), sqrt(sx)));
@@ -560,12 +557,16 @@ __global__ void k_import(int64_t N, const double4 *x4, const double4 *y, const d
         xs = V4{(R)xi.x, (R)xi.y, (R)xi.z, (R)xi.w};
     }
     if (sizeof(R) == 4) {
-        const_cast<V4 *>(a.x)[p] = xs;
         a.ax[p] = u0;
         a.ay[p] = u1;
         a.az[p] = u2;
     }
-    const_cast<V4 *>(a.ucur)[p] = V4{(R)u0, (R)u1, (R)u2, R(0)};
+    // the reference position lives in both halves of the double buffer
+    V4 *cur = const_cast<V4 *>(a.xu);
+    cur[2 * p] = xs;
+    a.xn[2 * p] = xs;
+    cur[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, R(0)};
+    a.xn[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, R(0)};
     a.v[p] = V4{(R)vi.x, (R)vi.y, (R)vi.z, R(0)};
     a.f[p] = V4{(R)fi.x, (R)fi.y, (R)fi.z, R(0)};
     a.p[p] = V4{(R)pi.x, (R)pi.y, (R)pi.z, R(0)};
@@ -724,7 +725,7 @@ template <class R>
 struct Fast {
     using V4 = typename Tr<R>::V4;
     using V2 = typename Tr<R>::V2;
-    DBuf<V4> x, u[2], v, f, p;
+    DBuf<V4> xu[2], v, f, p;  // xu: interleaved (x, u) records, 2N entries each
     DBuf<double> ax, ay, az;
     DBuf<R> irho, mass;
     DBuf<V2> mab;
@@ -732,6 +733,8 @@ struct Fast {
     DBuf<FPair<R>> fp;
     DBuf<uint8_t> bcbits;
     DBuf<double> gpart;
+    DBuf<GateItem> gitems;
+    std::vector<GateItem> gitems_h;
     DBuf<V4> tune;        // autotuner output scratch
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     int cur = 0;
@@ -795,9 +798,8 @@ template <class R>
 StepArgs<R> args(pd_env *env, Fast<R> &F) {
     StepArgs<R> a{};
     a.N = env->N;
-    a.x = sizeof(R) == 4 ? F.x.p : (const typename Tr<R>::V4 *)(void *)env->x4.p;
-    a.ucur = F.u[F.cur].p;
-    a.unext = F.u[1 - F.cur].p;
+    a.xu = F.xu[F.cur].p;
+    a.xn = F.xu[1 - F.cur].p;
     a.ax = F.ax.p;
     a.ay = F.ay.p;
     a.az = F.az.p;
@@ -843,15 +845,14 @@ uint32_t dir_bits(const pd_env *env) {
 template <class R>
 pd_status init_fast(pd_env *env, Fast<R> &F) {
     const int64_t N = env->N;
-    if (!F.u[0].p) {
+    if (!F.xu[0].p) {
         if (sizeof(R) == 4) {
-            PD_TRY(F.x.alloc(N));
             PD_TRY(F.ax.alloc(N));
             PD_TRY(F.ay.alloc(N));
             PD_TRY(F.az.alloc(N));
         }
-        PD_TRY(F.u[0].alloc(N));
-        PD_TRY(F.u[1].alloc(N));
+        PD_TRY(F.xu[0].alloc(2 * N));
+        PD_TRY(F.xu[1].alloc(2 * N));
         PD_TRY(F.v.alloc(N));
         PD_TRY(F.f.alloc(N));
         PD_TRY(F.p.alloc(N));
@@ -859,7 +860,6 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         PD_TRY(F.mass.alloc(N));
         PD_TRY(F.mab.alloc(N));
         PD_TRY(F.bcbits.alloc(N));
-        PD_TRY(F.gpart.alloc(3 * kGB));
         // parameters in the working precision
         std::vector<FBlock<R>> fb;
         std::vector<FPair<R>> fp;
@@ -902,14 +902,28 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
 
 template <class R>
 pd_status gate_if_needed(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
+    std::vector<GateItem> items;
     for (size_t b = 0; b < env->hb.size(); ++b) {
         const HostBlock &hb = env->hb[b];
         if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
-        k_fgate_partial<R><<<kGB, kGT, 0, env->st>>>(a, hb.first_int, hb.n, F.gpart.p, env->deformed.p + b);
-        k_fgate_final<<<1, 1, 0, env->st>>>(F.gpart.p, env->deformed.p + b);
-        note_launch();
-        note_launch();
+        items.push_back(GateItem{hb.first_int, hb.n, (int32_t)b, 0});
     }
+    if (items.empty()) return PD_OK;
+    const int ni = (int)items.size();
+    const int gx = std::max(1, std::min(kGB, (kGB * 8) / ni));
+    if (F.gitems_h.size() != items.size() ||
+        std::memcmp(F.gitems_h.data(), items.data(), items.size() * sizeof(GateItem)) != 0) {
+        PD_TRY(F.gitems.alloc(items.size()));
+        PD_TRY(F.gpart.alloc(3 * (size_t)ni * gx));
+        CK(cudaMemcpyAsync(F.gitems.p, items.data(), items.size() * sizeof(GateItem), cudaMemcpyHostToDevice,
+                           env->st));
+        CK(cudaStreamSynchronize(env->st));
+        F.gitems_h = items;
+    }
+    k_fgate_partial<R><<<dim3(gx, ni), kGT, 0, env->st>>>(a, F.gitems.p, gx, F.gpart.p);
+    k_fgate_final<<<(ni + 127) / 128, 128, 0, env->st>>>(F.gitems.p, ni, gx, F.gpart.p, env->deformed.p);
+    note_launch();
+    note_launch();
     return PD_OK;
 }
 

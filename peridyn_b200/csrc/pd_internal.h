@@ -119,9 +119,14 @@ void launch_momentum(cudaStream_t st, int64_t N, const double *mass, const doubl
                      double4 *p);
 void launch_zero4(cudaStream_t st, int64_t N, double4 *a);
 
-// Deformed gate (general_material.jl:243-255).
-void launch_gate(cudaStream_t st, int64_t first, int64_t n, const double4 *x4,
-                 const double4 *y, double *partials, int32_t *deformed_flag);
+// Deformed gate (general_material.jl:243-255), for every listed block in
+// two launches: grid.y = list entry, grid.x = gx CTAs per block.
+struct GateItem {
+    int64_t first, n;
+    int32_t block, pad;
+};
+void launch_gate_multi(cudaStream_t st, const GateItem *items, int nitems, int gx, const double4 *x4,
+                       const double4 *y, double *partials, int32_t *deformed);
 
 // Damage / diagnostics.
 void launch_damage(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,

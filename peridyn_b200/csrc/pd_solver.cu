@@ -168,10 +168,25 @@ pd_status update_acc_serial(pd_env *env) {
     cudaStream_t st = env->st;
     Geo g = env->geo();
     // force_density! gate for blocks still undeformed
+    std::vector<GateItem> items;
     for (size_t b = 0; b < env->hb.size(); ++b) {
         const HostBlock &hb = env->hb[b];
         if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
-        launch_gate(st, hb.first_int, hb.n, env->x4.p, env->y.p, env->partials.p, env->deformed.p + b);
+        items.push_back(GateItem{hb.first_int, hb.n, (int32_t)b, 0});
+    }
+    if (!items.empty()) {
+        const int ni = (int)items.size();
+        const int gx = std::max(1, std::min(148, (148 * 8) / ni));
+        if (env->gate_items_h.size() != items.size() ||
+            std::memcmp(env->gate_items_h.data(), items.data(), items.size() * sizeof(GateItem)) != 0) {
+            PD_TRY(env->gate_items.alloc(items.size()));
+            PD_TRY(env->gate_part.alloc(3 * (size_t)ni * gx));
+            CK(cudaMemcpyAsync(env->gate_items.p, items.data(), items.size() * sizeof(GateItem),
+                               cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+            env->gate_items_h = items;
+        }
+        launch_gate_multi(st, env->gate_items.p, ni, gx, env->x4.p, env->y.p, env->gate_part.p, env->deformed.p);
     }
     // out_of_loop!: dilatation for state-based blocks
     bool any_lps = false;
