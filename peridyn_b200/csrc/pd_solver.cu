@@ -4,6 +4,7 @@
 // -fmad=false (the QSDrag update below must round like the reference).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "pd_env_impl.h"
