@@ -128,6 +128,22 @@ struct Split {
     static constexpr int MINB = 1024 / BT;            // resident blocks per SM aimed for (<= 64 registers)
 };
 
+// The index loads of a bond walk depend on nothing, but each thread only
+// has a few of them in flight.  At kernel entry every warp asks L2 for all
+// 128-byte index lines of the chunks it will walk (one line per lane), so
+// the walk's loads hit L2 instead of waiting on HBM one chunk at a time.
+template <int WPS>
+__device__ __forceinline__ void prefetch_slice_indices(const int32_t *nbr, const int64_t *slice_ptr, int64_t s,
+                                                       int w, int lane) {
+    constexpr int CS = Split<WPS>::CS;
+    const int64_t s0 = slice_ptr[s];
+    const int32_t len = (int32_t)((slice_ptr[s + 1] - s0) >> 5);
+    for (int32_t c0 = w * CS; c0 < len; c0 += WPS * CS) {
+        const int32_t k = c0 + lane;
+        if (lane < CS && k < len) asm volatile("prefetch.global.L2 [%0];" ::"l"(nbr + s0 + 32 * (int64_t)k));
+    }
+}
+
 // Combine the WPS partial sums of one slice without a block barrier: each
 // warp publishes its partials, and the last warp of the slice to arrive
 // adds them in warp order (fixed, so the result does not depend on which
@@ -310,7 +326,8 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 // MODE 2: full step, last of the chunk: f, p, kick, BC vel, store v and f.
 // MODE 3: integration only (forces already in f, e.g. after contacts).
 // MODE 4: integration only, last of the chunk.
-// MODE 5: force only into a scratch array, no bond breaking (autotuning).
+// MODE 5: force only into a scratch array, no bond breaking.
+// MODE 6: MODE 1 without bond breaking, on scratch outputs (autotuning).
 template <class R, int MODE>
 __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
 
@@ -327,7 +344,9 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.slice_ptr, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
+    constexpr bool kBreak = MODE != 5 && MODE != 6;
     R f[3] = {0, 0, 0};
     if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
@@ -335,17 +354,17 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
             if (B.kind == PD_MAT_BOND_BASED)
-                bond_gather<R, PD_MAT_BOND_BASED, MODE != 5, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
+                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
             else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, MODE != 5, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1],
-                                                                             f[2]);
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1],
+                                                                          f[2]);
         }
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 3>(sh, arrive, wid, lane, f)) return;
     const R fx = f[0], fy = f[1], fz = f[2];
     if (p >= a.N) return;
     if (ti < 0) {
-        if (MODE == 1) a.xn[2 * p + 1] = V4{};
+        if (MODE == 1 || MODE == 6) a.xn[2 * p + 1] = V4{};
         return;
     }
     const R ir = a.irho[p];
@@ -443,6 +462,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.slice_ptr, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
@@ -736,6 +756,7 @@ struct Fast {
     DBuf<GateItem> gitems;
     std::vector<GateItem> gitems_h;
     DBuf<V4> tune;        // autotuner output scratch
+    DBuf<double> tune_d;
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     int cur = 0;
     int wps = 0;          // warps per 32-particle slice (autotuned)
@@ -985,13 +1006,26 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
             return PD_OK;
         }
     }
-    PD_TRY(F.tune.alloc(env->N));
+    // The timed kernel is the full step (force + integration, MODE 6 = MODE 1
+    // without bond breaking) writing every output into scratch arrays, so
+    // the environment's state is left untouched.
+    const int64_t N = env->N;
+    PD_TRY(F.tune.alloc(5 * N));
+    PD_TRY(F.tune_d.alloc(3 * N));
+    CK(cudaMemsetAsync(F.tune.p, 0, 5 * N * sizeof(typename Tr<R>::V4), env->st));
+    CK(cudaMemsetAsync(F.tune_d.p, 0, 3 * N * sizeof(double), env->st));
     std::vector<int32_t> ones(env->hb.size(), 1);
     PD_TRY(F.ones.alloc(ones.size()));
     CK(cudaMemcpyAsync(F.ones.p, ones.data(), ones.size() * 4, cudaMemcpyHostToDevice, env->st));
     StepArgs<R> a = args(env, F);
-    a.f = F.tune.p;
-    a.p = F.tune.p;
+    a.v = F.tune.p;
+    a.f = F.tune.p + N;
+    a.p = F.tune.p + 2 * N;
+    a.xn = F.tune.p + 3 * N;
+    a.ax = F.tune_d.p;
+    a.ay = F.tune_d.p + N;
+    a.az = F.tune_d.p + 2 * N;
+    a.nbc = 0;
     a.deformed = F.ones.p;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -1003,11 +1037,11 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
         for (int u : {Unroll<R>::LO, Unroll<R>::HI}) shapes.push_back(10 * wps + u);
     for (int w : shapes) {
         if (lps) launch_theta(env->st, w, a);
-        launch_step<R, 5>(env->st, w, a);
+        launch_step<R, 6>(env->st, w, a);
         cudaEventRecord(e0, env->st);
         for (int r = 0; r < 3; ++r) {
             if (lps) launch_theta(env->st, w, a);
-            launch_step<R, 5>(env->st, w, a);
+            launch_step<R, 6>(env->st, w, a);
         }
         cudaEventRecord(e1, env->st);
         cudaError_t err = cudaEventSynchronize(e1);
@@ -1027,6 +1061,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     cudaEventDestroy(e1);
     CK(cudaGetLastError());
     F.tune.reset();
+    F.tune_d.reset();
     F.wps = best_w;
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tune_cache[key] = best_w;
