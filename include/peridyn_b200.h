@@ -216,6 +216,12 @@ PD_API pd_status pd_env_diagnostics(pd_env *env, double *out8);
 PD_API pd_status pd_env_deformed(pd_env *env, uint8_t *flags);
 /* PD_ERR_NAN when y, v or f holds a NaN or Inf (const_macros.jl:60-74). */
 PD_API pd_status pd_env_check_finite(pd_env *env);
+/* Bond storage of a finalized environment (extension, no reference
+ * counterpart): out4[0] = 32-particle slices, out4[1] = slices stored as a
+ * shared neighbour-offset stencil, out4[2] = bond slots, out4[3] = entries
+ * of the neighbour-index array.  PD_FAMILY_LAYOUT=explicit in the process
+ * environment at finalize disables the stencil form. */
+PD_API pd_status pd_env_layout(const pd_env *env, int64_t *out4);
 
 /* ---------------------------------------------------------------------- */
 /* Device-pointer entry point for a single block                           */

@@ -410,18 +410,30 @@ __device__ __forceinline__ int ref_cell(const RefCells &c, double v, int d) {
 }
 
 __global__ void k_c11_neighs(int64_t first, int64_t n, const double4 *__restrict__ y,
-                             const int64_t *__restrict__ slice_ptr, const int32_t *__restrict__ cnt,
-                             const int32_t *__restrict__ nbr, const uint32_t *__restrict__ words, RefCells rc,
-                             double equi2, int32_t *__restrict__ nb11) {
+                             const SliceInfo *__restrict__ si, const int32_t *__restrict__ cnt,
+                             const int32_t *__restrict__ nbr, const uint32_t *__restrict__ words,
+                             const uint32_t *__restrict__ fam, RefCells rc, double equi2,
+                             int32_t *__restrict__ nb11) {
     int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (li >= n) return;
     int64_t p = first + li;
     int32_t res = -1;
-    if (cnt[p] > 0) {
-        int64_t base = slice_ptr[p >> 5] + (p & 31), wb = (slice_ptr[p >> 5] >> 5) + (p & 31);
-        bool intact0 = words[wb] & 1u;
+    // The first family member is the first slot whose family bit is set.
+    const BondRef fr = bond_ref(si, nbr, fam, p);
+    const int32_t c = cnt[p];
+    int32_t k0 = -1;
+    for (int32_t k = 0; k < c; k += 32) {
+        uint32_t m = *fr.word(k);
+        if (m) {
+            k0 = k + __ffs(m) - 1;
+            break;
+        }
+    }
+    if (k0 >= 0) {
+        const uint32_t w = words[(fr.w - fam) + 32 * (int64_t)(k0 >> 5)];
+        bool intact0 = (w >> (k0 & 31)) & 1u;
         if (!intact0) {
-            int32_t q = nbr[base];
+            int32_t q = fr.q(k0);
             double4 a = y[p], b = y[q];
             bool adj = abs(ref_cell(rc, a.x, 0) - ref_cell(rc, b.x, 0)) <= 1 &&
                        abs(ref_cell(rc, a.y, 1) - ref_cell(rc, b.y, 1)) <= 1 &&
@@ -613,8 +625,8 @@ pd_status update11(pd_env *env, const HostContact &hc, DevContact &dc, int64_t m
     for (int d = 0; d < 3; ++d) rc.mn[d] = m[d];
     rc.h = hc.distance;
     rc.maxpart = (double)max_part;
-    k_c11_neighs<<<gridn(dc.n1), kT, 0, st>>>(dc.first1, dc.n1, env->y.p, env->slice_ptr.p, env->cnt.p, env->nbr.p,
-                                              env->words[env->cur].p, rc, hc.equi_dist * hc.equi_dist, dc.nb.p); pd::note_launch();
+    k_c11_neighs<<<gridn(dc.n1), kT, 0, st>>>(dc.first1, dc.n1, env->y.p, env->sinfo.p, env->cnt.p, env->nbr.p,
+                                              env->words[env->cur].p, env->fam.p, rc, hc.equi_dist * hc.equi_dist, dc.nb.p); pd::note_launch();
     CK(cudaGetLastError());
     dc.has_neighs = true;
     PD_TRY(build_reverse(env, dc, dc.n1, dc.first1, dc.n1, dc.first1, dc.nb.p, 1, true));

@@ -3,6 +3,8 @@
 // src/solvers/*.jl on one CUDA stream.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -69,9 +71,10 @@ pd::Geo pd_env::geo() const {
     g.blocks = blocks_d.p;
     g.pairs = pairs.p;
     g.tdens = tdens.p;
-    g.slice_ptr = slice_ptr.p;
+    g.si = sinfo.p;
     g.cnt = cnt.p;
     g.nbr = nbr.p;
+    g.fam = fam.p;
     g.deformed = deformed.p;
     return g;
 }
@@ -376,6 +379,120 @@ extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block
 }
 
 // ---------------------------------------------------------------------
+// Runtime bond layout.  Input: the build layout (SELL-32, bond k of lane l
+// of slice s at nbr_b[slice_ptr[s] + 32k + l], intact bit k%32 of word
+// slice_ptr[s]/32 + 32(k/32) + l, cnt[p] members in descending index order).
+// Output: one SliceInfo per slice.  A slice whose lanes' neighbour offsets
+// q - p form a small union (a lattice, where every particle sees the same
+// stencil) stores one offset per slot and reads no per-bond index; the
+// others keep the explicit indices.  cnt becomes the number of slots to scan.
+// ---------------------------------------------------------------------
+static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &slice_ptr, std::vector<int32_t> &cnt,
+                                      const std::vector<int32_t> &nbr_b, const std::vector<uint32_t> &w_b) {
+    const int64_t N = env->N, S = N / kSlice;
+    const char *lay = std::getenv("PD_FAMILY_LAYOUT");
+    const bool force_explicit = lay && std::strcmp(lay, "explicit") == 0;
+    std::vector<SliceInfo> si(S + 1);
+    std::vector<std::vector<int32_t>> uni(S);
+    int64_t nbr_len = 0, nwords = 0, nst = 0;
+    std::vector<int32_t> offs;
+    for (int64_t s = 0; s < S; ++s) {
+        int32_t maxc = 0;
+        offs.clear();
+        for (int l = 0; l < kSlice; ++l) {
+            const int64_t p = s * kSlice + l;
+            maxc = std::max(maxc, cnt[p]);
+            const int64_t base = slice_ptr[s] + l;
+            for (int32_t k = 0; k < cnt[p]; ++k) offs.push_back(nbr_b[base + 32 * (int64_t)k] - (int32_t)p);
+        }
+        std::sort(offs.begin(), offs.end(), std::greater<int32_t>());
+        offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
+        const int64_t U = (int64_t)offs.size();
+        bool stencil = !force_explicit && maxc > 0 && U <= (int64_t)maxc + maxc / 4 + 32;
+        // every slot a lane scans must name an in-range record
+        for (int l = 0; stencil && l < kSlice; ++l) {
+            const int64_t p = s * kSlice + l;
+            if (cnt[p] == 0) continue;
+            stencil = p + offs.front() < N && p + offs.back() >= 0;
+        }
+        SliceInfo &d = si[s];
+        d.nbr = nbr_len;
+        d.word = nwords;
+        if (stencil) {
+            d.mode = kStencil;
+            d.len = (int32_t)round_up(U, 32);
+            nbr_len += d.len;
+            uni[s] = offs;
+            ++nst;
+        } else {
+            d.mode = kExplicit;
+            d.len = (int32_t)round_up(maxc, 32);
+            nbr_len += (int64_t)kSlice * d.len;
+        }
+        nwords += d.len;
+    }
+    si[S].nbr = nbr_len;
+    si[S].word = nwords;
+    si[S].len = 0;
+    si[S].mode = kExplicit;
+    std::vector<int32_t> nbr(std::max<int64_t>(nbr_len, 32), 0);
+    std::vector<uint32_t> words(std::max<int64_t>(nwords, 1), 0), fam(std::max<int64_t>(nwords, 1), 0);
+    std::vector<int32_t> cnt_rt(N, 0);
+    for (int64_t s = 0; s < S; ++s) {
+        const SliceInfo &d = si[s];
+        if (d.mode == kStencil) {
+            const std::vector<int32_t> &u = uni[s];
+            for (size_t j = 0; j < u.size(); ++j) nbr[d.nbr + j] = u[j];
+        }
+        for (int l = 0; l < kSlice; ++l) {
+            const int64_t p = s * kSlice + l;
+            const int64_t base = slice_ptr[s] + l, wb = slice_ptr[s] / 32 + l, ow = d.word + l;
+            int32_t j = 0, last = -1;
+            for (int32_t k = 0; k < cnt[p]; ++k) {
+                const int32_t q = nbr_b[base + 32 * (int64_t)k];
+                int32_t slot = k;
+                if (d.mode == kStencil) {
+                    // both lists descend: advance to this offset
+                    const std::vector<int32_t> &u = uni[s];
+                    while (u[j] != q - (int32_t)p) ++j;
+                    slot = j;
+                } else {
+                    nbr[d.nbr + 32 * (int64_t)k + l] = q;
+                }
+                const uint32_t bit = 1u << (slot & 31);
+                fam[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+                if ((w_b[wb + 32 * (int64_t)(k >> 5)] >> (k & 31)) & 1u) words[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+                last = slot;
+            }
+            cnt_rt[p] = last + 1;
+        }
+    }
+    cnt.swap(cnt_rt);
+    env->sinfo_h = si;
+    env->cnt_h = cnt;
+    env->nnz = (int64_t)kSlice * nwords;
+    env->nbr_len = nbr_len;
+    env->stencil_slices = nst;
+    cudaStream_t st = env->st;
+    const int64_t nw = std::max<int64_t>(nwords, 1);
+    PD_TRY(env->sinfo.alloc(S + 1));
+    PD_TRY(env->nbr.alloc((int64_t)nbr.size()));
+    PD_TRY(env->words[0].alloc(nw));
+    PD_TRY(env->words[1].alloc(nw));
+    PD_TRY(env->words0.alloc(nw));
+    PD_TRY(env->fam.alloc(nw));
+    CK(cudaMemcpyAsync(env->sinfo.p, si.data(), (S + 1) * sizeof(SliceInfo), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->words[0].p, words.data(), nw * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->words[1].p, words.data(), nw * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->words0.p, words.data(), nw * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->fam.p, fam.data(), nw * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
 // finalize: layout, upload, families, weighted volume, intact0
 // ---------------------------------------------------------------------
 extern "C" pd_status pd_env_finalize(pd_env *env) {
@@ -575,7 +692,8 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
             b.rows = maxc + 1;
         }
     }
-    // SELL-32 slice table
+    // Build layout: SELL-32 with one explicit index per (slot, lane), filled
+    // and sorted on the device.
     const int64_t S = N / kSlice;
     std::vector<int64_t> slice_ptr(S + 1, 0);
     for (int64_t s = 0; s < S; ++s) {
@@ -583,39 +701,41 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         for (int l = 0; l < kSlice; ++l) m = std::max(m, cnt[s * kSlice + l]);
         slice_ptr[s + 1] = slice_ptr[s] + (int64_t)kSlice * round_up(m, 32);
     }
-    env->nnz = slice_ptr[S];
-    env->slice_ptr_h = slice_ptr;
-    env->cnt_h = cnt;
-    PD_TRY(env->slice_ptr.alloc(S + 1));
-    PD_TRY(env->nbr.alloc(std::max<int64_t>(env->nnz, 32)));
-    PD_TRY(env->words[0].alloc(std::max<int64_t>(env->nnz / 32, 1)));
-    PD_TRY(env->words[1].alloc(std::max<int64_t>(env->nnz / 32, 1)));
-    PD_TRY(env->words0.alloc(std::max<int64_t>(env->nnz / 32, 1)));
-    CK(cudaMemcpyAsync(env->slice_ptr.p, slice_ptr.data(), (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(env->nbr.p, 0, std::max<int64_t>(env->nnz, 32) * sizeof(int32_t), st));
-    CK(cudaMemsetAsync(env->words[0].p, 0, std::max<int64_t>(env->nnz / 32, 1) * 4, st));
-    CK(cudaMemsetAsync(env->words[1].p, 0, std::max<int64_t>(env->nnz / 32, 1) * 4, st));
-    // GPU-built families: fill + sort; initial intact = all bonds
-    for (size_t bi = 0; bi < env->hb.size(); ++bi) {
-        HostBlock &b = env->hb[bi];
-        if (b.kind == PD_MAT_SKIP || b.host_family) continue;
-        launch_fill_neighbors(st, b.n, b.first_int, env->x4.p, d_cell_of.p + b.cell_part_off, d_cell_start.p,
-                              d_cell_list.p, cell_base[bi], cells[bi].dims, b.horizon, env->slice_ptr.p,
-                              env->nbr.p);
+    const int64_t bnnz = slice_ptr[S];
+    std::vector<int32_t> nbr_b;
+    std::vector<uint32_t> w_b;
+    {
+        DBuf<int64_t> d_slice_ptr;
+        DBuf<int32_t> d_nbr;
+        DBuf<uint32_t> d_words;
+        PD_TRY(d_slice_ptr.alloc(S + 1));
+        PD_TRY(d_nbr.alloc(std::max<int64_t>(bnnz, 32)));
+        PD_TRY(d_words.alloc(std::max<int64_t>(bnnz / 32, 1)));
+        CK(cudaMemcpyAsync(d_slice_ptr.p, slice_ptr.data(), (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d_nbr.p, 0, std::max<int64_t>(bnnz, 32) * sizeof(int32_t), st));
+        CK(cudaMemsetAsync(d_words.p, 0, std::max<int64_t>(bnnz / 32, 1) * 4, st));
+        for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+            HostBlock &b = env->hb[bi];
+            if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+            launch_fill_neighbors(st, b.n, b.first_int, env->x4.p, d_cell_of.p + b.cell_part_off, d_cell_start.p,
+                                  d_cell_list.p, cell_base[bi], cells[bi].dims, b.horizon, d_slice_ptr.p, d_nbr.p);
+        }
+        launch_sort_neighbors(st, N, d_slice_ptr.p, env->cnt.p, d_nbr.p);
+        launch_init_intact(st, N, d_slice_ptr.p, env->cnt.p, d_words.p);
+        CK(cudaGetLastError());
+        nbr_b.assign(bnnz, 0);
+        w_b.assign(bnnz / 32, 0);
+        if (bnnz > 0) {
+            CK(cudaMemcpyAsync(nbr_b.data(), d_nbr.p, bnnz * 4, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(w_b.data(), d_words.p, (bnnz / 32) * 4, cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaStreamSynchronize(st));
     }
-    launch_sort_neighbors(st, N, env->slice_ptr.p, env->cnt.p, env->nbr.p);
-    launch_init_intact(st, N, env->slice_ptr.p, env->cnt.p, env->words[0].p);
-    CK(cudaGetLastError());
     // host-provided families (already descending): write entries and bits
     bool any_host = false;
     for (auto &b : env->hb) any_host |= b.host_family;
     if (any_host) {
-        std::vector<int32_t> nbr_h(env->nnz, 0);
-        std::vector<uint32_t> w_h(env->nnz / 32, 0);
-        CK(cudaMemcpyAsync(nbr_h.data(), env->nbr.p, env->nnz * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(w_h.data(), env->words[0].p, (env->nnz / 32) * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
         for (auto &b : env->hb) {
             if (!b.host_family) continue;
             for (int64_t i = 0; i < b.n; ++i) {
@@ -625,9 +745,9 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
                 for (int64_t r = 0; r < b.rows; ++r) {
                     int64_t j = b.family[(size_t)i * b.rows + r];
                     if (j <= 0) continue;
-                    nbr_h[base + 32 * k] = (int32_t)(b.first_int + j - 1);
+                    nbr_b[base + 32 * k] = (int32_t)(b.first_int + j - 1);
                     uint32_t bit = 1u << (k % 32);
-                    uint32_t &w = w_h[wb + 32 * (k / 32)];
+                    uint32_t &w = w_b[wb + 32 * (k / 32)];
                     if (b.intact[(size_t)i * b.rows + r]) w |= bit;
                     else w &= ~bit;
                     ++k;
@@ -642,13 +762,13 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
                     int64_t p = b.first_int + i;
                     int64_t base = slice_ptr[p / 32] + (p % 32), wb = slice_ptr[p / 32] / 32 + (p % 32);
                     for (int64_t k = 0; k < cnt[p]; ++k) {
-                        int64_t q = nbr_h[base + 32 * k];
-                        bool bit = (w_h[wb + 32 * (k / 32)] >> (k % 32)) & 1u;
+                        int64_t q = nbr_b[base + 32 * k];
+                        bool bit = (w_b[wb + 32 * (k / 32)] >> (k % 32)) & 1u;
                         int64_t qb = slice_ptr[q / 32] + (q % 32), qwb = slice_ptr[q / 32] / 32 + (q % 32);
                         bool found = false;
                         for (int64_t kk = 0; kk < cnt[q]; ++kk)
-                            if (nbr_h[qb + 32 * kk] == p) {
-                                found = ((w_h[qwb + 32 * (kk / 32)] >> (kk % 32)) & 1u) == bit;
+                            if (nbr_b[qb + 32 * kk] == p) {
+                                found = ((w_b[qwb + 32 * (kk / 32)] >> (kk % 32)) & 1u) == bit;
                                 break;
                             }
                         if (!found)
@@ -660,18 +780,17 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
                 }
             }
         }
-        CK(cudaMemcpyAsync(env->nbr.p, nbr_h.data(), env->nnz * 4, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(env->words[0].p, w_h.data(), (env->nnz / 32) * 4, cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));
     }
+    // Runtime layout (stencil or explicit per slice), uploaded.
+    PD_TRY(build_runtime_layout(env, slice_ptr, cnt, nbr_b, w_b));
+    nbr_b.clear();
+    nbr_b.shrink_to_fit();
+    w_b.clear();
+    w_b.shrink_to_fit();
     env->cur = 0;
-    CK(cudaMemcpyAsync(env->words0.p, env->words[0].p, std::max<int64_t>(env->nnz / 32, 1) * 4,
-                       cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(env->words[1].p, env->words[0].p, std::max<int64_t>(env->nnz / 32, 1) * 4,
-                       cudaMemcpyDeviceToDevice, st));
     // weighted volume (peri.jl:342-354) and intact0 (environment.jl:169)
     launch_weighted_volume(st, env->geo(), env->mth.p);
-    launch_popcount(st, N, env->slice_ptr.p, env->cnt.p, env->words[0].p, env->intact0.p);
+    launch_popcount(st, N, env->sinfo.p, env->cnt.p, env->words[0].p, env->intact0.p);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
 
@@ -722,7 +841,7 @@ extern "C" pd_status pd_env_num_bonds(pd_env *env, int64_t *intact_bonds) {
     CK(cudaSetDevice(env->device));
     DBuf<int32_t> tmp;
     PD_TRY(tmp.alloc(env->N));
-    launch_popcount(env->st, env->N, env->slice_ptr.p, env->cnt.p, env->words[env->cur].p, tmp.p);
+    launch_popcount(env->st, env->N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, tmp.p);
     std::vector<int32_t> h(env->N);
     CK(cudaMemcpyAsync(h.data(), tmp.p, env->N * 4, cudaMemcpyDeviceToHost, env->st));
     CK(cudaStreamSynchronize(env->st));
@@ -744,25 +863,33 @@ extern "C" pd_status pd_env_get_family(pd_env *env, int64_t block, int64_t *fami
     if (block < 0 || block >= (int64_t)env->hb.size()) return fail(PD_ERR_ARG, "no block %lld", (long long)block);
     CK(cudaSetDevice(env->device));
     const HostBlock &b = env->hb[block];
-    int64_t s0 = b.first_int / 32, s1 = (b.first_int + round_up(b.n, 32)) / 32;
-    int64_t e0 = env->slice_ptr_h[s0], e1 = env->slice_ptr_h[s1];
+    const int64_t s0 = b.first_int / 32, s1 = (b.first_int + round_up(b.n, 32)) / 32;
+    const SliceInfo *si = env->sinfo_h.data();
+    const int64_t e0 = si[s0].nbr, e1 = si[s1].nbr, w0 = si[s0].word, w1 = si[s1].word;
     std::vector<int32_t> nb(e1 - e0);
-    std::vector<uint32_t> w((e1 - e0) / 32);
-    if (e1 > e0) {
+    std::vector<uint32_t> w(w1 - w0), fm(w1 - w0);
+    if (e1 > e0)
         CK(cudaMemcpyAsync(nb.data(), env->nbr.p + e0, (e1 - e0) * 4, cudaMemcpyDeviceToHost, env->st));
-        CK(cudaMemcpyAsync(w.data(), env->words[env->cur].p + e0 / 32, (e1 - e0) / 32 * 4, cudaMemcpyDeviceToHost,
-                           env->st));
-        CK(cudaStreamSynchronize(env->st));
+    if (w1 > w0) {
+        CK(cudaMemcpyAsync(w.data(), env->words[env->cur].p + w0, (w1 - w0) * 4, cudaMemcpyDeviceToHost, env->st));
+        CK(cudaMemcpyAsync(fm.data(), env->fam.p + w0, (w1 - w0) * 4, cudaMemcpyDeviceToHost, env->st));
     }
+    CK(cudaStreamSynchronize(env->st));
     const int64_t R = b.rows;
     if (family) std::fill(family, family + (size_t)R * b.n, 0);
     if (intact) std::fill(intact, intact + (size_t)R * b.n, 0);
     for (int64_t i = 0; i < b.n; ++i) {
-        int64_t p = b.first_int + i;
-        int64_t base = env->slice_ptr_h[p / 32] - e0 + (p % 32), wb = (env->slice_ptr_h[p / 32] - e0) / 32 + (p % 32);
-        for (int64_t k = 0; k < env->cnt_h[p] && k < R; ++k) {
-            if (family) family[(size_t)i * R + k] = nb[base + 32 * k] - b.first_int + 1;
-            if (intact) intact[(size_t)i * R + k] = (w[wb + 32 * (k / 32)] >> (k % 32)) & 1u;
+        const int64_t p = b.first_int + i;
+        const SliceInfo &d = si[p / 32];
+        const int64_t wb = d.word - w0 + (p % 32);
+        int64_t r = 0;
+        for (int32_t k = 0; k < env->cnt_h[p] && r < R; ++k) {
+            const uint32_t bit = 1u << (k % 32);
+            if (!(fm[wb + 32 * (k / 32)] & bit)) continue;
+            const int64_t q = d.mode == kStencil ? p + nb[d.nbr - e0 + k] : nb[d.nbr - e0 + 32 * (int64_t)k + (p % 32)];
+            if (family) family[(size_t)i * R + r] = q - b.first_int + 1;
+            if (intact) intact[(size_t)i * R + r] = (w[wb + 32 * (k / 32)] & bit) != 0;
+            ++r;
         }
     }
     return PD_OK;
@@ -884,7 +1011,7 @@ extern "C" pd_status pd_env_reset_bonds(pd_env *env) {
 static pd_status damage_internal(pd_env *env, std::vector<double> &dint) {
     DBuf<double> d;
     PD_TRY(d.alloc(env->N));
-    launch_damage(env->st, env->N, env->slice_ptr.p, env->cnt.p, env->words[env->cur].p, env->intact0.p,
+    launch_damage(env->st, env->N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, env->intact0.p,
                   env->tinfo.p, d.p);
     CK(cudaGetLastError());
     dint.resize(env->N);
@@ -961,6 +1088,16 @@ extern "C" pd_status pd_env_check_finite(pd_env *env) {
     CK(cudaMemcpyAsync(&h, env->flag.p, 4, cudaMemcpyDeviceToHost, env->st));
     CK(cudaStreamSynchronize(env->st));
     if (h) return fail(PD_ERR_NAN, "NaN or Inf in y, v or f");
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_layout(const pd_env *env, int64_t *out4) {
+    PD_TRY(need_final(env));
+    if (!out4) return fail(PD_ERR_ARG, "out4 is NULL");
+    out4[0] = env->N / kSlice;
+    out4[1] = env->stencil_slices;
+    out4[2] = env->nnz;
+    out4[3] = env->nbr_len;
     return PD_OK;
 }
 

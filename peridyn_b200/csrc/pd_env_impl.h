@@ -139,17 +139,21 @@ struct pd_env {
     std::vector<int64_t> map_h;
     std::vector<pd::DevBlock> blocks_h;
     std::vector<int> deformed_h;
-    std::vector<int64_t> slice_ptr_h;
+    // runtime bond layout: S+1 slice descriptors (the last one only marks
+    // the end of nbr[] and of the bit arrays)
+    std::vector<pd::SliceInfo> sinfo_h;
     std::vector<int32_t> cnt_h;
-    int64_t nnz = 0;
+    int64_t nnz = 0;       // bond slots (bits per bit array)
+    int64_t nbr_len = 0;   // entries of nbr[]
+    int64_t stencil_slices = 0;
 
     pd::DBuf<int64_t> map;
     pd::DBuf<double4> x4, y, v, f, p;
     pd::DBuf<double> mass, dens, tdens;
     pd::DBuf<int32_t> tinfo, cnt, intact0, deformed;
-    pd::DBuf<int64_t> slice_ptr;
+    pd::DBuf<pd::SliceInfo> sinfo;
     pd::DBuf<int32_t> nbr;
-    pd::DBuf<uint32_t> words[2], words0;
+    pd::DBuf<uint32_t> words[2], words0, fam;
     int cur = 0;
     pd::DBuf<double2> mth;
     pd::DBuf<pd::DevBlock> blocks_d;

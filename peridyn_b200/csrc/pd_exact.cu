@@ -114,29 +114,30 @@ __global__ void k_init_intact(int64_t N, const int64_t *__restrict__ slice_ptr,
     }
 }
 
-__global__ void k_popcount(int64_t N, const int64_t *__restrict__ slice_ptr,
+__global__ void k_popcount(int64_t N, const SliceInfo *__restrict__ si,
                            const int32_t *__restrict__ cnt, const uint32_t *__restrict__ words,
                            int32_t *__restrict__ out) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= N) return;
     int32_t n = cnt[p], c = 0;
-    int64_t wb = word_base(slice_ptr, p);
-    for (int32_t w = 0; w * 32 < n; ++w) c += __popc(words[wb + 32 * (int64_t)w]);
+    const uint32_t *wp = words + si[p >> 5].word + (p & 31);
+    for (int32_t w = 0; w * 32 < n; ++w) c += __popc(wp[32 * (int64_t)w]);
     out[p] = c;
 }
 
 // peri.jl:342-354 weighted_volume: m_i = sum_j ((1/|X|) * (|X|*|X|)) * 1 * V_j
-// over the family in stored (descending) order.
+// over the family (every member, intact or not) in stored (descending) order.
 __global__ void k_weighted_volume(Geo g, double2 *__restrict__ mth) {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= g.N) return;
     if (g.tinfo[p] < 0) return;
     double4 xp = g.x4[p];
     int32_t n = g.cnt[p];
-    int64_t base = sell_base(g.slice_ptr, p);
+    const BondRef br = bond_ref(g.si, g.nbr, g.fam, p);
     double acc = 0.0;
     for (int32_t k = 0; k < n; ++k) {
-        int32_t q = g.nbr[base + 32 * (int64_t)k];
+        if (!((*br.word(k) >> (k & 31)) & 1u)) continue;
+        int32_t q = br.q(k);
         double4 xq = g.x4[q];
         double mg = mag3(xq.x - xp.x, xq.y - xp.y, xq.z - xp.z);
         double w = 1.0 / mg;
@@ -161,13 +162,13 @@ __global__ void k_theta_serial(Geo g, const double4 *__restrict__ y,
     double4 xp = g.x4[p], yp = y[p];
     double c_i = 3.0 / mth[p].x;
     int32_t n = g.cnt[p];
-    int64_t base = sell_base(g.slice_ptr, p), wb = word_base(g.slice_ptr, p);
+    const BondRef br = bond_ref(g.si, g.nbr, win, p);
     double th = 0.0;
     uint32_t w = 0;
     for (int32_t k = 0; k < n; ++k) {
-        if ((k & 31) == 0) w = win[wb + 32 * (int64_t)(k >> 5)];
+        if ((k & 31) == 0) w = *br.word(k);
         if (!((w >> (k & 31)) & 1u)) continue;
-        int32_t q = g.nbr[base + 32 * (int64_t)k];
+        int32_t q = br.q(k);
         double4 xq = g.x4[q], yq = y[q];
         double xij = mag3(xq.x - xp.x, xq.y - xp.y, xq.z - xp.z);
         double yij = mag3(yq.x - yp.x, yq.y - yp.y, yq.z - yp.z);
@@ -241,7 +242,8 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
     double2 mp = KIND == PD_MAT_ORDINARY_STATE_BASED ? mth[p] : make_double2(0.0, 0.0);
     double rho_p = g.tdens[B.type_base + tp];
     int32_t n = g.cnt[p];
-    int64_t base = sell_base(g.slice_ptr, p), wb = word_base(g.slice_ptr, p);
+    const BondRef br = bond_ref(g.si, g.nbr, win, p);
+    uint32_t *wo = wout + g.si[p >> 5].word + (p & 31);
     double fx = 0.0, fy = 0.0, fz = 0.0;
     if (accumulate) {
         double4 f0 = f[p];
@@ -253,9 +255,9 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
     // Pass A: q < p, ascending (walk the descending list from the end).
     int32_t k = n - 1;
     for (; k >= 0; --k) {
-        int32_t q = g.nbr[base + 32 * (int64_t)k];
+        int32_t q = br.q(k);
         if (q > p) break;
-        uint32_t w = win[wb + 32 * (int64_t)(k >> 5)];
+        uint32_t w = *br.word(k);
         if (!((w >> (k & 31)) & 1u)) continue;
         if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
@@ -268,11 +270,11 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
     uint32_t w = 0;
     for (k = 0; k < n; ++k) {
         if ((k & 31) == 0) {
-            if (k > 0) wout[wb + 32 * (int64_t)((k >> 5) - 1)] = w;
-            w = win[wb + 32 * (int64_t)(k >> 5)];
+            if (k > 0) wo[32 * (int64_t)((k >> 5) - 1)] = w;
+            w = *br.word(k);
         }
         if (!((w >> (k & 31)) & 1u)) continue;
-        int32_t q = g.nbr[base + 32 * (int64_t)k];
+        int32_t q = br.q(k);
         if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
             fy = fy + t1;
@@ -281,11 +283,11 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
             w &= ~(1u << (k & 31));
         }
     }
-    if (n > 0) wout[wb + 32 * (int64_t)((n - 1) >> 5)] = w;
+    if (n > 0) wo[32 * (int64_t)((n - 1) >> 5)] = w;
     // Pass C: q > p, ascending.
     for (k = kc; k >= 0; --k) {
-        int32_t q = g.nbr[base + 32 * (int64_t)k];
-        uint32_t ww = win[wb + 32 * (int64_t)(k >> 5)];
+        int32_t q = br.q(k);
+        uint32_t ww = *br.word(k);
         if (!((ww >> (k & 31)) & 1u)) continue;
         if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(kThreads)
     if (p >= p1) return;
     int32_t ti = g.tinfo[p];
     int32_t n = g.cnt[p];
-    int64_t wb = word_base(g.slice_ptr, p);
+    const int64_t wb = g.si[p >> 5].word + (p & 31);
     bool active = false;
     int kind = PD_MAT_SKIP;
     if (ti >= 0) {
@@ -476,7 +478,7 @@ __global__ void k_gate_final(const GateItem *__restrict__ items, int nitems, int
 }
 
 // peri.jl:587-594 cal_damage: 1 - sum(intact) / intact0
-__global__ void k_damage(int64_t N, const int64_t *__restrict__ slice_ptr,
+__global__ void k_damage(int64_t N, const SliceInfo *__restrict__ si,
                          const int32_t *__restrict__ cnt, const uint32_t *__restrict__ words,
                          const int32_t *__restrict__ intact0, const int32_t *__restrict__ tinfo,
                          double *__restrict__ damage) {
@@ -487,7 +489,7 @@ __global__ void k_damage(int64_t N, const int64_t *__restrict__ slice_ptr,
         return;
     }
     int32_t n = cnt[p], c = 0;
-    int64_t wb = word_base(slice_ptr, p);
+    const int64_t wb = si[p >> 5].word + (p & 31);
     for (int32_t w = 0; w * 32 < n; ++w) c += __popc(words[wb + 32 * (int64_t)w]);
     damage[p] = 1.0 - (double)c / (double)intact0[p];
 }
@@ -587,9 +589,9 @@ void launch_init_intact(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
     k_init_intact<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, words); pd::note_launch();
 }
 
-void launch_popcount(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+void launch_popcount(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,
                      const uint32_t *words, int32_t *out) {
-    k_popcount<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, words, out); pd::note_launch();
+    k_popcount<<<grid_for(N), kThreads, 0, st>>>(N, si, cnt, words, out); pd::note_launch();
 }
 
 void launch_weighted_volume(cudaStream_t st, const Geo &g, double2 *mth) {
@@ -652,10 +654,10 @@ void launch_gate_multi(cudaStream_t st, const GateItem *items, int nitems, int g
     pd::note_launch();
 }
 
-void launch_damage(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+void launch_damage(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,
                    const uint32_t *words, const int32_t *intact0, const int32_t *tinfo,
                    double *damage) {
-    k_damage<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, words, intact0, tinfo, damage); pd::note_launch();
+    k_damage<<<grid_for(N), kThreads, 0, st>>>(N, si, cnt, words, intact0, tinfo, damage); pd::note_launch();
 }
 
 void launch_sum4(cudaStream_t st, int64_t N, const double4 *a, double *partials, double *out3) {

@@ -88,7 +88,7 @@ struct StepArgs {
     const R *irho, *mass;
     typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
     const int32_t *tinfo, *cnt, *nbr;
-    const int64_t *slice_ptr;
+    const SliceInfo *si;
     uint32_t *words;
     const FBlock<R> *fb;
     const FPair<R> *fp;
@@ -129,19 +129,28 @@ struct Split {
 };
 
 // The index loads of a bond walk depend on nothing, but each thread only
-// has a few of them in flight.  At kernel entry every warp asks L2 for all
-// 128-byte index lines of the chunks it will walk (one line per lane), so
-// the walk's loads hit L2 instead of waiting on HBM one chunk at a time.
+// has a few of them in flight.  At kernel entry every warp of an
+// explicit-index slice asks L2 for all 128-byte index lines of the chunks it
+// will walk (one line per lane), so the walk's loads hit L2 instead of
+// waiting on HBM one chunk at a time.  Stencil slices read no indices.
 template <int WPS>
-__device__ __forceinline__ void prefetch_slice_indices(const int32_t *nbr, const int64_t *slice_ptr, int64_t s,
-                                                       int w, int lane) {
+__device__ __forceinline__ void prefetch_slice_indices(const int32_t *nbr, const SliceInfo *si, int64_t s, int w,
+                                                       int lane) {
     constexpr int CS = Split<WPS>::CS;
-    const int64_t s0 = slice_ptr[s];
-    const int32_t len = (int32_t)((slice_ptr[s + 1] - s0) >> 5);
-    for (int32_t c0 = w * CS; c0 < len; c0 += WPS * CS) {
+    const SliceInfo d = si[s];
+    if (d.mode != kExplicit) return;
+    for (int32_t c0 = w * CS; c0 < d.len; c0 += WPS * CS) {
         const int32_t k = c0 + lane;
-        if (lane < CS && k < len) asm volatile("prefetch.global.L2 [%0];" ::"l"(nbr + s0 + 32 * (int64_t)k));
+        if (lane < CS && k < d.len) asm volatile("prefetch.global.L2 [%0];" ::"l"(nbr + d.nbr + 32 * (int64_t)k));
     }
+}
+
+// Neighbour of slot j of a chunk: explicit slices store one index per
+// (slot, lane); stencil slices one offset per slot, shared by the warp, so
+// the 32 lanes gather 32 consecutive records.
+template <bool ST>
+__device__ __forceinline__ int32_t slot_neighbour(const int32_t *np, int32_t j, int64_t p) {
+    return ST ? (int32_t)p + __ldg(np + j) : __ldg(np + 32 * j);
 }
 
 // Combine the WPS partial sums of one slice without a block barrier: each
@@ -177,22 +186,12 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 // acceleration before the 1/rho scaling.  Every bond appears in both
 // endpoint families and the serial loop adds its term to f_p from both
 // visits, hence the factor 2 (t/|Y| rather than t/(2|Y|)).
-template <class R, int KIND, bool kBreak, int WPS, int U>
-__device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
-                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
-                                            R &fz) {
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST>
+__device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
+                                          uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
+                                          typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz) {
     using V4 = typename Tr<R>::V4;
     constexpr int CS = Split<WPS>::CS;
-    const int32_t n = a.cnt[p];
-    const int64_t sp = a.slice_ptr[p >> 5];
-    const int32_t *nb = a.nbr + sp + (p & 31);
-    uint32_t *wp = a.words + (sp >> 5) + (p & 31);
-    R Ap = 0, Bp = 0;
-    if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
-        typename Tr<R>::V2 m = a.mab[p];
-        Ap = m.x;
-        Bp = m.y;
-    }
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
         uint32_t *wptr = wp + 32 * (w0 >> 5);
@@ -201,13 +200,14 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         if (!bits) continue;
         // Dense walk over the chunk: intact bonds dominate, so testing the
         // bit per bond is cheaper than extracting set bits; the unrolled
-        // iterations' index and neighbour loads overlap.
+        // iterations' index and neighbour loads overlap.  Empty stencil
+        // slots point at an in-range record and carry a 0 bit.
         const int32_t kend = min(CS, n - w0);
-        const int32_t *np = nb + 32 * w0;
+        const int32_t *np = nb + (ST ? 1 : 32) * w0;
         uint32_t brk = 0;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j) {
-            const int32_t q = __ldg(np + 32 * j);
+            const int32_t q = slot_neighbour<ST>(np, j, p);
             const V4 *r = a.xu + 2 * (int64_t)q;
             const V4 xq = r[0];
             const V4 uq = r[1];
@@ -221,8 +221,8 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
             // 2 xi.eta + eta.eta = eta . (xi + Y)
             const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
             const R dl = (ly + lx) * lx;
-            if (B.nt > 1) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             const bool live = (bits >> j) & 1u;
+            if (B.nt > 1 && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             if (!(num < pp.cs * dl)) {
                 if (kBreak && live) brk |= 1u << j;
                 continue;
@@ -244,6 +244,26 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         // bonds break rarely; two warps may own the halves of one word
         if (kBreak && brk) atomicAnd(wptr, ~(CS == 32 ? brk : (brk << (w0 & 31))));
     }
+}
+
+template <class R, int KIND, bool kBreak, int WPS, int U>
+__device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
+                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
+                                            R &fz) {
+    const int32_t n = a.cnt[p];
+    const SliceInfo d = a.si[p >> 5];
+    uint32_t *wp = a.words + d.word + (p & 31);
+    R Ap = 0, Bp = 0;
+    if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
+        typename Tr<R>::V2 m = a.mab[p];
+        Ap = m.x;
+        Bp = m.y;
+    }
+    if (d.mode == kStencil)
+        bond_walk<R, KIND, kBreak, WPS, U, true>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx, fy, fz);
+    else
+        bond_walk<R, KIND, kBreak, WPS, U, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up, Ap, Bp,
+                                                  fx, fy, fz);
 }
 
 // BC velocity (boundary_conditions.jl:122-126): FixBC v = 0, ToFroBC v = dir*rate.
@@ -344,7 +364,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
-    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.slice_ptr, p >> 5, w, lane);
+    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     constexpr bool kBreak = MODE != 5 && MODE != 6;
     R f[3] = {0, 0, 0};
@@ -447,6 +467,37 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     store_u(a, p, u0, u1, u2);
 }
 
+template <class R, int WPS, int U, bool ST>
+__device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
+                                        const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up) {
+    using V4 = typename Tr<R>::V4;
+    constexpr int CS = Split<WPS>::CS;
+    R acc = 0;
+    for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
+        const uint32_t word = wp[32 * (w0 >> 5)];
+        const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+        if (!bits) continue;
+        const int32_t kend = min(CS, n - w0);
+        const int32_t *np = nb + (ST ? 1 : 32) * w0;
+#pragma unroll U
+        for (int32_t j = 0; j < kend; ++j) {
+            const int32_t q = slot_neighbour<ST>(np, j, p);
+            const V4 *r = a.xu + 2 * (int64_t)q;
+            const V4 xq = r[0];
+            const V4 uq = r[1];
+            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
+            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
+            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
+            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
+            const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
+            const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+            if ((bits >> j) & 1u) acc += Tr<R>::div(num, ly + lx) * xq.w;
+        }
+    }
+    return acc;
+}
+
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
 template <class R, int WPS, int U>
@@ -462,38 +513,19 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
-    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.slice_ptr, p >> 5, w, lane);
+    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
     if (lps) {
         const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
         const int32_t n = a.cnt[p];
-        const int64_t sp = a.slice_ptr[p >> 5];
-        const int32_t *nb = a.nbr + sp + (p & 31);
-        const uint32_t *wp = a.words + (sp >> 5) + (p & 31);
-        for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
-            const uint32_t word = wp[32 * (w0 >> 5)];
-            const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
-            if (!bits) continue;
-            const int32_t kend = min(CS, n - w0);
-            const int32_t *np = nb + 32 * w0;
-#pragma unroll U
-            for (int32_t j = 0; j < kend; ++j) {
-                const int32_t q = __ldg(np + 32 * j);
-                const V4 *r = a.xu + 2 * (int64_t)q;
-                const V4 xq = r[0];
-                const V4 uq = r[1];
-                const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
-                const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
-                const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-                const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-                const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-                const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
-                const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
-                if ((bits >> j) & 1u) acc += Tr<R>::div(num, ly + lx) * xq.w;
-            }
-        }
+        const SliceInfo d = a.si[p >> 5];
+        const uint32_t *wp = a.words + d.word + (p & 31);
+        if (d.mode == kStencil)
+            acc = theta_walk<R, WPS, U, true>(a, p, w, n, a.nbr + d.nbr, wp, xp, up);
+        else
+            acc = theta_walk<R, WPS, U, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, xp, up);
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 1>(sh, arrive, wid, lane, &acc)) return;
     if (!lps) return;
@@ -833,7 +865,7 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.tinfo = env->tinfo.p;
     a.cnt = env->cnt.p;
     a.nbr = env->nbr.p;
-    a.slice_ptr = env->slice_ptr.p;
+    a.si = env->sinfo.p;
     a.words = env->words[env->cur].p;
     a.fb = F.fb.p;
     a.fp = F.fp.p;

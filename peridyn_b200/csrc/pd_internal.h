@@ -12,13 +12,15 @@
 //      v[i], f[i], p[i]                     velocity, acceleration, momentum
 //      mth[i] = (m, theta)                  weighted volume, dilatation
 //      tinfo[i] = block << 8 | local type   (-1 for padding)
-//  * Families in SELL-32 form: slice s holds particles 32s..32s+31; the
-//    k-th bond of lane l lives at nbr[slice_ptr[s] + 32k + l] (coalesced
-//    across a warp).  Bonds of a particle are in descending index order,
-//    the reference's family column order (general_material.jl:88-90).
-//    slice lengths are multiples of 32, so slice_ptr[s] is a multiple of
-//    1024 and the intact bit of bond k sits in word
-//    slice_ptr[s]/32 + 32*(k/32) + l, bit k%32.
+//  * Families are built in SELL-32 form ("build layout"): slice s holds
+//    particles 32s..32s+31 and the k-th bond of lane l lives at
+//    nbr[slice_ptr[s] + 32k + l].  Bonds of a particle are in descending
+//    index order, the reference's family column order
+//    (general_material.jl:88-90).
+//  * The step kernels use the "runtime layout" (SliceInfo below): per slice
+//    either one neighbour offset per slot shared by the 32 lanes (stencil)
+//    or the build layout's explicit indices, plus intact and family-member
+//    bit arrays with one 32-bit word per (lane, 32 slots).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -46,6 +48,46 @@ struct DevBlock {
     double3 center;     // FP32C coordinate origin of the block
 };
 
+// Bond storage of one 32-particle slice (runtime layout).  Slot k of lane
+// l is bond k of particle 32s + l; bit k%32 of word
+// words[word + 32*(k/32) + l] is its intact flag (a second array of the same
+// layout marks which slots hold a family member at all).
+//  kExplicit: the neighbour is nbr[nbr + 32k + l] (int32, internal index).
+//  kStencil:  every lane's slot k has the same index offset: the
+//             neighbour is p + nbr[nbr + k].  Slots a particle does not use
+//             are permanently 0 bits.  Warps then gather contiguous
+//             neighbour records and no per-bond index is read at all.
+// Slots are in descending offset order, so each particle meets its bonds in
+// descending neighbour index -- the reference's family order.
+constexpr int kExplicit = 0, kStencil = 1;
+struct SliceInfo {
+    int64_t nbr;   // offset into nbr[]
+    int64_t word;  // offset into the bit arrays
+    int32_t len;   // slots per particle, multiple of 32
+    int32_t mode;  // kExplicit / kStencil
+};
+
+// Access to one particle's bonds.
+struct BondRef {
+    const int32_t *nb;
+    uint32_t *w;
+    int32_t mode;
+    int32_t p;
+    __device__ __forceinline__ int32_t q(int32_t k) const { return mode == kStencil ? p + nb[k] : nb[32 * k]; }
+    __device__ __forceinline__ uint32_t *word(int32_t k) const { return w + 32 * (k >> 5); }
+};
+
+__device__ __forceinline__ BondRef bond_ref(const SliceInfo *si, const int32_t *nbr, const uint32_t *words,
+                                            int64_t p) {
+    const SliceInfo s = si[p >> 5];
+    BondRef b;
+    b.mode = s.mode;
+    b.p = (int32_t)p;
+    b.nb = nbr + s.nbr + (s.mode == kStencil ? 0 : (p & 31));
+    b.w = const_cast<uint32_t *>(words) + s.word + (p & 31);
+    return b;
+}
+
 struct PairParam {
     double cs;    // critical stretch
     double k35;   // 3K - 5G   (LPS)
@@ -61,9 +103,10 @@ struct Geo {
     const DevBlock *blocks;
     const PairParam *pairs;
     const double *tdens;       // per block-type density
-    const int64_t *slice_ptr;  // N/32 entries
-    const int32_t *cnt;        // bonds per particle
-    const int32_t *nbr;        // SELL neighbour indices (internal)
+    const SliceInfo *si;       // N/32 slice descriptors
+    const int32_t *cnt;        // slots to scan per particle
+    const int32_t *nbr;        // bond index data (see SliceInfo)
+    const uint32_t *fam;       // family-member bits (same layout as intact)
     const int32_t *deformed;   // per block
 };
 
@@ -97,7 +140,8 @@ void launch_sort_neighbors(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                            const int32_t *cnt, int32_t *nbr);
 void launch_init_intact(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                         const int32_t *cnt, uint32_t *words);
-void launch_popcount(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+// Runtime layout (SliceInfo) from here on.
+void launch_popcount(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,
                      const uint32_t *words, int32_t *out);
 void launch_weighted_volume(cudaStream_t st, const Geo &g, double2 *mth);
 
@@ -129,7 +173,7 @@ void launch_gate_multi(cudaStream_t st, const GateItem *items, int nitems, int g
                        const double4 *y, double *partials, int32_t *deformed);
 
 // Damage / diagnostics.
-void launch_damage(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+void launch_damage(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,
                    const uint32_t *words, const int32_t *intact0, const int32_t *tinfo,
                    double *damage);
 void launch_sum4(cudaStream_t st, int64_t N, const double4 *a, double *partials, double *out3);

@@ -103,7 +103,7 @@ extern "C" pd_status pd_force_density_device_static(pd_env *env, int64_t block, 
     // force_density_T! has no deformed gate: mark the block active
     CK(cudaMemcpyAsync(env->deformed.p + block, &kOne, sizeof(int32_t), cudaMemcpyHostToDevice, st));
     launch_force_serial(st, g, ys, env->mth.p, env->words[env->cur].p, env->words[1 - env->cur].p, fs, 1, p0, p1);
-    const int64_t w0 = env->slice_ptr_h[p0 / 32] / 32, w1 = env->slice_ptr_h[p1 / 32] / 32;
+    const int64_t w0 = env->sinfo_h[p0 / 32].word, w1 = env->sinfo_h[p1 / 32].word;
     if (w1 > w0)
         CK(cudaMemcpyAsync(env->words[env->cur].p + w0, env->words[1 - env->cur].p + w0, (w1 - w0) * sizeof(uint32_t),
                            cudaMemcpyDeviceToDevice, st));

@@ -26,7 +26,8 @@ void pd_env::release_device() {
     cnt.reset();
     intact0.reset();
     deformed.reset();
-    slice_ptr.reset();
+    sinfo.reset();
+    fam.reset();
     nbr.reset();
     words[0].reset();
     words[1].reset();
@@ -361,7 +362,7 @@ extern "C" pd_status pd_force_density_device(pd_env *env, int64_t block, double 
     CK(cudaMemcpyAsync(env->deformed.p + block, one.data(), 4, cudaMemcpyHostToDevice, st));
     launch_force_serial(st, g, env->tmp_y.p, env->mth.p, env->words[env->cur].p, env->words[1 - env->cur].p,
                         env->tmp_f.p, 1, p0, p1);
-    int64_t w0 = env->slice_ptr_h[p0 / 32] / 32, w1 = env->slice_ptr_h[p1 / 32] / 32;
+    int64_t w0 = env->sinfo_h[p0 / 32].word, w1 = env->sinfo_h[p1 / 32].word;
     if (w1 > w0)
         CK(cudaMemcpyAsync(env->words[env->cur].p + w0, env->words[1 - env->cur].p + w0, (w1 - w0) * 4,
                            cudaMemcpyDeviceToDevice, st));

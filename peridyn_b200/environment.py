@@ -177,6 +177,13 @@ class GeneralEnvironment:
         _abi.check(_abi.lib().pd_env_deformed(self._h, _abi.u8ptr(flags)))
         return flags.astype(bool)
 
+    def layout(self):
+        """Bond storage: slices, stencil slices, bond slots, index entries."""
+        out = np.zeros(4, dtype=np.int64)
+        _abi.check(_abi.lib().pd_env_layout(self._h, _abi.i64ptr(out)))
+        return {"slices": int(out[0]), "stencil_slices": int(out[1]), "slots": int(out[2]),
+                "index_entries": int(out[3])}
+
 
 def Env(id, materials, short_range_contact, boundary_conds, dt, state=2, bskin=0.5, units=False, **kwargs):
     """environment.jl:166-235 ``Env(id, materials, short_range_contact,

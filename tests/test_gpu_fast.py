@@ -9,6 +9,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import configs, lattice
+from tests.cases import random_cloud
 
 pytestmark = pytest.mark.gpu
 
@@ -43,12 +44,18 @@ def _errors(env, ora):
     return eu, ev, mism
 
 
+@pytest.mark.parametrize("layout", ["auto", "explicit"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
 @pytest.mark.parametrize("builder,nsteps", [
     (lambda: configs.pmb_cube(n=12, peak=20.0), 200),
     (lambda: configs.lps_bar(nx=40, ny=10, nz=10), 300),
+    (random_cloud, 100),
 ])
-def test_trajectory_error_bound(oracle, precision, builder, nsteps):
+def test_trajectory_error_bound(oracle, precision, builder, nsteps, layout, monkeypatch):
+    if layout == "explicit":
+        monkeypatch.setenv("PD_FAMILY_LAYOUT", "explicit")
+    else:
+        monkeypatch.delenv("PD_FAMILY_LAYOUT", raising=False)
     w = builder()
     env, ora = _run_pair(oracle, w, precision, nsteps)
     eu, ev, mism = _errors(env, ora)

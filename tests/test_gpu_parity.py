@@ -8,8 +8,28 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import _abi, configs, lattice
+from tests.cases import random_cloud
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["auto", "explicit"])
+def layout(request, monkeypatch):
+    """Bond storage form chosen at finalize: per-slice stencil where the
+    offsets allow it ("auto") or explicit indices everywhere."""
+    if request.param == "explicit":
+        monkeypatch.setenv("PD_FAMILY_LAYOUT", "explicit")
+    else:
+        monkeypatch.delenv("PD_FAMILY_LAYOUT", raising=False)
+    return request.param
+
+
+def _check_layout(env, layout):
+    st = env.layout()
+    if layout == "explicit":
+        assert st["stencil_slices"] == 0
+    else:
+        assert st["stencil_slices"] > 0
 
 
 def _pair(oracle, w, precision="fp64_serial", families=None):
@@ -50,9 +70,10 @@ def multitype_block():
 
 @pytest.mark.parametrize("builder", [lambda: configs.pmb_cube(n=11), small_bar, multitype_block,
                                      lambda: configs.batched_cubes(nspec=5, edge_lo=5, edge_hi=9)])
-def test_family_weighted_volume_bit_exact(oracle, builder):
+def test_family_weighted_volume_bit_exact(oracle, builder, layout):
     w = builder()
     env, ora = _pair(oracle, w)
+    _check_layout(env, layout)
     _assert_bonds_equal(env, ora)
     for b, B in enumerate(ora.blocks):
         assert np.array_equal(w["materials"][b].general.weighted_volume, B.m)
@@ -71,9 +92,29 @@ def test_knife_edge_exact_lattice_counts(oracle):
 
 
 @pytest.mark.parametrize("builder", [lambda: configs.pmb_cube(n=10), small_bar, multitype_block])
-def test_update_acc_bit_exact_with_breaking(oracle, builder):
+def test_update_acc_bit_exact_with_breaking(oracle, builder, layout):
     w = builder()
     env, ora = _pair(oracle, w)
+    _check_layout(env, layout)
+    _update_acc_with_breaking(env, ora)
+    env.close()
+
+
+def test_update_acc_disordered_cloud(oracle):
+    w = random_cloud()
+    env, ora = _pair(oracle, w)
+    st = env.layout()
+    assert st["stencil_slices"] < st["slices"] // 4
+    _update_acc_with_breaking(env, ora)
+    for _ in range(10):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=10)
+    _assert_state_equal(env, ora)
+    _assert_bonds_equal(env, ora)
+    env.close()
+
+
+def _update_acc_with_breaking(env, ora):
     rng = np.random.default_rng(1)
     y = ora.y + rng.normal(0.0, 4e-6, size=ora.y.shape)
     ora.y[:] = y
@@ -89,14 +130,14 @@ def test_update_acc_bit_exact_with_breaking(oracle, builder):
         if B.kind == 1:
             assert np.array_equal(env.theta(b), B.theta)
     assert np.array_equal(pb.cal_damage(env), ora.damage())
-    env.close()
 
 
 @pytest.mark.parametrize("builder,nsteps", [(lambda: configs.pmb_cube(n=10, peak=60.0), 60), (small_bar, 60),
                                             (multitype_block, 30)])
-def test_velocity_verlet_trajectory_bit_exact(oracle, builder, nsteps):
+def test_velocity_verlet_trajectory_bit_exact(oracle, builder, nsteps, layout):
     w = builder()
     env, ora = _pair(oracle, w)
+    _check_layout(env, layout)
     ora.update_acc()
     pb.update_acc(env)
     ora.apply_bc_at0()
@@ -217,7 +258,7 @@ def test_contact12_neighbours_and_forces_bit_exact(oracle):
     env.close()
 
 
-def test_contact11_self_contact_bit_exact(oracle):
+def test_contact11_self_contact_bit_exact(oracle, layout):
     x, vol = lattice.cuboid(8, 8, 6, 1e-3, jitter=3e-5, seed=2)
     fam, intact = oracle.cal_family(x, 3.015e-3, 200)
     rng = np.random.default_rng(8)
@@ -243,6 +284,7 @@ def test_contact11_self_contact_bit_exact(oracle):
     cm = pb.LinearSpringContactModel(1e18, mat, distanceX=5, max_neighs=20)
     w = {"materials": [mat], "contacts": [cm], "bcs": [], "dt": 1e-9}
     env, ora = _pair(oracle, w, families=[(fam, intact)])
+    _check_layout(env, layout)
     hits = 0
     for _ in range(8):
         ora.update_neighs()
