@@ -46,6 +46,13 @@ struct Tr<float> {
     using V2 = float2;
     static __device__ __forceinline__ float rsq(float a) { return rsqrtf(a); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    // One 256-bit load of a particle record (x, volume | u, -); the record
+    // buffer is not written while a kernel reads it.
+    static __device__ __forceinline__ void load_rec(const float4 *r, float4 &x, float4 &u) {
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
+            : "l"(r));
+    }
 };
 template <>
 struct Tr<double> {
@@ -53,6 +60,10 @@ struct Tr<double> {
     using V2 = double2;
     static __device__ __forceinline__ double rsq(double a) { return rsqrt(a); }
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ void load_rec(const double4 *r, double4 &x, double4 &u) {
+        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w) : "l"(r));
+        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r + 1));
+    }
 };
 
 template <class R>
@@ -186,7 +197,7 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 // acceleration before the 1/rho scaling.  Every bond appears in both
 // endpoint families and the serial loop adds its term to f_p from both
 // visits, hence the factor 2 (t/|Y| rather than t/(2|Y|)).
-template <class R, int KIND, bool kBreak, int WPS, int U, bool ST>
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
                                           typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz) {
@@ -198,19 +209,18 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
         const uint32_t word = *wptr;
         const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
         if (!bits) continue;
-        // Dense walk over the chunk: intact bonds dominate, so testing the
-        // bit per bond is cheaper than extracting set bits; the unrolled
-        // iterations' index and neighbour loads overlap.  Empty stencil
-        // slots point at an in-range record and carry a 0 bit.
+        // Dense, branch-free walk over the chunk: intact bonds dominate, so
+        // every slot is evaluated and its term selected by its bit; the
+        // unrolled iterations' index and neighbour loads overlap.  Empty
+        // stencil slots point at an in-range record and carry a 0 bit.
         const int32_t kend = min(CS, n - w0);
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         uint32_t brk = 0;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
-            const V4 *r = a.xu + 2 * (int64_t)q;
-            const V4 xq = r[0];
-            const V4 uq = r[1];
+            V4 xq, uq;
+            Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
             const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
             const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
             const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
@@ -222,12 +232,9 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
             const R dl = (ly + lx) * lx;
             const bool live = (bits >> j) & 1u;
-            if (B.nt > 1 && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
-            if (!(num < pp.cs * dl)) {
-                if (kBreak && live) brk |= 1u << j;
-                continue;
-            }
-            if (!live) continue;
+            if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
+            const bool ok = num < pp.cs * dl;
+            if (kBreak) brk |= (uint32_t)(live && !ok) << j;
             const R s = Tr<R>::div(num, dl);
             R t;
             if (KIND == PD_MAT_BOND_BASED) {
@@ -236,7 +243,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
                 typename Tr<R>::V2 mq = a.mab[q];
                 t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
             }
-            const R coef = t * ry * xq.w;
+            const R coef = (live && ok) ? t * ry * xq.w : R(0);
             fx += coef * Y0;
             fy += coef * Y1;
             fz += coef * Y2;
@@ -259,11 +266,21 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         Ap = m.x;
         Bp = m.y;
     }
-    if (d.mode == kStencil)
-        bond_walk<R, KIND, kBreak, WPS, U, true>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx, fy, fz);
-    else
-        bond_walk<R, KIND, kBreak, WPS, U, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up, Ap, Bp,
-                                                  fx, fy, fz);
+    if (B.nt > 1) {
+        if (d.mode == kStencil)
+            bond_walk<R, KIND, kBreak, WPS, U, true, true>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+                                                           fy, fz);
+        else
+            bond_walk<R, KIND, kBreak, WPS, U, false, true>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
+                                                            Ap, Bp, fx, fy, fz);
+    } else {
+        if (d.mode == kStencil)
+            bond_walk<R, KIND, kBreak, WPS, U, true, false>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+                                                            fy, fz);
+        else
+            bond_walk<R, KIND, kBreak, WPS, U, false, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
+                                                             up, Ap, Bp, fx, fy, fz);
+    }
 }
 
 // BC velocity (boundary_conditions.jl:122-126): FixBC v = 0, ToFroBC v = dir*rate.
@@ -372,7 +389,8 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         const int b = ti >> 8, tp = ti & 255;
         const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
-            const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
+            V4 xp, up;
+            Tr<R>::load_rec(a.xu + 2 * p, xp, up);
             if (B.kind == PD_MAT_BOND_BASED)
                 bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
             else
@@ -482,9 +500,8 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
-            const V4 *r = a.xu + 2 * (int64_t)q;
-            const V4 xq = r[0];
-            const V4 uq = r[1];
+            V4 xq, uq;
+            Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
             const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
             const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
             const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
@@ -518,7 +535,8 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
     if (lps) {
-        const V4 xp = a.xu[2 * p], up = a.xu[2 * p + 1];
+        V4 xp, up;
+        Tr<R>::load_rec(a.xu + 2 * p, xp, up);
         const int32_t n = a.cnt[p];
         const SliceInfo d = a.si[p >> 5];
         const uint32_t *wp = a.words + d.word + (p & 31);
