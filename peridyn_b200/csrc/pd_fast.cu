@@ -215,9 +215,9 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
         // stencil slots point at an in-range record and carry a 0 bit.
         const int32_t kend = min(CS, n - w0);
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
-        uint32_t brk = 0;
+        uint32_t okm = 0, bit = 1u;  // okm: slots within the critical stretch
 #pragma unroll U
-        for (int32_t j = 0; j < kend; ++j) {
+        for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
             Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
@@ -231,14 +231,15 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             // 2 xi.eta + eta.eta = eta . (xi + Y)
             const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
             const R dl = (ly + lx) * lx;
-            const bool live = (bits >> j) & 1u;
+            const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             const bool ok = num < pp.cs * dl;
-            if (kBreak) brk |= (uint32_t)(live && !ok) << j;
+            if (kBreak) okm |= ok ? bit : 0u;
             const R s = Tr<R>::div(num, dl);
+            // bond-based records carry c * V in w (k_import), so t = s there
             R t;
             if (KIND == PD_MAT_BOND_BASED) {
-                t = B.c11 * s;
+                t = s;
             } else {
                 typename Tr<R>::V2 mq = a.mab[q];
                 t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
@@ -249,6 +250,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             fz += coef * Y2;
         }
         // bonds break rarely; two warps may own the halves of one word
+        const uint32_t brk = bits & ~okm;
         if (kBreak && brk) atomicAnd(wptr, ~(CS == 32 ? brk : (brk << (w0 & 31))));
     }
 }
@@ -620,11 +622,14 @@ __global__ void k_import(int64_t N, const double4 *x4, const double4 *y, const d
     const double u0 = yi.x - xi.x, u1 = yi.y - xi.y, u2 = yi.z - xi.z;
     V4 xs;
     const int32_t ti = tinfo[p];
+    // w: the volume, times the bond constant c in bond-based blocks (the
+    // bond walk then needs no per-bond multiply by c)
+    const double wv = (ti >= 0 && blocks[ti >> 8].kind == PD_MAT_BOND_BASED) ? blocks[ti >> 8].c11 * xi.w : xi.w;
     if (sizeof(R) == 4 && ti >= 0) {
         const double3 c = blocks[ti >> 8].center;
-        xs = V4{(R)(xi.x - c.x), (R)(xi.y - c.y), (R)(xi.z - c.z), (R)xi.w};
+        xs = V4{(R)(xi.x - c.x), (R)(xi.y - c.y), (R)(xi.z - c.z), (R)wv};
     } else {
-        xs = V4{(R)xi.x, (R)xi.y, (R)xi.z, (R)xi.w};
+        xs = V4{(R)xi.x, (R)xi.y, (R)xi.z, (R)wv};
     }
     if (sizeof(R) == 4) {
         a.ax[p] = u0;
