@@ -46,6 +46,17 @@ struct Tr<float> {
     using V2 = float2;
     static __device__ __forceinline__ float rsq(float a) { return rsqrtf(a); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    // single-instruction approximations (relative error of order 2^-22)
+    static __device__ __forceinline__ float sqrt_(float a) {
+        float r;
+        asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+        return r;
+    }
+    static __device__ __forceinline__ float rcp(float a) {
+        float r;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+        return r;
+    }
     // One 256-bit load of a particle record (x, volume | u, -); the record
     // buffer is not written while a kernel reads it.
     static __device__ __forceinline__ void load_rec(const float4 *r, float4 &x, float4 &u) {
@@ -60,6 +71,8 @@ struct Tr<double> {
     using V2 = double2;
     static __device__ __forceinline__ double rsq(double a) { return rsqrt(a); }
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double sqrt_(double a) { return sqrt(a); }
+    static __device__ __forceinline__ double rcp(double a) { return 1.0 / a; }
     static __device__ __forceinline__ void load_rec(const double4 *r, double4 &x, double4 &u) {
         asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w) : "l"(r));
         asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r + 1));
@@ -226,25 +239,24 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
             const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
             const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R rx = Tr<R>::rsq(xx2), ry = Tr<R>::rsq(yy2);
-            const R lx = xx2 * rx, ly = yy2 * ry;
-            // 2 xi.eta + eta.eta = eta . (xi + Y)
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(yy2);
+            // 2 xi.eta + eta.eta = eta . (xi + Y);  stretch s = num / dl
             const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
-            const R dl = (ly + lx) * lx;
+            const R dl = ly * lx + xx2;  // (|Y| + |xi|) |xi|
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             const bool ok = num < pp.cs * dl;
             if (kBreak) okm |= ok ? bit : 0u;
-            const R s = Tr<R>::div(num, dl);
-            // bond-based records carry c * V in w (k_import), so t = s there
-            R t;
+            // coef = t V / |Y| with t * dl accumulated in tn; bond-based
+            // records carry c V in w (k_import), so tn = num there
+            R tn;
             if (KIND == PD_MAT_BOND_BASED) {
-                t = s;
+                tn = num;
             } else {
                 typename Tr<R>::V2 mq = a.mab[q];
-                t = pp.k35 * (Ap + mq.x) + pp.g15 * s * (Bp + mq.y);
+                tn = pp.k35 * (Ap + mq.x) * dl + pp.g15 * num * (Bp + mq.y);
             }
-            const R coef = (live && ok) ? t * ry * xq.w : R(0);
+            const R coef = (live && ok) ? tn * xq.w * Tr<R>::rcp(dl * ly) : R(0);
             fx += coef * Y0;
             fy += coef * Y1;
             fz += coef * Y2;
@@ -499,8 +511,9 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
         if (!bits) continue;
         const int32_t kend = min(CS, n - w0);
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
+        uint32_t bit = 1u;
 #pragma unroll U
-        for (int32_t j = 0; j < kend; ++j) {
+        for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
             Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
@@ -509,9 +522,10 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
             const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
             const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
             const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R lx = xx2 * Tr<R>::rsq(xx2), ly = yy2 * Tr<R>::rsq(yy2);
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(yy2);
             const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
-            if ((bits >> j) & 1u) acc += Tr<R>::div(num, ly + lx) * xq.w;
+            const R term = num * xq.w * Tr<R>::rcp(ly + lx);
+            acc += (bits & bit) ? term : R(0);
         }
     }
     return acc;
