@@ -210,6 +210,44 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 // acceleration before the 1/rho scaling.  Every bond appears in both
 // endpoint families and the serial loop adds its term to f_p from both
 // visits, hence the factor 2 (t/|Y| rather than t/(2|Y|)).
+// Bond kinematics from the neighbour record (xq, uq) and the negated own
+// record (nx, nu): deformed bond vector Y = xi + eta, |xi|^2 and the
+// cancellation-free stretch numerator num = eta . (xi + Y) = |Y|^2 - |xi|^2.
+template <class R>
+struct Kin {
+    R Y0, Y1, Y2, xx2, num;
+    __device__ __forceinline__ Kin(const typename Tr<R>::V4 &xq, const typename Tr<R>::V4 &uq,
+                                   const typename Tr<R>::V4 &nx, const typename Tr<R>::V4 &nu) {
+        const R x0 = xq.x + nx.x, x1 = xq.y + nx.y, x2 = xq.z + nx.z;
+        const R e0 = uq.x + nu.x, e1 = uq.y + nu.y, e2 = uq.z + nu.z;
+        Y0 = x0 + e0;
+        Y1 = x1 + e1;
+        Y2 = x2 + e2;
+        xx2 = x0 * x0 + x1 * x1 + x2 * x2;
+        num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+    }
+};
+// FP32: the (x, y) components as packed f32x2 operations.
+template <>
+struct Kin<float> {
+    float Y0, Y1, Y2, xx2, num;
+    __device__ __forceinline__ Kin(const float4 &xq, const float4 &uq, const float4 &nx, const float4 &nu) {
+        const float2 d = __fadd2_rn(make_float2(xq.x, xq.y), make_float2(nx.x, nx.y));
+        const float2 e = __fadd2_rn(make_float2(uq.x, uq.y), make_float2(nu.x, nu.y));
+        const float dz = xq.z + nx.z, ez = uq.z + nu.z;
+        const float2 Y = __fadd2_rn(d, e);
+        const float Yz = dz + ez;
+        const float2 S = __fadd2_rn(d, Y);
+        const float2 dd = __fmul2_rn(d, d);
+        const float2 es = __fmul2_rn(e, S);
+        xx2 = fmaf(dz, dz, dd.x + dd.y);
+        num = fmaf(ez, dz + Yz, es.x + es.y);
+        Y0 = Y.x;
+        Y1 = Y.y;
+        Y2 = Yz;
+    }
+};
+
 template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
@@ -217,6 +255,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
     using V4 = typename Tr<R>::V4;
     constexpr int CS = Split<WPS>::CS;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
+    const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
     for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
         uint32_t *wptr = wp + 32 * (w0 >> 5);
         const uint32_t word = *wptr;
@@ -234,14 +273,10 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
             Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
-            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
-            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
-            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(yy2);
-            // 2 xi.eta + eta.eta = eta . (xi + Y);  stretch s = num / dl
-            const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+            const Kin<R> k(xq, uq, nx, nu);
+            const R num = k.num, xx2 = k.xx2;
+            // stretch s = num / dl;  |Y|^2 = |xi|^2 + num
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
             const R dl = ly * lx + xx2;  // (|Y| + |xi|) |xi|
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
@@ -257,9 +292,9 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
                 tn = pp.k35 * (Ap + mq.x) * dl + pp.g15 * num * (Bp + mq.y);
             }
             const R coef = (live && ok) ? tn * xq.w * Tr<R>::rcp(dl * ly) : R(0);
-            fx += coef * Y0;
-            fy += coef * Y1;
-            fz += coef * Y2;
+            fx += coef * k.Y0;
+            fy += coef * k.Y1;
+            fz += coef * k.Y2;
         }
         // bonds break rarely; two warps may own the halves of one word
         const uint32_t brk = bits & ~okm;
@@ -505,6 +540,7 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
     using V4 = typename Tr<R>::V4;
     constexpr int CS = Split<WPS>::CS;
     R acc = 0;
+    const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
     for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
         const uint32_t word = wp[32 * (w0 >> 5)];
         const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
@@ -517,13 +553,9 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
             Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
-            const R x0 = xq.x - xp.x, x1 = xq.y - xp.y, x2 = xq.z - xp.z;
-            const R e0 = uq.x - up.x, e1 = uq.y - up.y, e2 = uq.z - up.z;
-            const R Y0 = x0 + e0, Y1 = x1 + e1, Y2 = x2 + e2;
-            const R xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-            const R yy2 = Y0 * Y0 + Y1 * Y1 + Y2 * Y2;
-            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(yy2);
-            const R num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+            const Kin<R> k(xq, uq, nx, nu);
+            const R num = k.num;
+            const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
             const R term = num * xq.w * Tr<R>::rcp(ly + lx);
             acc += (bits & bit) ? term : R(0);
         }
