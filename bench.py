@@ -55,10 +55,13 @@ def build_workload(name, args):
     raise SystemExit(f"unknown workload {name}")
 
 
-# Algorithmic bytes of one bond-force launch: per intact directed bond the
-# int32 neighbour index plus one intact bit; per particle the state the
-# kernel must stream (listed per precision below).
-BOND_BYTES = 4.125
+# Algorithmic bytes of one bond-force launch: the bond storage the walk must
+# read (one intact bit per bond slot plus the neighbour-index array: one
+# int32 per (slot, particle) in explicit slices, one per slot in stencil
+# slices) and per particle the state the kernel streams (listed per
+# precision below).
+def bond_bytes(layout):
+    return layout["slots"] / 8.0 + 4.0 * layout["index_entries"]
 
 
 def particle_bytes(precision, lps):
@@ -179,6 +182,54 @@ def traffic_for(workload, precision):
         return None
 
 
+def time_precision(work, precision, sim_steps, device, flush, dist):
+    """The same workload on another precision path: 1 warm-up and 2 timed
+    runs, timed like the main measurement."""
+    import torch
+
+    import peridyn_b200 as pb
+    from peridyn_b200 import _abi
+
+    env = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision=precision,
+                 device=device)
+    L = _abi.lib()
+    sp = ctypes_void()
+    _abi.check(L.pd_env_stream(env._h, ctypes.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", device))
+    y0, v0, _, _ = env.get_state()
+    t_total, bonds = 0.0, 0.0
+    for k in range(3):
+        env.set_state(y=y0, v=v0, f=np.zeros_like(y0))
+        _abi.check(L.pd_env_reset_bonds(env._h))
+        _abi.check(L.pd_env_reset_deformed(env._h))
+        env.time_step = 0
+        if work["bcs"]:
+            pb.apply_bc_at0(env, 0)
+        pb.update_neighs(env)
+        pb.update_acc(env)
+        b0 = env.num_bonds()
+        flush.zero_()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _abi.check(L.pd_env_vv_steps(env._h, sim_steps))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k > 0:
+            t_total += e0.elapsed_time(e1) / 1e3
+            bonds += 0.5 * (b0 + env.num_bonds()) * sim_steps
+    env.close()
+    if dist is not None:
+        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+    return {"precision": precision, "value": bonds / t_total, "unit": UNIT, "ms_per_step": 1e3 * t_total / 2,
+            "steps": 2, "warmup": 1}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -211,7 +262,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="lps_bar", choices=["lps_bar", "pmb_cube", "batched", "disk_impact"])
-    ap.add_argument("--precision", default="fp64_serial", choices=["fp64_serial", "fp64", "fp32c"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp64_serial", "fp64", "fp32c"])
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip timing the plain FP64 GPU path beside an FP32C run")
     ap.add_argument("--sim-steps", type=int, default=0, help="VV steps per bench step (default: workload's)")
     ap.add_argument("--nspec", type=int, default=256)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
@@ -278,10 +331,12 @@ def main():
     times = []
     bonds = []
     launches0 = _abi.kernel_launches()
-    _abi.check(L.pd_env_profile(env._h, 1))
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
+        for k in range(args.steps):
             reset()
+            if k == args.steps - 1:
+                # per-launch events around the bond kernel in the last timed step
+                _abi.check(L.pd_env_profile(env._h, 1))
             b0 = env.num_bonds()
             flush.zero_()
             torch.cuda.synchronize()
@@ -355,7 +410,8 @@ def main():
         accuracy = accuracy_vs_serial(work, args.precision, sim_steps, env, local)
     # roofline of the bond-force kernel
     n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
-    bytes_launch = bonds_start * BOND_BYTES + n_int * particle_bytes(args.precision, lps)
+    layout = env.layout()
+    bytes_launch = bond_bytes(layout) + n_int * particle_bytes(args.precision, lps)
     avg_ms = prof_ms.value / max(1, prof_n.value)
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
     peaks = {}
@@ -367,6 +423,9 @@ def main():
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     traffic = traffic_for(work["workload"], args.precision)
     clk = clocks.summary()
+    fp64_cmp = None
+    if args.precision == "fp32c" and not args.no_fp64_compare:  # every rank: it holds collectives
+        fp64_cmp = time_precision(work, "fp64", sim_steps, local, flush, dist)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -393,6 +452,9 @@ def main():
         "clocks": clk,
         "accuracy": accuracy,
     }
+    line["config"]["bond_layout"] = layout
+    if fp64_cmp is not None:
+        line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:
         rate, n, dt = cpu_sample(work, args.cpu_sample_s, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",

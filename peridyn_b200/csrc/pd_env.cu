@@ -36,6 +36,8 @@ pd_status fail(pd_status s, const char *fmt, ...) {
 }
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void prof_begin(pd_env *env, cudaStream_t st) {
     if (!env->prof) return;

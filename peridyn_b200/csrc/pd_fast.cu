@@ -861,7 +861,28 @@ struct Fast {
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     int cur = 0;
     int wps = 0;          // warps per 32-particle slice (autotuned)
+    // CUDA graphs of kGraphSteps velocity-Verlet steps, keyed by the first
+    // step's arguments (buffer parity, BC directions) and the gate list.
+    struct Graph {
+        StepArgs<R> a0;
+        std::vector<GateItem> gate;
+        int wps;
+        int64_t kernels;  // kernel nodes per replay
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    // pinned copy of the device gate flags, read back without stalling
+    int32_t *flags_h = nullptr;
+    cudaEvent_t flags_ev = nullptr;
+    bool flags_pending = false;
+    ~Fast() {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        if (flags_h) cudaFreeHost(flags_h);
+        if (flags_ev) cudaEventDestroy(flags_ev);
+    }
 };
+constexpr int kGraphSteps = 32;
+static_assert(kGraphSteps % 2 == 0, "a replay must keep the record-buffer parity");
 
 // Kernel shape, chosen by the autotuner: cfg = 10 * WPS + U (warps per
 // slice, bonds in flight per thread).  FP32 tries U in {2, 4}, FP64 {1, 2}.
@@ -918,7 +939,8 @@ FastHolder *holder(pd_env *env) { return (FastHolder *)env->fast; }
 
 template <class R>
 StepArgs<R> args(pd_env *env, Fast<R> &F) {
-    StepArgs<R> a{};
+    StepArgs<R> a;
+    std::memset(&a, 0, sizeof(a));  // byte-comparable (graph cache keys)
     a.N = env->N;
     a.xu = F.xu[F.cur].p;
     a.xn = F.xu[1 - F.cur].p;
@@ -1023,29 +1045,76 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
 }
 
 template <class R>
-pd_status gate_if_needed(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
+pd_status gate_prepare(pd_env *env, Fast<R> &F) {
     std::vector<GateItem> items;
     for (size_t b = 0; b < env->hb.size(); ++b) {
         const HostBlock &hb = env->hb[b];
         if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
         items.push_back(GateItem{hb.first_int, hb.n, (int32_t)b, 0});
     }
-    if (items.empty()) return PD_OK;
-    const int ni = (int)items.size();
-    const int gx = std::max(1, std::min(kGB, (kGB * 8) / ni));
     if (F.gitems_h.size() != items.size() ||
         std::memcmp(F.gitems_h.data(), items.data(), items.size() * sizeof(GateItem)) != 0) {
-        PD_TRY(F.gitems.alloc(items.size()));
-        PD_TRY(F.gpart.alloc(3 * (size_t)ni * gx));
-        CK(cudaMemcpyAsync(F.gitems.p, items.data(), items.size() * sizeof(GateItem), cudaMemcpyHostToDevice,
-                           env->st));
-        CK(cudaStreamSynchronize(env->st));
+        if (!items.empty()) {
+            const int ni = (int)items.size();
+            const int gx = std::max(1, std::min(kGB, (kGB * 8) / ni));
+            PD_TRY(F.gitems.alloc(items.size()));
+            PD_TRY(F.gpart.alloc(3 * (size_t)ni * gx));
+            CK(cudaMemcpyAsync(F.gitems.p, items.data(), items.size() * sizeof(GateItem), cudaMemcpyHostToDevice,
+                               env->st));
+            CK(cudaStreamSynchronize(env->st));
+        }
         F.gitems_h = items;
     }
+    return PD_OK;
+}
+
+// Deformed gate of the blocks in F.gitems_h (prepared by gate_prepare):
+// kernel launches only, so it can be captured in a graph.
+template <class R>
+void gate_launch(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
+    if (F.gitems_h.empty()) return;
+    const int ni = (int)F.gitems_h.size();
+    const int gx = std::max(1, std::min(kGB, (kGB * 8) / ni));
     k_fgate_partial<R><<<dim3(gx, ni), kGT, 0, env->st>>>(a, F.gitems.p, gx, F.gpart.p);
     k_fgate_final<<<(ni + 127) / 128, 128, 0, env->st>>>(F.gitems.p, ni, gx, F.gpart.p, env->deformed.p);
     note_launch();
     note_launch();
+}
+
+template <class R>
+pd_status gate_if_needed(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
+    PD_TRY(gate_prepare(env, F));
+    gate_launch(env, a, F);
+    return PD_OK;
+}
+
+// Non-blocking refresh of the host copy of the gate flags: issue an async
+// read-back, and take its result on a later call once it has landed.
+template <class R>
+pd_status poll_gate_flags(pd_env *env, Fast<R> &F) {
+    if (F.gitems_h.empty()) return PD_OK;
+    const size_t nb = env->hb.size();
+    if (!F.flags_h) {
+        CK(cudaMallocHost(&F.flags_h, nb * sizeof(int32_t)));
+        CK(cudaEventCreateWithFlags(&F.flags_ev, cudaEventDisableTiming));
+    }
+    if (F.flags_pending) {
+        const cudaError_t q = cudaEventQuery(F.flags_ev);
+        if (q == cudaErrorNotReady) return PD_OK;
+        if (q != cudaSuccess) return cuda_fail(q, "gate flag read-back", __FILE__, __LINE__);
+        F.flags_pending = false;
+        // drop the gate once every listed block has deformed (a partial
+        // change would only cost a re-capture; the kernels skip deformed
+        // blocks by themselves)
+        for (const GateItem &it : F.gitems_h)
+            if (!F.flags_h[it.block]) return PD_OK;
+        for (size_t b = 0; b < nb; ++b)
+            if (F.flags_h[b]) env->deformed_h[b] = 1;
+        return gate_prepare(env, F);
+    }
+    CK(cudaMemcpyAsync(F.flags_h, env->deformed.p, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaEventRecord(F.flags_ev, env->st));
+    F.flags_pending = true;
     return PD_OK;
 }
 
@@ -1169,6 +1238,79 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     return PD_OK;
 }
 
+// check!(env) then time_step += 1 (velocity_verlet.jl:81-85): ToFro
+// direction flips when time_step > applyafter and time_step % freq == 0.
+void advance_bc_clock(pd_env *env) {
+    for (auto &h : env->hbc) {
+        if (h.kind != PD_BC_TOFRO) continue;
+        const double r = std::fmod((double)env->ts, h.freq);
+        if ((env->ts > h.applyafter) && (r == 0.0)) h.dir = -h.dir;
+    }
+    env->ts += 1;
+}
+
+// True when none of the next n steps flips a BC direction.
+bool flip_free_steps(const pd_env *env, int64_t n) {
+    for (const auto &h : env->hbc) {
+        if (h.kind != PD_BC_TOFRO) continue;
+        for (int64_t k = 0; k < n; ++k) {
+            const int64_t ts = env->ts + k;
+            if ((ts > h.applyafter) && std::fmod((double)ts, h.freq) == 0.0) return false;
+        }
+    }
+    return true;
+}
+
+// Launch kGraphSteps full steps (MODE 1) from the current state: the
+// cached graph for these arguments, captured on first use.
+template <class R>
+pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
+    cudaStream_t st = env->st;
+    StepArgs<R> a0 = args(env, F);
+    a0.dir_vel = a0.dir_pos = dir_bits(env);
+    typename Fast<R>::Graph *hit = nullptr;
+    for (auto &g : F.graphs)
+        if (g.wps == F.wps && g.gate.size() == F.gitems_h.size() &&
+            std::memcmp(&g.a0, &a0, sizeof(a0)) == 0 &&
+            std::memcmp(g.gate.data(), F.gitems_h.data(), g.gate.size() * sizeof(GateItem)) == 0) {
+            hit = &g;
+            break;
+        }
+    if (!hit) {
+        if (F.graphs.size() >= 8) {
+            for (auto &g : F.graphs) cudaGraphExecDestroy(g.exec);
+            F.graphs.clear();
+        }
+        const int cur0 = F.cur;
+        const int64_t n0 = launch_count();
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kGraphSteps; ++k) {
+            StepArgs<R> a = args(env, F);
+            a.dir_vel = a.dir_pos = a0.dir_vel;
+            gate_launch(env, a, F);
+            if (lps) launch_theta(st, F.wps, a);
+            launch_step<R, 1>(st, F.wps, a);
+            F.cur = 1 - F.cur;
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+        F.cur = cur0;  // kGraphSteps is even: the parity is unchanged
+        const int64_t kernels = launch_count() - n0;  // captured, not run
+        add_launches(-kernels);
+        if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return cuda_fail(ie, "graph instantiate", __FILE__, __LINE__);
+        F.graphs.push_back(typename Fast<R>::Graph{a0, F.gitems_h, F.wps, kernels, exec});
+        hit = &F.graphs.back();
+    }
+    CK(cudaGraphLaunch(hit->exec, st));
+    add_launches(hit->kernels);
+    for (int k = 0; k < kGraphSteps; ++k) advance_bc_clock(env);
+    return PD_OK;
+}
+
 template <class R>
 pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
     cudaStream_t st = env->st;
@@ -1184,19 +1326,24 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
         note_launch();
         F.cur = 1 - F.cur;
     }
-    for (int64_t s = 0; s < nsteps; ++s) {
+    // Steps without contacts run as replays of a captured graph of
+    // kGraphSteps steps while the BC directions stay constant; the rest
+    // (contacts, direction flips, the last step, profiling) launch directly.
+    const bool graphs = !contacts && !env->prof && !std::getenv("PD_NO_GRAPHS");
+    PD_TRY(gate_prepare(env, F));
+    for (int64_t s = 0; s < nsteps;) {
+        if (graphs && nsteps - 1 - s >= kGraphSteps && flip_free_steps(env, kGraphSteps)) {
+            PD_TRY(poll_gate_flags(env, F));
+            PD_TRY(replay_graph(env, F, lps));
+            s += kGraphSteps;
+            continue;
+        }
         const bool last = s == nsteps - 1;
         StepArgs<R> a = args(env, F);
         a.dir_vel = dir_bits(env);
-        // check!(env) then time_step += 1 (velocity_verlet.jl:81-85)
-        for (auto &h : env->hbc) {
-            if (h.kind != PD_BC_TOFRO) continue;
-            const double r = std::fmod((double)env->ts, h.freq);
-            if ((env->ts > h.applyafter) && (r == 0.0)) h.dir = -h.dir;
-        }
-        env->ts += 1;
+        advance_bc_clock(env);
         a.dir_pos = dir_bits(env);
-        PD_TRY(gate_if_needed(env, a, F));
+        gate_launch(env, a, F);
         if (lps) launch_theta(st, wps, a);
         prof_begin(env, st);
         if (!contacts) {
@@ -1213,8 +1360,15 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
         }
         if (!last) F.cur = 1 - F.cur;
         if ((s & 63) == 63) CK(cudaGetLastError());
+        ++s;
     }
     CK(cudaGetLastError());
+    if (F.flags_pending) {  // land the last read-back before the state can be reset
+        CK(cudaEventSynchronize(F.flags_ev));
+        for (size_t b = 0; b < env->hb.size(); ++b)
+            if (F.flags_h[b]) env->deformed_h[b] = 1;
+        F.flags_pending = false;
+    }
     return PD_OK;
 }
 

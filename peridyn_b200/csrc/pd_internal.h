@@ -32,8 +32,11 @@ namespace pd {
 
 constexpr int kSlice = 32;
 
-// Counts every kernel launch the library issues (pd_kernel_launches).
+// Counts every kernel launch the library issues (pd_kernel_launches);
+// graph replays add their kernel nodes.
 void note_launch();
+void add_launches(int64_t n);
+int64_t launch_count();
 
 struct DevBlock {
     int32_t kind;       // PD_MAT_*

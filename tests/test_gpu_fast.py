@@ -156,3 +156,52 @@ def test_update_acc_fast_matches_oracle(oracle):
         assert rel_l2(env.f, ora.f) <= tol
         assert np.allclose(env.theta(0), ora.blocks[0].theta, rtol=tol, atol=tol * np.abs(ora.blocks[0].theta).max())
         env.close()
+
+
+def _tofro_bar():
+    x, vol = lattice.cuboid(14, 6, 6, 1e-3, jitter=1e-5, seed=4)
+    gen = pb.GeneralMaterial(x.copy(order="F"), np.zeros_like(x, order="F"), x, vol, np.ones(x.shape[1], np.int64),
+                             3.015e-3, max_neigh=200)
+    mat = pb.PeridynamicsMaterial(gen, pb.OrdinaryStateBasedSpecific([20e9], [9e9], [0.05], [2000.0]))
+    bcs = [pb.FixBC(x[0] < 2e-3), pb.ToFroBC(x[0] > 12e-3, [2.0, 0.3, 0.0], 40, applyafter=10)]
+    return {"materials": [mat], "contacts": [], "bcs": bcs, "dt": 2e-8}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("builder", [_tofro_bar, lambda: configs.batched_cubes(nspec=6, edge_lo=5, edge_hi=9)])
+def test_graph_replay_matches_direct_launches(precision, builder, monkeypatch):
+    # graph replays of 32 steps (between BC direction flips, gate kernels
+    # included while a block is undeformed) against one launch per kernel
+    w = builder()
+
+    def run():
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+        if w["bcs"]:
+            pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=150)
+        pb.velocity_verlet_step(env, nsteps=75)
+        out = env.get_state(), [env._family(b)[1] for b in range(len(w["materials"]))], env.deformed()
+        env.close()
+        return out
+
+    monkeypatch.setenv("PD_NO_GRAPHS", "1")
+    (s1, i1, d1) = run()
+    monkeypatch.delenv("PD_NO_GRAPHS")
+    (s2, i2, d2) = run()
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    for a, b in zip(i1, i2):
+        assert np.array_equal(a, b)
+    assert np.array_equal(d1, d2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_rigid_gate_fast_long_run(precision):
+    # long enough for graph replays: the gate stays in every replayed step
+    w = configs.pmb_cube(n=8, peak=0.0)
+    w["materials"][0].general.velocity[0] = 3.0
+    env = pb.Env(1, w["materials"], [], [], w["dt"], precision=precision)
+    pb.velocity_verlet_step(env, nsteps=100)
+    assert not env.deformed()[0]
+    assert np.all(env.f == 0.0)
+    env.close()
