@@ -260,6 +260,53 @@ PD_API pd_status pd_kernel_launches(int64_t *count);
  * device time (ms) and the number of timed launches since enabling. */
 PD_API pd_status pd_env_profile(pd_env *env, int32_t enable);
 PD_API pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t *launches);
+/* Kernel shape of the throughput modes (extension): warps per 32-particle
+ * slice (1, 2, 4, 8) and bonds in flight per thread (FP32C: 2 or 4, FP64:
+ * 1 or 2).  (0, 0) returns to the autotuner, which times every shape on
+ * the first step and caches the fastest per problem size. */
+PD_API pd_status pd_env_set_kernel_shape(pd_env *env, int32_t warps_per_slice, int32_t unroll);
+
+/* ---------------------------------------------------------------------- */
+/* Serving (extension): a request loop that admits simulation jobs by HBM  */
+/* footprint, keeps their state resident and advances every admitted job   */
+/* on its own stream in chunks, so the work of jobs that arrive while      */
+/* others run overlaps on the device (continuous batching).  Thread-safe.  */
+/* ---------------------------------------------------------------------- */
+typedef struct pd_server pd_server;
+enum { PD_JOB_QUEUED = 0, PD_JOB_RUNNING = 1, PD_JOB_DONE = 2, PD_JOB_FAILED = 3, PD_JOB_CANCELLED = 4 };
+typedef struct pd_job_info {
+    int32_t state;            /* PD_JOB_* */
+    int32_t status;           /* pd_status of a failed job, else PD_OK */
+    int64_t steps_done;       /* velocity-Verlet steps completed */
+    int64_t particles;        /* environment particles */
+    int64_t footprint_bytes;  /* HBM reserved at admission */
+    int64_t bond_updates;     /* intact directed bonds x steps (mean of start and end) */
+    double queue_ms;          /* submit -> admission */
+    double latency_ms;        /* submit -> completion (0 until done) */
+} pd_job_info;
+/* hbm_budget_bytes <= 0: 90% of the device's free memory at creation.
+ * max_active: jobs resident at once.  chunk_steps: steps a job advances
+ * per scheduling round (rounded to the graph replay length when larger). */
+PD_API pd_status pd_server_create(pd_server **out, int32_t device, int64_t hbm_budget_bytes, int32_t max_active,
+                                  int64_t chunk_steps);
+/* Takes ownership of an assembled, NOT finalized environment (blocks, BCs
+ * and contacts added) on the server's device; the server finalizes it at
+ * admission, applies the BC snapshot and the initial force evaluation
+ * (run!'s save_state! at t0, solvers.jl:97-187), then advances nsteps
+ * velocity-Verlet steps.  The kernel shape of throughput-mode jobs is fixed
+ * from the problem size (not timed), so a job's result does not depend on
+ * what else runs beside it. */
+PD_API pd_status pd_server_submit(pd_server *srv, pd_env *env, int64_t nsteps, int64_t *job);
+PD_API pd_status pd_server_poll(pd_server *srv, int64_t job, pd_job_info *info);
+/* Blocks until the job is done, failed or cancelled, or timeout_s passes
+ * (PD_ERR_TIMEOUT). */
+PD_API pd_status pd_server_wait(pd_server *srv, int64_t job, double timeout_s, pd_job_info *info);
+/* Final state of a done job in environment order (y, v: 3 x N column-major;
+ * damage: N; any may be NULL); releases the job's record. */
+PD_API pd_status pd_server_result(pd_server *srv, int64_t job, double *y, double *v, double *damage);
+PD_API pd_status pd_server_cancel(pd_server *srv, int64_t job);
+/* Cancels queued and running jobs and joins the worker. */
+PD_API pd_status pd_server_destroy(pd_server *srv);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,7 @@ from .boundary_conditions import FixBC, MoveBC, ToFroBC
 from .contacts import (LinearSpringContactModel, NonLinearSpringContactModel, NonLinearSpringContactModel11,
                        NonLinearSpringContactModel12, ShortRangeContactModel)
 from .environment import Env, GeneralEnvironment
+from .serving import Server, serve_stream
 from .materials import (BondBasedMaterial, BondBasedSpecific, GeneralMaterial, OrdinaryStateBasedMaterial,
                         OrdinaryStateBasedSpecific, PeridynamicsMaterial, SkipMaterial, SkipSpecific,
                         julia_pow_int, make_matrix)

@@ -73,6 +73,21 @@ class MaterialDesc(ctypes.Structure):
     ]
 
 
+class JobInfo(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("steps_done", ctypes.c_int64),
+        ("particles", ctypes.c_int64),
+        ("footprint_bytes", ctypes.c_int64),
+        ("bond_updates", ctypes.c_int64),
+        ("queue_ms", ctypes.c_double),
+        ("latency_ms", ctypes.c_double),
+    ]
+
+
+JOB_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
 _SIGNATURES = {
     "pd_abi_version": (ctypes.c_int, []),
     "pd_status_string": (ctypes.c_char_p, [ctypes.c_int32]),
@@ -120,6 +135,15 @@ _SIGNATURES = {
     "pd_kernel_launches": (ctypes.c_int32, [c_i64p]),
     "pd_env_profile": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
     "pd_env_profile_read": (ctypes.c_int32, [c_vp, c_dp, c_i64p]),
+    "pd_env_set_kernel_shape": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.c_int32]),
+    "pd_server_create": (ctypes.c_int32, [ctypes.POINTER(c_vp), ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                                          ctypes.c_int64]),
+    "pd_server_submit": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_int64, c_i64p]),
+    "pd_server_poll": (ctypes.c_int32, [c_vp, ctypes.c_int64, ctypes.c_void_p]),
+    "pd_server_wait": (ctypes.c_int32, [c_vp, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p]),
+    "pd_server_result": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_dp, c_dp, c_dp]),
+    "pd_server_cancel": (ctypes.c_int32, [c_vp, ctypes.c_int64]),
+    "pd_server_destroy": (ctypes.c_int32, [c_vp]),
 }
 
 _lib = None

@@ -25,9 +25,10 @@ UNITS = [
     ("pd_solver.cu", ["-fmad=false"]),
     ("pd_env.cu", ["-fmad=false"]),
     # FP32 denormals never occur in displacements or bond vectors; flushing
-    # them lets rsqrtf/__fdividef map to single MUFU operations
+    # them lets the approximate sqrt/reciprocal map to single MUFU operations
     ("pd_fast.cu", ["-fmad=true", "-ftz=true"]),
     ("pd_noalloc.cu", ["-fmad=false"]),
+    ("pd_server.cu", ["-fmad=false"]),
 ]
 
 

@@ -110,3 +110,45 @@ def disk_impact(radius=0.05, thickness=0.005, spacing=2.5e-4, sphere_radius=0.01
         dt = 0.5 * math.sqrt(2 * rho / kx)
     return {"materials": [sph_m, disk_m], "contacts": [contact], "bcs": [], "dt": dt, "steps": steps,
             "workload": "disk_impact"}
+
+
+def lps_cube(dims, spacing=1.0e-3, jitter=1.0e-5, seed=1, horizon_factor=3.015, E=70e9, nu=0.25, rho=2700.0,
+             cs=0.01, peak=10.0, sigma=3.0e-3, dt=1.0e-8, steps=1000):
+    """State-based (LPS) cuboid with the Gaussian pulse of pmb_cube."""
+    nx, ny, nz = dims
+    x, vol = lattice.cuboid(nx, ny, nz, spacing, jitter=jitter, seed=seed)
+    gen = GeneralMaterial(x.copy(order="F"), lattice.gaussian_pulse(x, peak, sigma), x, vol,
+                          np.ones(x.shape[1], dtype=np.int64), horizon_factor * spacing, max_neigh=200)
+    K = E / 3 / (1 - 2 * nu)
+    G = E / 2 / (1 + nu)
+    mat = PeridynamicsMaterial(gen, OrdinaryStateBasedSpecific([K], [G], [cs], [rho]), name="lps_cube")
+    return {"materials": [mat], "contacts": [], "bcs": [], "dt": dt, "steps": steps,
+            "workload": f"lps_cube_{nx}x{ny}x{nz}"}
+
+
+def serving_jobs(njobs, seed=5, rate=50.0, n_lo=5.0e3, n_hi=5.0e5, steps_lo=500, steps_hi=5000,
+                 precision="fp32c"):
+    """Mixed stream of PMB and state-based cube jobs: particle counts
+    log-uniform over [n_lo, n_hi], steps uniform over steps_lo..steps_hi,
+    critical stretch U(0.002, 0.01) and pulse peak U(5, 50) m/s as in
+    batched_cubes; Poisson arrivals at ``rate`` jobs/s.  Returns (jobs,
+    arrival times in s)."""
+    u = lattice.uniform(seed, 6 * njobs)
+    jobs, arrivals, t = [], [], 0.0
+    for k in range(njobs):
+        uk = u[6 * k:6 * k + 6]
+        n = math.exp(math.log(n_lo) + (math.log(n_hi) - math.log(n_lo)) * uk[0])
+        e = max(4, int(round(n ** (1.0 / 3.0))))
+        nsteps = steps_lo + int(uk[1] * (steps_hi - steps_lo + 1))
+        cs = 0.002 + 0.008 * uk[2]
+        peak = 5.0 + 45.0 * uk[3]
+        if uk[4] < 0.5:
+            w = pmb_cube(dims=(e, e, e), cs=cs, peak=peak, seed=seed * 7919 + k, steps=nsteps)
+        else:
+            w = lps_cube((e, e, e), cs=cs, peak=peak, seed=seed * 7919 + k, steps=nsteps)
+        w["nsteps"] = nsteps
+        w["precision"] = precision
+        jobs.append(w)
+        t += -math.log(1.0 - uk[5]) / rate
+        arrivals.append(t)
+    return jobs, arrivals

@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <functional>
+#include <iterator>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -88,6 +90,25 @@ pd::Geo pd_env::geo() const {
 namespace {
 
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+// fn(begin, end) over [0, n) split across the host's cores.
+template <class F>
+void parallel_for(int64_t n, F fn) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw ? hw : 1, 32));
+    if (n < 256 || nt == 1) {
+        fn((int64_t)0, n);
+        return;
+    }
+    const int64_t per = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int64_t t = 0; t < nt; ++t) {
+        const int64_t a = t * per, b = std::min(n, a + per);
+        if (a >= b) break;
+        th.emplace_back(fn, a, b);
+    }
+    for (auto &x : th) x.join();
+}
 
 bool symmetric(const std::vector<double> &m, int nt) {
     for (int i = 0; i < nt; ++i)
@@ -396,42 +417,52 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     const bool force_explicit = lay && std::strcmp(lay, "explicit") == 0;
     std::vector<SliceInfo> si(S + 1);
     std::vector<std::vector<int32_t>> uni(S);
+    // pass 1 (per slice): the union of the lanes' offsets q - p, merged from
+    // the lanes' descending lists; stencil form when it stays small
+    parallel_for(S, [&](int64_t s0, int64_t s1) {
+        std::vector<int32_t> cur, lane, tmp;
+        for (int64_t s = s0; s < s1; ++s) {
+            int32_t maxc = 0;
+            for (int l = 0; l < kSlice; ++l) maxc = std::max(maxc, cnt[s * kSlice + l]);
+            const int64_t limit = (int64_t)maxc + maxc / 4 + 32;
+            bool stencil = !force_explicit && maxc > 0;
+            cur.clear();
+            for (int l = 0; stencil && l < kSlice; ++l) {
+                const int64_t p = s * kSlice + l;
+                const int64_t base = slice_ptr[s] + l;
+                lane.resize(cnt[p]);
+                for (int32_t k = 0; k < cnt[p]; ++k) lane[k] = nbr_b[base + 32 * (int64_t)k] - (int32_t)p;
+                tmp.clear();
+                std::set_union(cur.begin(), cur.end(), lane.begin(), lane.end(), std::back_inserter(tmp),
+                               std::greater<int32_t>());
+                cur.swap(tmp);
+                if ((int64_t)cur.size() > limit) stencil = false;
+            }
+            // every slot a lane scans must name an in-range record
+            for (int l = 0; stencil && l < kSlice; ++l) {
+                const int64_t p = s * kSlice + l;
+                if (cnt[p] == 0) continue;
+                stencil = p + cur.front() < N && p + cur.back() >= 0;
+            }
+            SliceInfo &d = si[s];
+            if (stencil) {
+                d.mode = kStencil;
+                d.len = (int32_t)round_up((int64_t)cur.size(), 32);
+                uni[s] = cur;
+            } else {
+                d.mode = kExplicit;
+                d.len = (int32_t)round_up(maxc, 32);
+            }
+        }
+    });
     int64_t nbr_len = 0, nwords = 0, nst = 0;
-    std::vector<int32_t> offs;
     for (int64_t s = 0; s < S; ++s) {
-        int32_t maxc = 0;
-        offs.clear();
-        for (int l = 0; l < kSlice; ++l) {
-            const int64_t p = s * kSlice + l;
-            maxc = std::max(maxc, cnt[p]);
-            const int64_t base = slice_ptr[s] + l;
-            for (int32_t k = 0; k < cnt[p]; ++k) offs.push_back(nbr_b[base + 32 * (int64_t)k] - (int32_t)p);
-        }
-        std::sort(offs.begin(), offs.end(), std::greater<int32_t>());
-        offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
-        const int64_t U = (int64_t)offs.size();
-        bool stencil = !force_explicit && maxc > 0 && U <= (int64_t)maxc + maxc / 4 + 32;
-        // every slot a lane scans must name an in-range record
-        for (int l = 0; stencil && l < kSlice; ++l) {
-            const int64_t p = s * kSlice + l;
-            if (cnt[p] == 0) continue;
-            stencil = p + offs.front() < N && p + offs.back() >= 0;
-        }
         SliceInfo &d = si[s];
         d.nbr = nbr_len;
         d.word = nwords;
-        if (stencil) {
-            d.mode = kStencil;
-            d.len = (int32_t)round_up(U, 32);
-            nbr_len += d.len;
-            uni[s] = offs;
-            ++nst;
-        } else {
-            d.mode = kExplicit;
-            d.len = (int32_t)round_up(maxc, 32);
-            nbr_len += (int64_t)kSlice * d.len;
-        }
+        nbr_len += d.mode == kStencil ? d.len : (int64_t)kSlice * d.len;
         nwords += d.len;
+        nst += d.mode == kStencil;
     }
     si[S].nbr = nbr_len;
     si[S].word = nwords;
@@ -440,35 +471,37 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     std::vector<int32_t> nbr(std::max<int64_t>(nbr_len, 32), 0);
     std::vector<uint32_t> words(std::max<int64_t>(nwords, 1), 0), fam(std::max<int64_t>(nwords, 1), 0);
     std::vector<int32_t> cnt_rt(N, 0);
-    for (int64_t s = 0; s < S; ++s) {
-        const SliceInfo &d = si[s];
-        if (d.mode == kStencil) {
+    // pass 2 (per slice, disjoint outputs): slots, bits and slot counts
+    parallel_for(S, [&](int64_t s0, int64_t s1) {
+        for (int64_t s = s0; s < s1; ++s) {
+            const SliceInfo &d = si[s];
             const std::vector<int32_t> &u = uni[s];
-            for (size_t j = 0; j < u.size(); ++j) nbr[d.nbr + j] = u[j];
-        }
-        for (int l = 0; l < kSlice; ++l) {
-            const int64_t p = s * kSlice + l;
-            const int64_t base = slice_ptr[s] + l, wb = slice_ptr[s] / 32 + l, ow = d.word + l;
-            int32_t j = 0, last = -1;
-            for (int32_t k = 0; k < cnt[p]; ++k) {
-                const int32_t q = nbr_b[base + 32 * (int64_t)k];
-                int32_t slot = k;
-                if (d.mode == kStencil) {
-                    // both lists descend: advance to this offset
-                    const std::vector<int32_t> &u = uni[s];
-                    while (u[j] != q - (int32_t)p) ++j;
-                    slot = j;
-                } else {
-                    nbr[d.nbr + 32 * (int64_t)k + l] = q;
+            if (d.mode == kStencil)
+                for (size_t j = 0; j < u.size(); ++j) nbr[d.nbr + j] = u[j];
+            for (int l = 0; l < kSlice; ++l) {
+                const int64_t p = s * kSlice + l;
+                const int64_t base = slice_ptr[s] + l, wb = slice_ptr[s] / 32 + l, ow = d.word + l;
+                int32_t j = 0, last = -1;
+                for (int32_t k = 0; k < cnt[p]; ++k) {
+                    const int32_t q = nbr_b[base + 32 * (int64_t)k];
+                    int32_t slot = k;
+                    if (d.mode == kStencil) {
+                        // both lists descend: advance to this offset
+                        while (u[j] != q - (int32_t)p) ++j;
+                        slot = j;
+                    } else {
+                        nbr[d.nbr + 32 * (int64_t)k + l] = q;
+                    }
+                    const uint32_t bit = 1u << (slot & 31);
+                    fam[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+                    if ((w_b[wb + 32 * (int64_t)(k >> 5)] >> (k & 31)) & 1u)
+                        words[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+                    last = slot;
                 }
-                const uint32_t bit = 1u << (slot & 31);
-                fam[ow + 32 * (int64_t)(slot >> 5)] |= bit;
-                if ((w_b[wb + 32 * (int64_t)(k >> 5)] >> (k & 31)) & 1u) words[ow + 32 * (int64_t)(slot >> 5)] |= bit;
-                last = slot;
+                cnt_rt[p] = last + 1;
             }
-            cnt_rt[p] = last + 1;
         }
-    }
+    });
     cnt.swap(cnt_rt);
     env->sinfo_h = si;
     env->cnt_h = cnt;
@@ -989,6 +1022,7 @@ extern "C" pd_status pd_env_set_time_step(pd_env *env, int64_t ts) {
 extern "C" pd_status pd_env_reset_deformed(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
+    PD_TRY(pd::fast_land_flags(env));
     std::vector<int32_t> h(env->deformed0.begin(), env->deformed0.end());
     CK(cudaMemcpyAsync(env->deformed.p, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice, env->st));
     CK(cudaStreamSynchronize(env->st));
@@ -1150,3 +1184,22 @@ extern "C" pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t 
     if (launches) *launches = env->prof_launches;
     return PD_OK;
 }
+
+namespace pd {
+int64_t footprint_estimate(const pd_env *env) {
+    // per particle: FP64 state and tables (~300 B), throughput-mode records
+    // (~250 B); per bond slot: build-layout index + bits (4.2 B, transient)
+    // and runtime bits (4 arrays) + explicit index (4.5 B)
+    int64_t bytes = 64ll << 20;  // stream, scratch, reductions
+    for (const auto &b : env->hb) {
+        const int64_t np = (b.n + 31) / 32 * 32;
+        const int64_t rows = b.host_family ? std::max<int64_t>(b.rows, 1) : std::min<int64_t>(b.max_neigh, b.n);
+        bytes += np * 560 + np * rows * 9;
+    }
+    for (const auto &c : env->hc) {
+        const int64_t n1 = env->hb[c.b1].n;
+        bytes += n1 * std::max<int64_t>(c.max_neighs, 1) * 8 + (64ll << 10);
+    }
+    return bytes;
+}
+}  // namespace pd

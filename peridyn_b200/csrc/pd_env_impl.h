@@ -182,6 +182,7 @@ struct pd_env {
     // fast (FP64 / FP32C) state; see pd_fast.cu
     bool fast_valid = false;
     void *fast = nullptr;
+    int shape = 0;  // fixed kernel shape 10 * warps_per_slice + unroll, 0 = autotune
 
     pd::Geo geo() const;
     void release_device();
@@ -201,6 +202,11 @@ pd_status contacts_force(pd_env *env);
 pd_status sync_state_to_fp64(pd_env *env, bool invalidate = true);
 void fast_release(pd_env *env);
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps);
+pd_status fast_vv_enqueue(pd_env *env, int64_t nsteps);
+pd_status fast_land_flags(pd_env *env);
+// Device bytes an assembled environment will hold once finalized (upper
+// estimate from particle counts and family rows; for admission control).
+int64_t footprint_estimate(const pd_env *env);
 pd_status fast_update_acc(pd_env *env);
 pd_status update_acc_serial(pd_env *env);
 }  // namespace pd

@@ -1158,6 +1158,10 @@ std::map<std::tuple<int64_t, int64_t, int, bool>, int> g_tune_cache;
 template <class R>
 pd_status autotune(pd_env *env, Fast<R> &F) {
     if (F.wps) return PD_OK;
+    if (env->shape) {  // pd_env_set_kernel_shape
+        F.wps = env->shape;
+        return PD_OK;
+    }
     const bool lps = any_lps(env);
     const auto key = std::make_tuple(env->N, env->nnz, env->precision, lps);
     {
@@ -1312,7 +1316,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
 }
 
 template <class R>
-pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
+pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true) {
     cudaStream_t st = env->st;
     const unsigned grid = gridn(env->N);
     const bool lps = any_lps(env);
@@ -1363,7 +1367,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps) {
         ++s;
     }
     CK(cudaGetLastError());
-    if (F.flags_pending) {  // land the last read-back before the state can be reset
+    if (blocking && F.flags_pending) {  // land the last read-back before the state can be reset
         CK(cudaEventSynchronize(F.flags_ev));
         for (size_t b = 0; b < env->hb.size(); ++b)
             if (F.flags_h[b]) env->deformed_h[b] = 1;
@@ -1440,6 +1444,34 @@ pd_status sync_state_to_fp64(pd_env *env, bool invalidate) {
     return PD_OK;
 }
 
+// Enqueue nsteps on the environment's stream without waiting for them
+// (serving); the host copy of the gate flags catches up on later calls.
+pd_status fast_vv_enqueue(pd_env *env, int64_t nsteps) {
+    if (nsteps == 0) return PD_OK;
+    PD_TRY(ensure_fast(env));
+    FastHolder *h = holder(env);
+    if (h->prec == PD_PREC_FP32C) PD_TRY(vv_chunk(env, h->f32, nsteps, false));
+    else PD_TRY(vv_chunk(env, h->f64, nsteps, false));
+    h->dirty = true;
+    return PD_OK;
+}
+
+// Wait for and apply an outstanding gate-flag read-back (before anything
+// resets the flags).
+pd_status fast_land_flags(pd_env *env) {
+    if (!env->fast) return PD_OK;
+    FastHolder *h = holder(env);
+    auto land = [&](auto &F) -> pd_status {
+        if (!F.flags_pending) return PD_OK;
+        CK(cudaEventSynchronize(F.flags_ev));
+        for (size_t b = 0; b < env->hb.size(); ++b)
+            if (F.flags_h[b]) env->deformed_h[b] = 1;
+        F.flags_pending = false;
+        return PD_OK;
+    };
+    return h->prec == PD_PREC_FP32C ? land(h->f32) : land(h->f64);
+}
+
 void fast_release(pd_env *env) {
     delete holder(env);
     env->fast = nullptr;
@@ -1470,3 +1502,19 @@ pd_status fast_update_acc(pd_env *env) {
 }
 
 }  // namespace pd
+
+extern "C" pd_status pd_env_set_kernel_shape(pd_env *env, int32_t warps_per_slice, int32_t unroll) {
+    if (!env) return pd::fail(PD_ERR_ARG, "environment handle is NULL");
+    const int lo = env->precision == PD_PREC_FP32C ? pd::Unroll<float>::LO : pd::Unroll<double>::LO;
+    const int hi = env->precision == PD_PREC_FP32C ? pd::Unroll<float>::HI : pd::Unroll<double>::HI;
+    const int w = warps_per_slice, u = unroll;
+    if (!(w == 0 && u == 0) && !((w == 1 || w == 2 || w == 4 || w == 8) && (u == lo || u == hi)))
+        return pd::fail(PD_ERR_ARG, "kernel shape (%d, %d) not available: warps per slice 1/2/4/8, unroll %d or %d", w,
+                    u, lo, hi);
+    env->shape = w == 0 ? 0 : 10 * w + u;
+    if (env->fast) {
+        pd::holder(env)->f32.wps = 0;
+        pd::holder(env)->f64.wps = 0;
+    }
+    return PD_OK;
+}

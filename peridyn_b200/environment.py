@@ -16,7 +16,7 @@ from .contacts import NonLinearSpringContactModel11, NonLinearSpringContactModel
 
 class GeneralEnvironment:
     def __init__(self, id, materials, short_range_contact, boundary_conds, dt, state=2, bskin=0.5, units=False,
-                 precision="fp64_serial", device=0, families=None):
+                 precision="fp64_serial", device=0, families=None, finalize=True):
         L = _abi.lib()
         self.id = int(id)
         self.state = int(state)
@@ -35,14 +35,14 @@ class GeneralEnvironment:
         _abi.check(L.pd_env_create(ctypes.byref(h), int(device), prec, self.dt))
         self._h = h
         try:
-            self._assemble(L, families)
+            self._assemble(L, families, finalize)
         except Exception:
             L.pd_env_destroy(self._h)
             self._h = None
             raise
 
     # ------------------------------------------------------------------
-    def _assemble(self, L, families):
+    def _assemble(self, L, families, finalize=True):
         types, bids = [], []
         for b, mat in enumerate(self.material_blocks):
             gen = mat.general
@@ -83,6 +83,8 @@ class GeneralEnvironment:
                 raise TypeError("unknown contact model")
             _abi.check(L.pd_env_add_contact(self._h, cm.kind, b1, b2, cm.exponent, cm.stifness, cm.equi_dist,
                                             cm.distance, rows, None))
+        if not finalize:  # handed to a Server, which finalizes at admission
+            return
         _abi.check(L.pd_env_finalize(self._h))
         self.volume = np.zeros(self.N)
         self.mass = np.zeros(self.N)
@@ -105,6 +107,16 @@ class GeneralEnvironment:
         intact = np.zeros((rows.value, n), dtype=np.uint8, order="F")
         _abi.check(L.pd_env_get_family(self._h, block, _abi.i64ptr(fam), _abi.u8ptr(intact)))
         return fam, intact.astype(bool)
+
+    def _detach(self):
+        """Give up ownership of the library handle (it now belongs to a
+        server) and return it."""
+        h, self._h = self._h, None
+        return h
+
+    def set_kernel_shape(self, warps_per_slice=0, unroll=0):
+        """Fix the throughput-mode kernel shape; (0, 0) = autotune."""
+        _abi.check(_abi.lib().pd_env_set_kernel_shape(self._h, int(warps_per_slice), int(unroll)))
 
     # ------------------------------------------------------------------
     def close(self):
