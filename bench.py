@@ -75,18 +75,42 @@ def particle_bytes(precision, lps):
     return 141 + (8 if lps else 0)
 
 
+NEIGH_EVERY = 100  # contact neighbour update cadence (run!'s neigh_update_freq)
+
+
+def advance(env, work, nsteps):
+    """nsteps velocity-Verlet steps; with contacts the contact neighbours
+    are rebuilt every NEIGH_EVERY steps, as run! does (solvers.jl:176-178)."""
+    from peridyn_b200 import _abi
+
+    L = _abi.lib()
+    if not work["contacts"]:
+        _abi.check(L.pd_env_vv_steps(env._h, nsteps))
+        return
+    done = 0
+    while done < nsteps:
+        k = min(NEIGH_EVERY, nsteps - done)
+        _abi.check(L.pd_env_vv_steps(env._h, k))
+        done += k
+        if done < nsteps:
+            _abi.check(L.pd_env_update_neighs(env._h, 30))
+
+
 def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
     """Error of a throughput-mode run against the serial-order FP64 path
-    (bit-identical to the CPU oracle) over the same run."""
+    (bit-identical to the CPU oracle) over the same run; for the contact
+    workload, whose serial run would take minutes, against the one-pass FP64
+    GPU path."""
     import peridyn_b200 as pb
 
-    ref = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision="fp64_serial",
+    ref_prec = "fp64" if work["contacts"] else "fp64_serial"
+    ref = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision=ref_prec,
                  device=device)
     if work["bcs"]:
         pb.apply_bc_at0(ref, 0)
     pb.update_neighs(ref)
     pb.update_acc(ref)
-    pb.velocity_verlet_step(ref, nsteps=sim_steps)
+    advance(ref, work, sim_steps)
     yr, vr, _, _ = ref.get_state()
     yf, vf, _, _ = env_fast.get_state()
     x = np.hstack([m.general.x for m in work["materials"]])
@@ -99,7 +123,9 @@ def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
         broken += int((fr > 0).sum() - ir.sum())
     ref.close()
     l2 = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-    return {"vs": "fp64_serial GPU path (bit-identical to the CPU oracle)", "vv_steps": int(sim_steps),
+    vs = ("fp64 one-pass GPU path" if ref_prec == "fp64" else
+          "fp64_serial GPU path (bit-identical to the CPU oracle)")
+    return {"vs": vs, "vv_steps": int(sim_steps),
             "displacement_rel_l2": l2(yf - x, yr - x), "velocity_rel_l2": l2(vf, vr),
             "broken_bonds_fp64": broken, "broken_bond_mismatch": mism}
 
@@ -215,7 +241,7 @@ def time_precision(work, precision, sim_steps, device, flush, dist):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _abi.check(L.pd_env_vv_steps(env._h, sim_steps))
+        advance(env, work, sim_steps)
         e1.record(stream)
         torch.cuda.synchronize()
         if k > 0:
@@ -228,6 +254,65 @@ def time_precision(work, precision, sim_steps, device, flush, dist):
         t_total = float(t.item())
     return {"precision": precision, "value": bonds / t_total, "unit": UNIT, "ms_per_step": 1e3 * t_total / 2,
             "steps": 2, "warmup": 1}
+
+
+def run_serving(args, rank, world, local):
+    """Serving stream: Poisson arrivals of mixed PMB / state-based jobs
+    submitted to a pd_server at their arrival times; aggregate bond-updates/s
+    over the stream's wall time and p50/p99 job latency (submit to result),
+    FP32C beside the plain FP64 GPU path.  One bench step = one stream."""
+    import torch
+
+    import peridyn_b200 as pb
+    from peridyn_b200 import configs
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    # each rank serves its own stream (seeded by rank): independent jobs, no collective on the data path
+    out = {}
+    for precision in ("fp32c", "fp64"):
+        jobs, arrivals = configs.serving_jobs(args.jobs, seed=5 + 1000 * rank, precision=precision)
+        warm, warm_arr = configs.serving_jobs(4, seed=99, n_lo=5e3, n_hi=2e4, steps_lo=100, steps_hi=200,
+                                              precision=precision)
+        with pb.Server(device=local) as srv:
+            pb.serve_stream(srv, warm, [0.0] * len(warm))
+            runs = []
+            for _ in range(args.steps):
+                if dist is not None:
+                    dist.barrier()
+                recs, summary = pb.serve_stream(srv, jobs, arrivals)
+                runs.append(summary)
+        wall = max(r["wall_s"] for r in runs)
+        bonds = sum(r["bond_updates"] for r in runs) / len(runs)
+        if dist is not None:
+            t = torch.tensor([wall, bonds], device="cuda", dtype=torch.float64)
+            w_ = t[:1].clone()
+            dist.all_reduce(w_, op=dist.ReduceOp.MAX)
+            b_ = t[1:].clone()
+            dist.all_reduce(b_, op=dist.ReduceOp.SUM)
+            wall, bonds = float(w_.item()), float(b_.item())
+        out[precision] = {"value": bonds / wall, "wall_s": wall,
+                          "latency_ms": runs[-1]["latency_ms"], "jobs": runs[-1]["jobs"]}
+    if rank == 0:
+        main = out["fp32c"]
+        line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": 1, "ms_per_step": 1e3 * main["wall_s"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (f64 position accumulator)", "data": "synthetic",
+                "config": {"workload": f"serving_{args.jobs}_jobs_poisson50",
+                           "sizes": "log-uniform 5e3..5e5 particles", "steps": "U{500..5000}",
+                           "parallelism": f"one server per GPU x{world}" if world > 1 else "1 GPU"},
+                "latency_ms": main["latency_ms"], "fp64_compare": out["fp64"],
+                "e2e": {"value": main["value"], "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                        "note": "serving is end to end: host job description in, host results out"}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_reference(args, rank, world):
@@ -261,7 +346,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lps_bar", choices=["lps_bar", "pmb_cube", "batched", "disk_impact"])
+    ap.add_argument("--workload", default="lps_bar",
+                    choices=["lps_bar", "pmb_cube", "batched", "disk_impact", "serving"])
+    ap.add_argument("--jobs", type=int, default=48, help="serving: jobs per stream")
     ap.add_argument("--precision", default="fp32c", choices=["fp64_serial", "fp64", "fp32c"])
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip timing the plain FP64 GPU path beside an FP32C run")
@@ -276,6 +363,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "serving":
+        run_serving(args, rank, world, local)
         return
 
     import torch
@@ -320,7 +410,7 @@ def main():
         pb.update_acc(env)  # the run's initial force evaluation (save_state! at t0)
 
     def one_run():
-        _abi.check(L.pd_env_vv_steps(env._h, sim_steps))
+        advance(env, work, sim_steps)
 
     bonds_start = None
     # warm-up

@@ -78,11 +78,15 @@ def disk_impact(radius=0.05, thickness=0.005, spacing=2.5e-4, sphere_radius=0.01
                 dt=None, gap=None):
     """Bond-based disk (axis z) hit along -z by a stiff bond-based sphere,
     nonlinear contact (exponent 2) of stiffness contact_factor * c with
-    equilibrium distance = spacing and search distance = horizon."""
+    equilibrium distance = spacing and search distance = horizon.  ``gap``
+    is the z clearance between the lowest projectile particle and the
+    highest disk particle (default 0.9 spacing: inside the contact distance,
+    so the impact starts at the first step)."""
     horizon = horizon_factor * spacing
     xd, vd = lattice.disk(radius, thickness, spacing)
-    gap = spacing if gap is None else gap
-    zc = thickness / 2 + gap + sphere_radius + spacing / 2
+    gap = 0.9 * spacing if gap is None else gap
+    xs0, _ = lattice.sphere(sphere_radius, spacing, center=(0.0, 0.0, 0.0))
+    zc = xd[2].max() + gap - xs0[2].min()
     xs, vs = lattice.sphere(sphere_radius, spacing, center=(0.0, 0.0, zc))
     gen_d = GeneralMaterial(xd.copy(order="F"), np.zeros_like(xd, order="F"), xd, vd,
                             np.full(xd.shape[1], 1, dtype=np.int64), horizon, max_neigh=200)
