@@ -501,6 +501,7 @@ def main():
     # roofline of the bond-force kernel
     n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
     layout = env.layout()
+    shape = env.kernel_shape()
     bytes_launch = bond_bytes(layout) + n_int * particle_bytes(args.precision, lps)
     avg_ms = prof_ms.value / max(1, prof_n.value)
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
@@ -543,6 +544,8 @@ def main():
         "accuracy": accuracy,
     }
     line["config"]["bond_layout"] = layout
+    line["config"]["kernel_shape"] = {"warps_per_slice": shape[0], "unroll": shape[1], "chosen_by":
+                                      "PD_KERNEL_SHAPE" if os.environ.get("PD_KERNEL_SHAPE") else "autotuner"}
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:

@@ -265,6 +265,9 @@ PD_API pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t *lau
  * 1 or 2).  (0, 0) returns to the autotuner, which times every shape on
  * the first step and caches the fastest per problem size. */
 PD_API pd_status pd_env_set_kernel_shape(pd_env *env, int32_t warps_per_slice, int32_t unroll);
+/* The shape the throughput path runs with (after autotuning); (0, 0)
+ * before the first throughput-mode step or in the serial mode. */
+PD_API pd_status pd_env_kernel_shape(pd_env *env, int32_t *warps_per_slice, int32_t *unroll);
 
 /* ---------------------------------------------------------------------- */
 /* Serving (extension): a request loop that admits simulation jobs by HBM  */

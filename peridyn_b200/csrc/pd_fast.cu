@@ -1209,28 +1209,35 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     std::vector<int> shapes;
     for (int wps : {1, 2, 4, 8})
         for (int u : {Unroll<R>::LO, Unroll<R>::HI}) shapes.push_back(10 * wps + u);
-    for (int w : shapes) {
-        if (lps) launch_theta(env->st, w, a);
-        launch_step<R, 6>(env->st, w, a);
-        cudaEventRecord(e0, env->st);
-        for (int r = 0; r < 3; ++r) {
+    // two sweeps over the shapes, 8 timed steps each, best of the two per
+    // shape: short kernels are noisy one launch at a time
+    std::vector<float> t(shapes.size(), 1e30f);
+    for (int sweep = 0; sweep < 2; ++sweep)
+        for (size_t i = 0; i < shapes.size(); ++i) {
+            const int w = shapes[i];
             if (lps) launch_theta(env->st, w, a);
             launch_step<R, 6>(env->st, w, a);
+            cudaEventRecord(e0, env->st);
+            for (int r = 0; r < 8; ++r) {
+                if (lps) launch_theta(env->st, w, a);
+                launch_step<R, 6>(env->st, w, a);
+            }
+            cudaEventRecord(e1, env->st);
+            cudaError_t err = cudaEventSynchronize(e1);
+            if (err != cudaSuccess) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return cuda_fail(err, "autotune", __FILE__, __LINE__);
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t[i] = std::min(t[i], ms);
         }
-        cudaEventRecord(e1, env->st);
-        cudaError_t err = cudaEventSynchronize(e1);
-        if (err != cudaSuccess) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return cuda_fail(err, "autotune", __FILE__, __LINE__);
+    for (size_t i = 0; i < shapes.size(); ++i)
+        if (t[i] < best) {
+            best = t[i];
+            best_w = shapes[i];
         }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) {
-            best = ms;
-            best_w = w;
-        }
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     CK(cudaGetLastError());
@@ -1516,5 +1523,14 @@ extern "C" pd_status pd_env_set_kernel_shape(pd_env *env, int32_t warps_per_slic
         pd::holder(env)->f32.wps = 0;
         pd::holder(env)->f64.wps = 0;
     }
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_kernel_shape(pd_env *env, int32_t *warps_per_slice, int32_t *unroll) {
+    if (!env || !warps_per_slice || !unroll) return pd::fail(PD_ERR_ARG, "NULL argument");
+    int cfg = 0;
+    if (env->fast) cfg = env->precision == PD_PREC_FP32C ? pd::holder(env)->f32.wps : pd::holder(env)->f64.wps;
+    *warps_per_slice = cfg / 10;
+    *unroll = cfg % 10;
     return PD_OK;
 }

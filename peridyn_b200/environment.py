@@ -114,6 +114,12 @@ class GeneralEnvironment:
         h, self._h = self._h, None
         return h
 
+    def kernel_shape(self):
+        """(warps per slice, unroll) the throughput path runs with."""
+        w, u = ctypes.c_int32(), ctypes.c_int32()
+        _abi.check(_abi.lib().pd_env_kernel_shape(self._h, ctypes.byref(w), ctypes.byref(u)))
+        return int(w.value), int(u.value)
+
     def set_kernel_shape(self, warps_per_slice=0, unroll=0):
         """Fix the throughput-mode kernel shape; (0, 0) = autotune."""
         _abi.check(_abi.lib().pd_env_set_kernel_shape(self._h, int(warps_per_slice), int(unroll)))
