@@ -216,6 +216,12 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 template <class R>
 struct Kin {
     R Y0, Y1, Y2, xx2, num;
+    // f += c Y
+    __device__ __forceinline__ void accumulate(R c, R &fx, R &fy, R &fz) const {
+        fx += c * Y0;
+        fy += c * Y1;
+        fz += c * Y2;
+    }
     __device__ __forceinline__ Kin(const typename Tr<R>::V4 &xq, const typename Tr<R>::V4 &uq,
                                    const typename Tr<R>::V4 &nx, const typename Tr<R>::V4 &nu) {
         const R x0 = xq.x + nx.x, x1 = xq.y + nx.y, x2 = xq.z + nx.z;
@@ -230,7 +236,12 @@ struct Kin {
 // FP32: the (x, y) components as packed f32x2 operations.
 template <>
 struct Kin<float> {
-    float Y0, Y1, Y2, xx2, num;
+    float2 Yxy;
+    float Y2, xx2, num;
+    __device__ __forceinline__ void accumulate(float c, float2 &fxy, float &fz) const {
+        fxy = __ffma2_rn(make_float2(c, c), Yxy, fxy);
+        fz += c * Y2;
+    }
     __device__ __forceinline__ Kin(const float4 &xq, const float4 &uq, const float4 &nx, const float4 &nu) {
         const float2 d = __fadd2_rn(make_float2(xq.x, xq.y), make_float2(nx.x, nx.y));
         const float2 e = __fadd2_rn(make_float2(uq.x, uq.y), make_float2(nu.x, nu.y));
@@ -242,8 +253,7 @@ struct Kin<float> {
         const float2 es = __fmul2_rn(e, S);
         xx2 = fmaf(dz, dz, dd.x + dd.y);
         num = fmaf(ez, dz + Yz, es.x + es.y);
-        Y0 = Y.x;
-        Y1 = Y.y;
+        Yxy = Y;
         Y2 = Yz;
     }
 };
@@ -256,6 +266,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
     constexpr int CS = Split<WPS>::CS;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
+    float2 fxy = make_float2(0.f, 0.f);  // FP32: packed (fx, fy)
     for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
         uint32_t *wptr = wp + 32 * (w0 >> 5);
         const uint32_t word = *wptr;
@@ -292,13 +303,16 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
                 tn = pp.k35 * (Ap + mq.x) * dl + pp.g15 * num * (Bp + mq.y);
             }
             const R coef = (live && ok) ? tn * xq.w * Tr<R>::rcp(dl * ly) : R(0);
-            fx += coef * k.Y0;
-            fy += coef * k.Y1;
-            fz += coef * k.Y2;
+            if constexpr (sizeof(R) == 4) k.accumulate(coef, fxy, fz);
+            else k.accumulate(coef, fx, fy, fz);
         }
         // bonds break rarely; two warps may own the halves of one word
         const uint32_t brk = bits & ~okm;
         if (kBreak && brk) atomicAnd(wptr, ~(CS == 32 ? brk : (brk << (w0 & 31))));
+    }
+    if constexpr (sizeof(R) == 4) {
+        fx += fxy.x;
+        fy += fxy.y;
     }
 }
 
