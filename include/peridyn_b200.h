@@ -75,8 +75,15 @@ enum { PD_MAT_BOND_BASED = 0, PD_MAT_ORDINARY_STATE_BASED = 1, PD_MAT_SKIP = 2 }
  *   cancellation-free stretch, FP64 position accumulator. */
 enum { PD_PREC_FP64_SERIAL = 0, PD_PREC_FP64 = 1, PD_PREC_FP32C = 2 };
 
-/* Boundary conditions: FixBC.jl, ToFroBC.jl (MoveBC = ToFroBC, freq=Inf). */
-enum { PD_BC_FIX = 0, PD_BC_TOFRO = 1 };
+/* Boundary conditions: FixBC.jl, ToFroBC.jl (MoveBC = ToFroBC, freq=Inf),
+ * DeltaScaleBC.jl, ScaleFixWaitBC.jl, ContainerBC.jl. */
+enum {
+    PD_BC_FIX = 0,
+    PD_BC_TOFRO = 1,
+    PD_BC_DELTA_SCALE = 2,
+    PD_BC_SCALE_FIX_WAIT = 3,
+    PD_BC_CONTAINER = 4
+};
 
 /* Contact models: contacts.jl ContactModel12 (two blocks) / ContactModel11
  * (self contact of one block); force law nonlinearspring.jl:124-145. */
@@ -147,6 +154,28 @@ PD_API pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block1, i
 PD_API pd_status pd_env_add_bc(pd_env *env, int32_t kind, const uint8_t *mask, const uint8_t *dims,
                         const double *rate, double freq, int64_t applyafter,
                         int32_t onlyatstart, int64_t *out_bc);
+
+/* DeltaScaleBC(bool, scale, fixpoint; dims, onlyatstart) (DeltaScaleBC.jl:
+ * 47-60): y = (last - fixpoint) * (1 + scale*dt*time_step) + fixpoint,
+ * v = 0, last = y at apply_bc_at0.  kind PD_BC_DELTA_SCALE; wait and
+ * scalemask are ignored.
+ * ScaleFixWaitBC(bool, scale, fixpoint, wait, scalebool; dims, applyafter,
+ * onlyatstart) (ScaleFixWaitBC.jl:46-71): y = last, v = 0, and at every
+ * step with time_step % wait == 0 the particles of scalemask are scaled
+ * about fixpoint by sqrt(1 + 2*scale*dt) and last is re-read.  kind
+ * PD_BC_SCALE_FIX_WAIT.  scale, fixpoint: 3 values; masks: N bytes. */
+PD_API pd_status pd_env_add_scaled_bc(pd_env *env, int32_t kind, const uint8_t *mask, const uint8_t *dims,
+                                      const double *scale, const double *fixpoint, int64_t wait,
+                                      const uint8_t *scalemask, int32_t onlyatstart, int64_t *out_bc);
+/* ContainerBC(bool; limits, dims, onlyatstart) (ContainerBC.jl:48-74): the
+ * velocity of a particle of the mask whose position leaves
+ * [limits[d], limits[3 + d]] in a constrained dimension d is set to 0 in
+ * those dimensions; positions are untouched.  limits: 3x2 column-major
+ * (lower bounds, then upper bounds), or NULL for the reference's
+ * limits=nothing form, which does nothing.  (The reference's constructor
+ * tests an undefined name `limit`; this is the documented behaviour.) */
+PD_API pd_status pd_env_add_container_bc(pd_env *env, const uint8_t *mask, const uint8_t *dims,
+                                         const double *limits, int32_t onlyatstart, int64_t *out_bc);
 
 /* Build everything on the device: families (GPU cell binning + sort,
  * peri.jl:459-576 and general_material.jl:85-90, unless set by

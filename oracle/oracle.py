@@ -198,6 +198,12 @@ class OracleEnv:
             Bc.onlyatstart = bool(bc.onlyatstart)
             Bc.direction = 1
             Bc.last = np.zeros((3, int(Bc.mask.sum())), order="F")
+            Bc.scale = np.asarray(getattr(bc, "scale", np.zeros(3)), dtype=np.float64)
+            Bc.fixpoint = np.asarray(getattr(bc, "fixpoint", np.zeros(3)), dtype=np.float64)
+            Bc.wait = int(getattr(bc, "wait", 1))
+            sb = getattr(bc, "scalebool", None)
+            Bc.smask = None if sb is None else np.asarray(sb, dtype=bool)
+            Bc.limits = getattr(bc, "limits", None)
             self.bcs.append(Bc)
 
     # ---------------------------------------------------------------- forces
@@ -279,15 +285,24 @@ class OracleEnv:
 
     # --------------------------------------------------------------- BCs
     def apply_bc_at0(self):
-        """FixBC.jl:63 / ToFroBC.jl:94: BC.last .= y[dims, bool]."""
+        """FixBC.jl:63 / ToFroBC.jl:94 / DeltaScaleBC.jl:71 /
+        ScaleFixWaitBC.jl:80: BC.last .= y[dims, bool]; ContainerBC.jl:84
+        does nothing."""
         for bc in self.bcs:
+            if bc.kind == 4:
+                continue
             for d in range(3):
                 if bc.dims[d]:
                     bc.last[d] = self.y[d, bc.mask]
 
     def _bc_pos(self, bc):
-        if bc.kind == 0:  # FixBC.jl:213
+        if bc.kind == 4:  # ContainerBC.jl:58-61: y unchanged
+            return
+        if bc.kind in (0, 3):  # FixBC.jl:213, ScaleFixWaitBC.jl:59
             new = bc.last
+        elif bc.kind == 2:  # DeltaScaleBC.jl:52-55
+            g = 1.0 + (bc.scale * self.dt) * float(self.time_step)
+            new = (bc.last - bc.fixpoint.reshape(3, 1)) * g.reshape(3, 1) + bc.fixpoint.reshape(3, 1)
         else:  # ToFroBC.jl:286-289
             new = bc.last + (self.dt * bc.direction * bc.rate).reshape(3, 1)
         idx = np.nonzero(bc.mask)[0]
@@ -301,12 +316,33 @@ class OracleEnv:
 
     def _bc_vel(self, bc):
         idx = np.nonzero(bc.mask)[0]
+        if bc.kind == 4:  # ContainerBC.jl:63-68
+            if bc.limits is None:
+                return
+            out = np.zeros(idx.size, dtype=bool)
+            for d in range(3):
+                if bc.dims[d]:
+                    yd = self.y[d, idx]
+                    out |= (yd < bc.limits[d, 0]) | (yd > bc.limits[d, 1])
+            for d in range(3):
+                if bc.dims[d]:
+                    self.v[d, idx[out]] = 0.0
+            return
         for d in range(3):
             if bc.dims[d]:
-                self.v[d, idx] = 0.0 if bc.kind == 0 else float(bc.direction) * bc.rate[d]
+                self.v[d, idx] = float(bc.direction) * bc.rate[d] if bc.kind == 1 else 0.0
 
     def _bc_check(self):
         for bc in self.bcs:
+            if bc.kind == 3 and self.time_step % bc.wait == 0:  # ScaleFixWaitBC.jl:63-68
+                sidx = np.nonzero(bc.smask)[0]
+                for d in range(3):
+                    if bc.dims[d]:
+                        g = math.sqrt(1.0 + (2.0 * bc.scale[d]) * self.dt)
+                        self.y[d, sidx] = (self.y[d, sidx] - bc.fixpoint[d]) * g + bc.fixpoint[d]
+                for d in range(3):
+                    if bc.dims[d]:
+                        bc.last[d] = self.y[d, bc.mask]
             if bc.kind == 1 and (self.time_step > bc.applyafter) and math.fmod(self.time_step, bc.freq) == 0:
                 bc.direction = -bc.direction
 

@@ -6,7 +6,7 @@ boundary conditions, Env, solvers, run!) and sequences device calls; all
 arithmetic runs in the CUDA library.
 """
 from ._abi import PDError, device_count, lib
-from .boundary_conditions import FixBC, MoveBC, ToFroBC
+from .boundary_conditions import ContainerBC, DeltaScaleBC, FixBC, MoveBC, ScaleFixWaitBC, ToFroBC
 from .contacts import (LinearSpringContactModel, NonLinearSpringContactModel, NonLinearSpringContactModel11,
                        NonLinearSpringContactModel12, ShortRangeContactModel)
 from .environment import Env, GeneralEnvironment

@@ -37,6 +37,9 @@ PRECISIONS = {"fp64_serial": PD_PREC_FP64_SERIAL, "fp64": PD_PREC_FP64, "fp32c":
 
 PD_BC_FIX = 0
 PD_BC_TOFRO = 1
+PD_BC_DELTA_SCALE = 2
+PD_BC_SCALE_FIX_WAIT = 3
+PD_BC_CONTAINER = 4
 
 PD_CONTACT_12 = 0
 PD_CONTACT_11 = 1
@@ -98,6 +101,9 @@ _SIGNATURES = {
     "pd_env_add_block": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_dp, c_dp, c_dp, c_dp, c_i64p,
                                           ctypes.POINTER(MaterialDesc), c_i64p]),
     "pd_env_set_family": (ctypes.c_int32, [c_vp, ctypes.c_int64, ctypes.c_int64, c_i64p, c_u8p]),
+    "pd_env_add_scaled_bc": (ctypes.c_int32, [c_vp, ctypes.c_int32, c_u8p, c_u8p, c_dp, c_dp, ctypes.c_int64, c_u8p,
+                                              ctypes.c_int32, c_i64p]),
+    "pd_env_add_container_bc": (ctypes.c_int32, [c_vp, c_u8p, c_u8p, c_dp, ctypes.c_int32, c_i64p]),
     "pd_env_add_contact": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
                                             c_i64p]),

@@ -375,6 +375,61 @@ extern "C" pd_status pd_env_add_bc(pd_env *env, int32_t kind, const uint8_t *mas
     return PD_OK;
 }
 
+static pd_status new_bc(pd_env *env, int32_t kind, const uint8_t *mask, const uint8_t *dims, int32_t onlyatstart,
+                        HostBC &bc) {
+    PD_TRY(check_env(env));
+    if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
+    if (!mask || !dims) return fail(PD_ERR_ARG, "mask/dims is NULL");
+    if (env->hbc.size() >= 64) return fail(PD_ERR_UNSUPPORTED, "at most 64 boundary conditions");
+    bc.kind = kind;
+    bc.dims = (dims[0] ? 1 : 0) | (dims[1] ? 2 : 0) | (dims[2] ? 4 : 0);
+    bc.freq = INFINITY;
+    bc.onlyatstart = onlyatstart;
+    for (int64_t e = 0; e < env->N_env; ++e)
+        if (mask[e]) bc.env_idx.push_back(e);
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_add_scaled_bc(pd_env *env, int32_t kind, const uint8_t *mask, const uint8_t *dims,
+                                          const double *scale, const double *fixpoint, int64_t wait,
+                                          const uint8_t *scalemask, int32_t onlyatstart, int64_t *out_bc) {
+    if (kind != PD_BC_DELTA_SCALE && kind != PD_BC_SCALE_FIX_WAIT)
+        return fail(PD_ERR_ARG, "kind must be PD_BC_DELTA_SCALE or PD_BC_SCALE_FIX_WAIT");
+    if (!scale || !fixpoint) return fail(PD_ERR_ARG, "scale/fixpoint is NULL");
+    if (kind == PD_BC_SCALE_FIX_WAIT && (!scalemask || wait == 0))
+        return fail(PD_ERR_ARG, "ScaleFixWaitBC needs scalebool and a nonzero wait");
+    HostBC bc;
+    PD_TRY(new_bc(env, kind, mask, dims, onlyatstart, bc));
+    for (int d = 0; d < 3; ++d) {
+        bc.scale[d] = scale[d];
+        bc.fix[d] = fixpoint[d];
+    }
+    if (kind == PD_BC_SCALE_FIX_WAIT) {
+        bc.wait = wait;
+        for (int64_t e = 0; e < env->N_env; ++e)
+            if (scalemask[e]) bc.scale_idx.push_back(e);
+    }
+    env->hbc.push_back(std::move(bc));
+    if (out_bc) *out_bc = (int64_t)env->hbc.size() - 1;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_add_container_bc(pd_env *env, const uint8_t *mask, const uint8_t *dims,
+                                             const double *limits, int32_t onlyatstart, int64_t *out_bc) {
+    HostBC bc;
+    PD_TRY(new_bc(env, PD_BC_CONTAINER, mask, dims, onlyatstart, bc));
+    if (limits) {
+        bc.has_limits = 1;
+        for (int d = 0; d < 3; ++d) {
+            bc.lo[d] = limits[d];
+            bc.hi[d] = limits[3 + d];
+        }
+    }
+    env->hbc.push_back(std::move(bc));
+    if (out_bc) *out_bc = (int64_t)env->hbc.size() - 1;
+    return PD_OK;
+}
+
 extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block1, int64_t block2,
                                         double exponent, double stiffness, double equi_dist,
                                         double distance, int64_t max_neighs, int64_t *out_contact) {
@@ -841,6 +896,13 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
             CK(cudaMemsetAsync(d.last.p, 0, idx.size() * sizeof(double4), st));
         }
         d.n = (int64_t)idx.size();
+        if (!hb.scale_idx.empty()) {
+            std::vector<int32_t> sidx(hb.scale_idx.size());
+            for (size_t j = 0; j < sidx.size(); ++j) sidx[j] = (int32_t)env->map_h[hb.scale_idx[j]];
+            PD_TRY(d.sidx.alloc(sidx.size()));
+            CK(cudaMemcpyAsync(d.sidx.p, sidx.data(), sidx.size() * 4, cudaMemcpyHostToDevice, st));
+            d.sn = (int64_t)sidx.size();
+        }
         env->bcs.push_back(std::move(d));
     }
     PD_TRY(pd::contacts_finalize(env));

@@ -93,12 +93,21 @@ struct HostBC {
     int64_t applyafter = 0;
     int dir = 1;
     std::vector<int64_t> env_idx;
+    double scale[3] = {0, 0, 0}, fix[3] = {0, 0, 0};  // DeltaScale / ScaleFixWait
+    int64_t wait = 1;                                   // ScaleFixWait
+    std::vector<int64_t> scale_idx;                     // ScaleFixWait scalebool
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};        // Container
+    int32_t has_limits = 0;
+    // check! (ScaleFixWaitBC.jl:63) at this time_step
+    bool scales_at(int64_t ts) const { return kind == PD_BC_SCALE_FIX_WAIT && wait != 0 && ts % wait == 0; }
 };
 
 struct DevBC {
     DBuf<int32_t> idx;
     DBuf<double4> last;
     int64_t n = 0;
+    DBuf<int32_t> sidx;
+    int64_t sn = 0;
 };
 
 struct HostContact {

@@ -360,7 +360,7 @@ __device__ __forceinline__ double &comp(double4 &a, int d) {
 }
 
 // boundary_conditions.jl:107-111 with FixBC.jl:213 / ToFroBC.jl:286-289
-__global__ void k_bc_pos(BCDev bc, double dt, int dir, double4 *__restrict__ y) {
+__global__ void k_bc_pos(BCDev bc, double dt, int dir, int64_t ts, double4 *__restrict__ y) {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= bc.n) return;
     int32_t i = bc.idx[j];
@@ -368,8 +368,13 @@ __global__ void k_bc_pos(BCDev bc, double dt, int dir, double4 *__restrict__ y) 
     double step = dt * (double)dir;
     for (int d = 0; d < 3; ++d) {
         if (!((bc.dims >> d) & 1)) continue;
-        if (bc.kind == PD_BC_FIX) {
+        if (bc.kind == PD_BC_FIX || bc.kind == PD_BC_SCALE_FIX_WAIT) {
+            // FixBC.jl:213, ScaleFixWaitBC.jl:59 xF = (last, last)
             comp(yi, d) = comp(last, d);
+        } else if (bc.kind == PD_BC_DELTA_SCALE) {
+            // DeltaScaleBC.jl:52-55: (last - fix) * (1 + scale*dt*time_step) + fix
+            const double g = 1.0 + (bc.scale[d] * dt) * (double)ts;
+            comp(yi, d) = (comp(last, d) - bc.fix[d]) * g + bc.fix[d];
         } else {
             double nl = comp(last, d) + step * bc.rate[d];
             comp(yi, d) = nl;
@@ -377,20 +382,46 @@ __global__ void k_bc_pos(BCDev bc, double dt, int dir, double4 *__restrict__ y) 
         }
     }
     y[i] = yi;
-    bc.last[j] = last;
+    if (bc.kind == PD_BC_TOFRO) bc.last[j] = last;
 }
 
 // boundary_conditions.jl:122-126 with FixBC.jl:214 / ToFroBC.jl:290
-__global__ void k_bc_vel(BCDev bc, int dir, double4 *__restrict__ v) {
+__global__ void k_bc_vel(BCDev bc, int dir, const double4 *__restrict__ y, double4 *__restrict__ v) {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= bc.n) return;
     int32_t i = bc.idx[j];
     double4 vi = v[i];
+    if (bc.kind == PD_BC_CONTAINER) {
+        // ContainerBC.jl:63-68: v[dims] = 0 where y left the limits
+        double4 yi = y[i];
+        bool out = false;
+        for (int d = 0; d < 3; ++d)
+            if ((bc.dims >> d) & 1) out |= (comp(yi, d) < bc.lo[d]) || (comp(yi, d) > bc.hi[d]);
+        if (!out) return;
+        for (int d = 0; d < 3; ++d)
+            if ((bc.dims >> d) & 1) comp(vi, d) = 0.0;
+        v[i] = vi;
+        return;
+    }
     for (int d = 0; d < 3; ++d) {
         if (!((bc.dims >> d) & 1)) continue;
-        comp(vi, d) = bc.kind == PD_BC_FIX ? 0.0 : (double)dir * bc.rate[d];
+        comp(vi, d) = bc.kind == PD_BC_TOFRO ? (double)dir * bc.rate[d] : 0.0;
     }
     v[i] = vi;
+}
+
+// ScaleFixWaitBC.jl:63-68 (check!): y[dims, scalebool] = (y - fix) * sqrt(1 + 2*scale*dt) + fix
+__global__ void k_bc_scale(BCDev bc, double dt, double4 *__restrict__ y) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= bc.sn) return;
+    const int32_t i = bc.sidx[j];
+    double4 yi = y[i];
+    for (int d = 0; d < 3; ++d) {
+        if (!((bc.dims >> d) & 1)) continue;
+        const double g = sqrt(1.0 + (2.0 * bc.scale[d]) * dt);
+        comp(yi, d) = (comp(yi, d) - bc.fix[d]) * g + bc.fix[d];
+    }
+    y[i] = yi;
 }
 
 // FixBC.jl:63 / ToFroBC.jl:94: BC.last .= y[dims, bool]
@@ -621,14 +652,22 @@ void launch_kick(cudaStream_t st, int64_t N, double c, const double4 *f, double4
     k_kick<<<grid_for(N, 256), 256, 0, st>>>(N, c, f, v); pd::note_launch();
 }
 
-void launch_bc_pos(cudaStream_t st, const BCDev &bc, double dt, int dir, double4 *y) {
-    if (bc.n <= 0) return;
-    k_bc_pos<<<grid_for(bc.n, 256), 256, 0, st>>>(bc, dt, dir, y); pd::note_launch();
+void launch_bc_pos(cudaStream_t st, const BCDev &bc, double dt, int dir, int64_t ts, double4 *y) {
+    if (bc.n <= 0 || bc.kind == PD_BC_CONTAINER) return;  // ContainerBC.jl:58-61 keeps y
+    k_bc_pos<<<grid_for(bc.n, 256), 256, 0, st>>>(bc, dt, dir, ts, y); pd::note_launch();
 }
 
-void launch_bc_vel(cudaStream_t st, const BCDev &bc, int dir, double4 *v) {
-    if (bc.n <= 0) return;
-    k_bc_vel<<<grid_for(bc.n, 256), 256, 0, st>>>(bc, dir, v); pd::note_launch();
+void launch_bc_vel(cudaStream_t st, const BCDev &bc, int dir, const double4 *y, double4 *v) {
+    if (bc.n <= 0 || (bc.kind == PD_BC_CONTAINER && !bc.has_limits)) return;
+    k_bc_vel<<<grid_for(bc.n, 256), 256, 0, st>>>(bc, dir, y, v); pd::note_launch();
+}
+
+void launch_bc_scale(cudaStream_t st, const BCDev &bc, double dt, double4 *y) {
+    if (bc.sn > 0) {
+        k_bc_scale<<<grid_for(bc.sn, 256), 256, 0, st>>>(bc, dt, y);
+        pd::note_launch();
+    }
+    launch_bc_snapshot(st, bc, y);
 }
 
 void launch_bc_snapshot(cudaStream_t st, const BCDev &bc, const double4 *y) {

@@ -93,9 +93,14 @@ constexpr int kMaxFastBC = 8;
 struct FBC {
     int32_t kind, dims;
     double rate[3];
+    double scale[3], fix[3];  // DeltaScale / ScaleFixWait
+    double lo[3], hi[3];      // Container limits
+    int32_t has_limits, pad;
     int64_t n;
     const int32_t *idx;  // ascending internal indices
     double4 *last;
+    int64_t sn;          // ScaleFixWait scalebool particles
+    const int32_t *sidx;
 };
 
 template <class R>
@@ -121,6 +126,7 @@ struct StepArgs {
     const uint8_t *bcbits;
     R c;
     double dt;
+    int64_t ts;  // time_step of the position BCs applied by this launch
     int nbc;
     uint32_t dir_vel, dir_pos;  // bit k set: BC k moves in the negative direction
     FBC bc[kMaxFastBC];
@@ -348,14 +354,30 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
 
 // BC velocity (boundary_conditions.jl:122-126): FixBC v = 0, ToFroBC v = dir*rate.
 template <class R>
-__device__ __forceinline__ void bc_velocity(const StepArgs<R> &a, uint8_t bits, R &v0, R &v1, R &v2) {
+// Fix / ScaleFixWait / DeltaScale: v = 0; ToFro: v = dir*rate; Container
+// (ContainerBC.jl:63-68): v = 0 once the current position left the limits.
+__device__ __forceinline__ void bc_velocity(const StepArgs<R> &a, int64_t p, uint8_t bits, R &v0, R &v1, R &v2) {
     for (int k = 0; k < a.nbc; ++k) {
         if (!((bits >> k) & 1)) continue;
         const FBC &b = a.bc[k];
         const double dir = ((a.dir_vel >> k) & 1) ? -1.0 : 1.0;
         R vv[3] = {v0, v1, v2};
-        for (int d = 0; d < 3; ++d)
-            if ((b.dims >> d) & 1) vv[d] = b.kind == PD_BC_FIX ? R(0) : R(dir * b.rate[d]);
+        if (b.kind == PD_BC_CONTAINER) {
+            if (!b.has_limits) continue;
+            double u0, u1, u2;
+            load_u(a, p, u0, u1, u2);
+            const double4 x = a.x64[p];
+            const double y[3] = {x.x + u0, x.y + u1, x.z + u2};
+            bool out = false;
+            for (int d = 0; d < 3; ++d)
+                if ((b.dims >> d) & 1) out |= (y[d] < b.lo[d]) || (y[d] > b.hi[d]);
+            if (!out) continue;
+            for (int d = 0; d < 3; ++d)
+                if ((b.dims >> d) & 1) vv[d] = R(0);
+        } else {
+            for (int d = 0; d < 3; ++d)
+                if ((b.dims >> d) & 1) vv[d] = b.kind == PD_BC_TOFRO ? R(dir * b.rate[d]) : R(0);
+        }
         v0 = vv[0];
         v1 = vv[1];
         v2 = vv[2];
@@ -371,20 +393,24 @@ __device__ __forceinline__ void bc_position(const StepArgs<R> &a, int64_t p, uin
     for (int k = 0; k < a.nbc; ++k) {
         if (!((bits >> k) & 1)) continue;
         const FBC &b = a.bc[k];
+        if (b.kind == PD_BC_CONTAINER) continue;
         const int64_t r = lower_bound_i32(b.idx, b.n, (int32_t)p);
         double4 last = b.last[r];
         const double step = a.dt * (((a.dir_pos >> k) & 1) ? -1.0 : 1.0);
         for (int d = 0; d < 3; ++d) {
             if (!((b.dims >> d) & 1)) continue;
-            if (b.kind == PD_BC_FIX) {
+            if (b.kind == PD_BC_FIX || b.kind == PD_BC_SCALE_FIX_WAIT) {
                 y[d] = cmp(last, d);
+            } else if (b.kind == PD_BC_DELTA_SCALE) {
+                const double g = 1.0 + (b.scale[d] * a.dt) * (double)a.ts;
+                y[d] = (cmp(last, d) - b.fix[d]) * g + b.fix[d];
             } else {
                 const double nl = cmp(last, d) + step * b.rate[d];
                 y[d] = nl;
                 cmp(last, d) = nl;
             }
         }
-        if (b.kind != PD_BC_FIX) b.last[r] = last;
+        if (b.kind == PD_BC_TOFRO) b.last[r] = last;
     }
     u0 = y[0] - x.x;
     u1 = y[1] - x.y;
@@ -506,7 +532,7 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
     }
     const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
     R v0 = vp.x + a.c * fx, v1 = vp.y + a.c * fy, v2 = vp.z + a.c * fz;
-    if (bits) bc_velocity(a, bits, v0, v1, v2);
+    if (bits) bc_velocity(a, p, bits, v0, v1, v2);
     if (MODE == 2 || MODE == 4) {
         a.v[p] = V4{v0, v1, v2, R(0)};
         a.f[p] = V4{fx, fy, fz, R(0)};
@@ -985,11 +1011,21 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
         FBC &b = a.bc[k];
         b.kind = h.kind;
         b.dims = h.dims;
-        for (int d = 0; d < 3; ++d) b.rate[d] = h.rate[d];
+        for (int d = 0; d < 3; ++d) {
+            b.rate[d] = h.rate[d];
+            b.scale[d] = h.scale[d];
+            b.fix[d] = h.fix[d];
+            b.lo[d] = h.lo[d];
+            b.hi[d] = h.hi[d];
+        }
+        b.has_limits = h.has_limits;
         b.n = env->bcs[k].n;
         b.idx = env->bcs[k].idx.p;
         b.last = env->bcs[k].last.p;
+        b.sn = env->bcs[k].sn;
+        b.sidx = env->bcs[k].sidx.p;
     }
+    a.ts = env->ts;
     return a;
 }
 
@@ -1263,6 +1299,59 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     return PD_OK;
 }
 
+// ScaleFixWaitBC.jl:63-68 check! on the throughput state: scale the
+// scalebool particles' positions about the fix point (through their FP64
+// displacement), then re-read BC.last from the positions.
+template <class R>
+__global__ void k_fscale(StepArgs<R> a, int k) {
+    const FBC &b = a.bc[k];
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= b.sn) return;
+    const int64_t p = b.sidx[j];
+    double u[3];
+    load_u(a, p, u[0], u[1], u[2]);
+    const double4 x = a.x64[p];
+    const double xx[3] = {x.x, x.y, x.z};
+    for (int d = 0; d < 3; ++d) {
+        if (!((b.dims >> d) & 1)) continue;
+        const double g = sqrt(1.0 + (2.0 * b.scale[d]) * a.dt);
+        u[d] = ((xx[d] + u[d]) - b.fix[d]) * g + b.fix[d] - xx[d];
+    }
+    // the current record buffer holds the state between steps
+    StepArgs<R> c = a;
+    c.xn = const_cast<typename Tr<R>::V4 *>(a.xu);
+    store_u(c, p, u[0], u[1], u[2]);
+}
+
+template <class R>
+__global__ void k_fsnapshot(StepArgs<R> a, int k) {
+    const FBC &b = a.bc[k];
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= b.n) return;
+    const int64_t p = b.idx[j];
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    const double4 x = a.x64[p];
+    double4 last = b.last[j];
+    if (b.dims & 1) last.x = x.x + u0;
+    if (b.dims & 2) last.y = x.y + u1;
+    if (b.dims & 4) last.z = x.z + u2;
+    b.last[j] = last;
+}
+
+// Any ScaleFixWait check! at this time_step?
+bool scale_check_due(const pd_env *env) {
+    for (const auto &h : env->hbc)
+        if (h.scales_at(env->ts)) return true;
+    return false;
+}
+
+bool time_dependent_bcs(const pd_env *env) {
+    for (const auto &h : env->hbc)
+        if (h.kind == PD_BC_DELTA_SCALE || h.kind == PD_BC_SCALE_FIX_WAIT) return true;
+    return false;
+}
+
 // check!(env) then time_step += 1 (velocity_verlet.jl:81-85): ToFro
 // direction flips when time_step > applyafter and time_step % freq == 0.
 void advance_bc_clock(pd_env *env) {
@@ -1293,6 +1382,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
     cudaStream_t st = env->st;
     StepArgs<R> a0 = args(env, F);
     a0.dir_vel = a0.dir_pos = dir_bits(env);
+    a0.ts = 0;  // graphs run only without time-dependent BCs
     typename Fast<R>::Graph *hit = nullptr;
     for (auto &g : F.graphs)
         if (g.wps == F.wps && g.gate.size() == F.gitems_h.size() &&
@@ -1312,6 +1402,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
         for (int k = 0; k < kGraphSteps; ++k) {
             StepArgs<R> a = args(env, F);
             a.dir_vel = a.dir_pos = a0.dir_vel;
+            a.ts = 0;
             gate_launch(env, a, F);
             if (lps) launch_theta(st, F.wps, a);
             launch_step<R, 1>(st, F.wps, a);
@@ -1354,7 +1445,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
     // Steps without contacts run as replays of a captured graph of
     // kGraphSteps steps while the BC directions stay constant; the rest
     // (contacts, direction flips, the last step, profiling) launch directly.
-    const bool graphs = !contacts && !env->prof && !std::getenv("PD_NO_GRAPHS");
+    const bool graphs = !contacts && !env->prof && !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
     PD_TRY(gate_prepare(env, F));
     for (int64_t s = 0; s < nsteps;) {
         if (graphs && nsteps - 1 - s >= kGraphSteps && flip_free_steps(env, kGraphSteps)) {
@@ -1364,26 +1455,53 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
             continue;
         }
         const bool last = s == nsteps - 1;
+        // a ScaleFixWait check! after this step's velocity BC ends the
+        // fused step there (MODE 2/4), scales, and restarts with a prologue
+        const bool check = scale_check_due(env);
+        const bool stop = last || check;
         StepArgs<R> a = args(env, F);
         a.dir_vel = dir_bits(env);
         advance_bc_clock(env);
         a.dir_pos = dir_bits(env);
+        a.ts = env->ts;
         gate_launch(env, a, F);
         if (lps) launch_theta(st, wps, a);
         prof_begin(env, st);
         if (!contacts) {
-            if (last) launch_step<R, 2>(st, wps, a);
+            if (stop) launch_step<R, 2>(st, wps, a);
             else launch_step<R, 1>(st, wps, a);
             prof_end(env, st);
         } else {
             launch_step<R, 0>(st, wps, a);
             prof_end(env, st);
             PD_TRY(contacts_fast(env, a));
-            if (last) k_integrate<R, 4><<<grid, kT, 0, st>>>(a);
+            if (stop) k_integrate<R, 4><<<grid, kT, 0, st>>>(a);
             else k_integrate<R, 3><<<grid, kT, 0, st>>>(a);
             note_launch();
         }
-        if (!last) F.cur = 1 - F.cur;
+        if (check) {
+            for (size_t k = 0; k < env->hbc.size(); ++k) {
+                if (!env->hbc[k].scales_at(env->ts - 1)) continue;
+                const int64_t sn = env->bcs[k].sn, n = env->bcs[k].n;
+                if (sn > 0) {
+                    k_fscale<R><<<gridn(sn, 256), 256, 0, st>>>(a, (int)k);
+                    note_launch();
+                }
+                if (n > 0) {
+                    k_fsnapshot<R><<<gridn(n, 256), 256, 0, st>>>(a, (int)k);
+                    note_launch();
+                }
+            }
+            if (!last) {
+                StepArgs<R> b = args(env, F);
+                b.dir_pos = dir_bits(env);
+                k_prologue<R><<<grid, kT, 0, st>>>(b);
+                note_launch();
+                F.cur = 1 - F.cur;
+            }
+        } else if (!last) {
+            F.cur = 1 - F.cur;
+        }
         if ((s & 63) == 63) CK(cudaGetLastError());
         ++s;
     }

@@ -117,9 +117,14 @@ struct BCDev {
     int32_t kind;
     int32_t dims;      // bit d set: dimension d constrained
     double rate[3];
+    double scale[3], fix[3];  // DeltaScale / ScaleFixWait
+    double lo[3], hi[3];      // Container limits
+    int32_t has_limits, pad;
     int64_t n;
     const int32_t *idx;  // internal indices, ascending
     double4 *last;       // BC.last per constrained particle
+    int64_t sn;          // ScaleFixWait: particles scaled at check time
+    const int32_t *sidx;
 };
 
 // ---------------------------------------------------------------------
@@ -159,9 +164,13 @@ void launch_force_serial(cudaStream_t st, const Geo &g, const double4 *y, const 
 void launch_kick_drift(cudaStream_t st, int64_t N, double c, double dt, const double4 *f,
                        double4 *v, double4 *y);
 void launch_kick(cudaStream_t st, int64_t N, double c, const double4 *f, double4 *v);
-void launch_bc_pos(cudaStream_t st, const BCDev &bc, double dt, int dir, double4 *y);
-void launch_bc_vel(cudaStream_t st, const BCDev &bc, int dir, double4 *v);
+// ts: time_step when the position BC is applied (DeltaScale)
+void launch_bc_pos(cudaStream_t st, const BCDev &bc, double dt, int dir, int64_t ts, double4 *y);
+// y: positions at the velocity BC (Container)
+void launch_bc_vel(cudaStream_t st, const BCDev &bc, int dir, const double4 *y, double4 *v);
 void launch_bc_snapshot(cudaStream_t st, const BCDev &bc, const double4 *y);
+// ScaleFixWait check!: scale the scalebool particles, then re-read last.
+void launch_bc_scale(cudaStream_t st, const BCDev &bc, double dt, double4 *y);
 void launch_momentum(cudaStream_t st, int64_t N, const double *mass, const double4 *v,
                      double4 *p);
 void launch_zero4(cudaStream_t st, int64_t N, double4 *a);

@@ -63,16 +63,30 @@ pd::BCDev bc_view(pd_env *env, size_t k) {
     b.kind = h.kind;
     b.dims = h.dims;
     for (int i = 0; i < 3; ++i) b.rate[i] = h.rate[i];
+    for (int i = 0; i < 3; ++i) {
+        b.scale[i] = h.scale[i];
+        b.fix[i] = h.fix[i];
+        b.lo[i] = h.lo[i];
+        b.hi[i] = h.hi[i];
+    }
+    b.has_limits = h.has_limits;
+    b.pad = 0;
     b.n = d.n;
     b.idx = d.idx.p;
     b.last = d.last.p;
+    b.sn = d.sn;
+    b.sidx = d.sidx.p;
     return b;
 }
 
 // ToFroBC.jl:101-105 check!: flip when time_step > applyafter and
 // time_step % freq == 0 (Int % Float64 is rem).
+// ScaleFixWaitBC.jl:63-68 check!: at time_step % wait == 0 scale the
+// scalebool particles about the fix point and re-read last.
 void bc_check(pd_env *env) {
-    for (auto &h : env->hbc) {
+    for (size_t k = 0; k < env->hbc.size(); ++k) {
+        auto &h = env->hbc[k];
+        if (h.scales_at(env->ts)) launch_bc_scale(env->st, bc_view(env, k), env->dt, env->y.p);
         if (h.kind != PD_BC_TOFRO) continue;
         double r = std::fmod((double)env->ts, h.freq);
         if ((env->ts > h.applyafter) && (r == 0.0)) h.dir = -h.dir;
@@ -238,7 +252,9 @@ extern "C" pd_status pd_env_apply_bc_at0(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));
     PD_TRY(sync_state_to_fp64(env, false));
-    for (size_t k = 0; k < env->hbc.size(); ++k) launch_bc_snapshot(env->st, bc_view(env, k), env->y.p);
+    for (size_t k = 0; k < env->hbc.size(); ++k)
+        if (env->hbc[k].kind != PD_BC_CONTAINER)  // ContainerBC.jl:84 does nothing
+            launch_bc_snapshot(env->st, bc_view(env, k), env->y.p);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(env->st));
     return PD_OK;
@@ -255,10 +271,11 @@ extern "C" pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps) {
     for (int64_t s = 0; s < nsteps; ++s) {
         launch_kick_drift(env->st, env->N, c, dt, env->f.p, env->v.p, env->y.p);
         for (size_t k = 0; k < env->hbc.size(); ++k)
-            launch_bc_pos(env->st, bc_view(env, k), dt, env->hbc[k].dir, env->y.p);
+            launch_bc_pos(env->st, bc_view(env, k), dt, env->hbc[k].dir, env->ts, env->y.p);
         PD_TRY(update_acc_serial(env));
         launch_kick(env->st, env->N, c, env->f.p, env->v.p);
-        for (size_t k = 0; k < env->hbc.size(); ++k) launch_bc_vel(env->st, bc_view(env, k), env->hbc[k].dir, env->v.p);
+        for (size_t k = 0; k < env->hbc.size(); ++k)
+            launch_bc_vel(env->st, bc_view(env, k), env->hbc[k].dir, env->y.p, env->v.p);
         bc_check(env);
         env->ts += 1;
         if ((s & 63) == 63) CK(cudaGetLastError());
@@ -280,8 +297,8 @@ extern "C" pd_status pd_env_qsdrag(pd_env *env, double step_size, double drag, i
     const int64_t N = env->N;
     // :112-115 apply BCs (position then velocity, per BC)
     for (size_t k = 0; k < env->hbc.size(); ++k) {
-        launch_bc_pos(st, bc_view(env, k), env->dt, env->hbc[k].dir, env->y.p);
-        launch_bc_vel(st, bc_view(env, k), env->hbc[k].dir, env->v.p);
+        launch_bc_pos(st, bc_view(env, k), env->dt, env->hbc[k].dir, env->ts, env->y.p);
+        launch_bc_vel(st, bc_view(env, k), env->hbc[k].dir, env->y.p, env->v.p);
     }
     const double dt = step_size;
     const double ps = env->hb[0].particle_size;

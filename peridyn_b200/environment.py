@@ -69,8 +69,21 @@ class GeneralEnvironment:
                 raise ValueError("boundary condition mask must cover every particle of the environment")
             rate = np.ascontiguousarray(bc.rate, dtype=np.float64)
             dims = np.ascontiguousarray(bc.dims, dtype=np.uint8)
-            _abi.check(L.pd_env_add_bc(self._h, bc.kind, _abi.u8ptr(bc.bool), _abi.u8ptr(dims), _abi.dptr(rate),
-                                       bc.freq, bc.applyafter, int(bc.onlyatstart), None))
+            if bc.kind in (_abi.PD_BC_DELTA_SCALE, _abi.PD_BC_SCALE_FIX_WAIT):
+                sb = getattr(bc, "scalebool", None)
+                if sb is not None and sb.size != self.N:
+                    raise ValueError("scalebool must cover every particle of the environment")
+                _abi.check(L.pd_env_add_scaled_bc(self._h, bc.kind, _abi.u8ptr(bc.bool), _abi.u8ptr(dims),
+                                                  _abi.dptr(bc.scale), _abi.dptr(bc.fixpoint),
+                                                  int(getattr(bc, "wait", 1)), _abi.u8ptr(sb),
+                                                  int(bc.onlyatstart), None))
+            elif bc.kind == _abi.PD_BC_CONTAINER:
+                lim = None if bc.limits is None else np.asfortranarray(bc.limits, dtype=np.float64)
+                _abi.check(L.pd_env_add_container_bc(self._h, _abi.u8ptr(bc.bool), _abi.u8ptr(dims), _abi.dptr(lim),
+                                                     int(bc.onlyatstart), None))
+            else:
+                _abi.check(L.pd_env_add_bc(self._h, bc.kind, _abi.u8ptr(bc.bool), _abi.u8ptr(dims),
+                                           _abi.dptr(rate), bc.freq, bc.applyafter, int(bc.onlyatstart), None))
         blocks = {id(m): b for b, m in enumerate(self.material_blocks)}
         for cm in self.short_range_contact:
             if isinstance(cm, NonLinearSpringContactModel12):

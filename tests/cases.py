@@ -16,3 +16,29 @@ def random_cloud():
                              np.ones(n, dtype=np.int64), 2.6e-3, max_neigh=300)
     mat = pb.PeridynamicsMaterial(gen, pb.OrdinaryStateBasedSpecific([20e9], [9e9], [0.004], [2000.0]))
     return {"materials": [mat], "contacts": [], "bcs": [], "dt": 2e-8, "steps": 20}
+
+
+def bar_with_bcs(kind, nx=20, ny=6, nz=6, steps=60):
+    """LPS bar with one of the scaling / container boundary conditions
+    beside a FixBC on the x = min layers."""
+    from peridyn_b200 import configs
+
+    w = configs.lps_bar(nx=nx, ny=ny, nz=nz, steps=steps)
+    mat = w["materials"][0]
+    x = mat.general.x
+    h = mat.general.horizon
+    xmin, xmax = x[0].min(), x[0].max()
+    fix = pb.FixBC(x[0] < xmin + h)
+    right = x[0] > xmax - h
+    cen = x.mean(axis=1)
+    if kind == "delta":
+        bc = pb.DeltaScaleBC(right, [2.0e3, 500.0, 0.0], [xmin, cen[1], cen[2]])
+    elif kind == "scalefixwait":
+        bc = pb.ScaleFixWaitBC(right, [3.0e3, 0.0, 0.0], [xmin, cen[1], cen[2]], 10, x[0] > cen[0])
+    else:
+        # the pull drives the right end out of the box; its velocity is zeroed there
+        lim = np.array([[xmin - h, xmax + 2.0e-7], [x[1].min() - h, x[1].max() + h], [x[2].min() - h, x[2].max() + h]])
+        mat.general.velocity[0] = np.where(right, 2.0, 0.0)
+        bc = pb.ContainerBC(x[0] > cen[0], limits=lim)
+    w["bcs"] = [fix, bc]
+    return w

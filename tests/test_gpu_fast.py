@@ -9,7 +9,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import configs, lattice
-from tests.cases import random_cloud
+from tests.cases import bar_with_bcs, random_cloud
 
 pytestmark = pytest.mark.gpu
 
@@ -204,4 +204,16 @@ def test_rigid_gate_fast_long_run(precision):
     pb.velocity_verlet_step(env, nsteps=100)
     assert not env.deformed()[0]
     assert np.all(env.f == 0.0)
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("kind", ["delta", "scalefixwait", "container"])
+def test_scaling_and_container_bcs_fast(oracle, precision, kind):
+    w = bar_with_bcs(kind)
+    env, ora = _run_pair(oracle, w, precision, 95)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= TOL[precision], f"displacement rel-L2 {eu:.3e}"
+    assert ev <= TOL[precision], f"velocity rel-L2 {ev:.3e}"
+    assert mism == 0
     env.close()

@@ -8,7 +8,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import _abi, configs, lattice
-from tests.cases import random_cloud
+from tests.cases import bar_with_bcs, random_cloud
 
 pytestmark = pytest.mark.gpu
 
@@ -329,3 +329,25 @@ def test_family_overflow_is_reported():
     with pytest.raises(pb.PDError) as e:
         pb.Env(1, [mat], [], [], 1e-3)
     assert e.value.status == _abi.PD_ERR_FAMILY_OVERFLOW
+
+
+@pytest.mark.parametrize("kind", ["delta", "scalefixwait", "container"])
+def test_scaling_and_container_bcs_bit_exact(oracle, kind):
+    # DeltaScaleBC.jl, ScaleFixWaitBC.jl (check! every 10 steps), ContainerBC.jl
+    w = bar_with_bcs(kind)
+    env, ora = _pair(oracle, w)
+    ora.apply_bc_at0()
+    pb.apply_bc_at0(env, 0)
+    ora.update_acc()
+    pb.update_acc(env)
+    for _ in range(45):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=25)
+    pb.velocity_verlet_step(env, nsteps=20)
+    _assert_state_equal(env, ora, kind)
+    _assert_bonds_equal(env, ora)
+    it_o = ora.minimize(1e-7, 10.0, max_iter=5)
+    it_g = pb.minimize(env, pb.QSDrag(1e-7, 10.0, max_iter=5))
+    assert it_o == it_g
+    _assert_state_equal(env, ora, kind + " after QSDrag")
+    env.close()

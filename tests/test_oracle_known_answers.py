@@ -215,3 +215,53 @@ def test_contact12_neighs_bruteforce(oracle):
         top = np.sort(cand)[::-1][:rows]
         expect[: top.size] = top
         assert np.array_equal(nb[:, i], expect)
+
+
+def test_scaling_bcs_known_answers(oracle):
+    # DeltaScaleBC.jl:52-55: y = (last - fix) * (1 + scale*dt*time_step) + fix
+    from tests.cases import bar_with_bcs
+
+    w = bar_with_bcs("delta")
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    ora.apply_bc_at0()
+    bc = ora.bcs[1]
+    last = bc.last.copy()
+    idx = np.nonzero(bc.mask)[0]
+    for ts in range(3):
+        ora.vv_step()  # position BC applied with time_step = ts
+        g = 1.0 + (bc.scale * ora.dt) * float(ts)
+        want = (last - bc.fixpoint[:, None]) * g[:, None] + bc.fixpoint[:, None]
+        assert np.array_equal(ora.y[:, idx], want)
+        assert np.all(ora.v[:, idx] == 0.0)
+    # ScaleFixWaitBC.jl:63-68: check! at time_step 0 scales the scalebool set
+    w = bar_with_bcs("scalefixwait")
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    ora.apply_bc_at0()
+    bc = ora.bcs[1]
+    y0 = ora.y.copy()
+    ora.vv_step()
+    s = np.nonzero(bc.smask & ~ora.bcs[0].mask)[0]
+    g = np.sqrt(1.0 + 2.0 * bc.scale[0] * ora.dt)
+    assert g > 1.0
+    # x of the scaled particles moved away from the fix point by the factor
+    ratio = (ora.y[0, s] - bc.fixpoint[0]) / (y0[0, s] - bc.fixpoint[0])
+    assert np.all(ratio > 1.0 + 0.5 * (g - 1.0))
+    assert np.array_equal(bc.last, ora.y[:, bc.mask])
+
+
+def test_container_bc_zeroes_escaping_velocities(oracle):
+    from tests.cases import bar_with_bcs
+
+    w = bar_with_bcs("container")
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    ora.apply_bc_at0()
+    bc = ora.bcs[1]
+    idx = np.nonzero(bc.mask)[0]
+    outside_seen = False
+    for _ in range(40):
+        ora.vv_step()
+        yb = ora.y[:, idx]
+        out = np.any((yb < bc.limits[:, :1]) | (yb > bc.limits[:, 1:]), axis=0)
+        assert np.all(ora.v[:, idx[out]] == 0.0)
+        outside_seen |= bool(out.any())
+    assert outside_seen
