@@ -337,6 +337,22 @@ PD_API pd_status pd_server_wait(pd_server *srv, int64_t job, double timeout_s, p
  * damage: N; any may be NULL); releases the job's record. */
 PD_API pd_status pd_server_result(pd_server *srv, int64_t job, double *y, double *v, double *damage);
 PD_API pd_status pd_server_cancel(pd_server *srv, int64_t job);
+/* ---------------------------------------------------------------------- */
+/* Output staging (extension): the save_state! snapshot (io.jl:44-54)       */
+/* without stalling the time loop.                                        */
+/* ---------------------------------------------------------------------- */
+/* Enqueue a snapshot of y, v, f (and damage) into staging slot 0 or 1: the
+ * state is packed on the environment's stream and copied to pinned host
+ * memory on a separate copy stream, so later steps run while the copy is in
+ * flight.  A slot holds one snapshot; staging into a slot whose previous
+ * snapshot was not read first waits for that copy. */
+PD_API pd_status pd_env_stage_state(pd_env *env, int32_t slot);
+/* Wait for the slot's copy and return it in environment order (y, v, f:
+ * 3 x N column-major; damage: N; any may be NULL) with the time_step it was
+ * taken at.  PD_ERR_STATE when nothing is staged in the slot. */
+PD_API pd_status pd_env_stage_read(pd_env *env, int32_t slot, double *y, double *v, double *f, double *damage,
+                                   int64_t *time_step);
+
 /* Cancels queued and running jobs and joins the worker. */
 PD_API pd_status pd_server_destroy(pd_server *srv);
 

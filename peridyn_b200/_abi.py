@@ -141,6 +141,8 @@ _SIGNATURES = {
     "pd_kernel_launches": (ctypes.c_int32, [c_i64p]),
     "pd_env_profile": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
     "pd_env_profile_read": (ctypes.c_int32, [c_vp, c_dp, c_i64p]),
+    "pd_env_stage_state": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
+    "pd_env_stage_read": (ctypes.c_int32, [c_vp, ctypes.c_int32, c_dp, c_dp, c_dp, c_dp, c_i64p]),
     "pd_env_set_kernel_shape": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.c_int32]),
     "pd_env_kernel_shape": (ctypes.c_int32, [c_vp, c_i32p, c_i32p]),
     "pd_server_create": (ctypes.c_int32, [ctypes.POINTER(c_vp), ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,

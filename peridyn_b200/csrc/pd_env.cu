@@ -248,6 +248,15 @@ extern "C" pd_status pd_env_destroy(pd_env *env) {
     if (!env) return PD_OK;
     cudaSetDevice(env->device);
     if (env->st) cudaStreamSynchronize(env->st);
+    if (env->copy_st) {
+        cudaStreamSynchronize(env->copy_st);
+        cudaStreamDestroy(env->copy_st);
+    }
+    for (auto &s : env->slots) {
+        if (s.host) cudaFreeHost(s.host);
+        if (s.packed) cudaEventDestroy(s.packed);
+        if (s.done) cudaEventDestroy(s.done);
+    }
     env->release_device();
     for (cudaEvent_t e : env->prof_ev) cudaEventDestroy(e);
     if (env->st) cudaStreamDestroy(env->st);
@@ -1265,3 +1274,56 @@ int64_t footprint_estimate(const pd_env *env) {
     return bytes;
 }
 }  // namespace pd
+
+// ---------------------------------------------------------------------
+// output staging
+// ---------------------------------------------------------------------
+extern "C" pd_status pd_env_stage_state(pd_env *env, int32_t slot) {
+    PD_TRY(need_final(env));
+    if (slot < 0 || slot > 1) return fail(PD_ERR_ARG, "slot must be 0 or 1");
+    CK(cudaSetDevice(env->device));
+    auto &S = env->slots[slot];
+    const int64_t NE = env->N_env, N = env->N;
+    const size_t count = (size_t)(9 * NE + N);  // y, v, f packed (3 x NE each) + damage (internal order)
+    if (!S.host) {
+        if (!env->copy_st) CK(cudaStreamCreateWithFlags(&env->copy_st, cudaStreamNonBlocking));
+        PD_TRY(S.dev.alloc(count));
+        CK(cudaMallocHost(&S.host, count * sizeof(double)));
+        CK(cudaEventCreateWithFlags(&S.packed, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming));
+    }
+    if (S.pending) CK(cudaEventSynchronize(S.done));  // the slot's previous copy is still in flight
+    PD_TRY(pd::sync_state_to_fp64(env, false));
+    launch_pack3(env->st, NE, env->y.p, env->map.p, S.dev.p);
+    launch_pack3(env->st, NE, env->v.p, env->map.p, S.dev.p + 3 * NE);
+    launch_pack3(env->st, NE, env->f.p, env->map.p, S.dev.p + 6 * NE);
+    launch_damage(env->st, N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, env->intact0.p, env->tinfo.p,
+                  S.dev.p + 9 * NE);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(S.packed, env->st));
+    CK(cudaStreamWaitEvent(env->copy_st, S.packed, 0));
+    CK(cudaMemcpyAsync(S.host, S.dev.p, count * sizeof(double), cudaMemcpyDeviceToHost, env->copy_st));
+    CK(cudaEventRecord(S.done, env->copy_st));
+    S.pending = true;
+    S.ts = env->ts;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_stage_read(pd_env *env, int32_t slot, double *y, double *v, double *f, double *damage,
+                                       int64_t *time_step) {
+    PD_TRY(need_final(env));
+    if (slot < 0 || slot > 1) return fail(PD_ERR_ARG, "slot must be 0 or 1");
+    auto &S = env->slots[slot];
+    if (!S.pending) return fail(PD_ERR_STATE, "nothing staged in slot %d", slot);
+    CK(cudaSetDevice(env->device));
+    CK(cudaEventSynchronize(S.done));
+    const int64_t NE = env->N_env;
+    if (y) std::memcpy(y, S.host, 3 * NE * sizeof(double));
+    if (v) std::memcpy(v, S.host + 3 * NE, 3 * NE * sizeof(double));
+    if (f) std::memcpy(f, S.host + 6 * NE, 3 * NE * sizeof(double));
+    if (damage)
+        for (int64_t e = 0; e < NE; ++e) damage[e] = S.host[9 * NE + env->map_h[e]];
+    if (time_step) *time_step = S.ts;
+    S.pending = false;
+    return PD_OK;
+}

@@ -188,6 +188,17 @@ struct pd_env {
     double prof_ms = 0.0;
     int64_t prof_launches = 0;
 
+    // output staging (pd_env_stage_state): device pack buffers, pinned host
+    // copies, completion events, one copy stream
+    struct StageSlot {
+        pd::DBuf<double> dev;
+        double *host = nullptr;
+        cudaEvent_t packed = nullptr, done = nullptr;
+        bool pending = false;
+        int64_t ts = 0;
+    } slots[2];
+    cudaStream_t copy_st = nullptr;
+
     // fast (FP64 / FP32C) state; see pd_fast.cu
     bool fast_valid = false;
     void *fast = nullptr;

@@ -121,6 +121,21 @@ class GeneralEnvironment:
         _abi.check(L.pd_env_get_family(self._h, block, _abi.i64ptr(fam), _abi.u8ptr(intact)))
         return fam, intact.astype(bool)
 
+    def stage_state(self, slot):
+        """Start an asynchronous snapshot of y, v, f and damage into staging
+        slot 0 or 1 (the copy overlaps later steps)."""
+        _abi.check(_abi.lib().pd_env_stage_state(self._h, int(slot)))
+
+    def read_stage(self, slot):
+        """Wait for a staged snapshot and return it (environment order)."""
+        n = self.N
+        y, v, f = (np.zeros((3, n), order="F") for _ in range(3))
+        d = np.zeros(n)
+        ts = ctypes.c_int64()
+        _abi.check(_abi.lib().pd_env_stage_read(self._h, int(slot), _abi.dptr(y), _abi.dptr(v), _abi.dptr(f),
+                                                _abi.dptr(d), ctypes.byref(ts)))
+        return {"position": y, "velocity": v, "acceleration": f, "damage": d, "time_step": int(ts.value)}
+
     def _detach(self):
         """Give up ownership of the library handle (it now belongs to a
         server) and return it."""

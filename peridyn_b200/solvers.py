@@ -106,13 +106,52 @@ def save_state(env, writer=None, filename=None):
     return damage
 
 
+class _StagedWriter:
+    """save_state! through the output staging slots: the snapshot is
+    copied to pinned memory while the next steps run, and the writer is
+    called for it just before its slot is needed again (or at the end)."""
+
+    def __init__(self, writer):
+        self.writer = writer
+        self.pending = {}  # id(env) -> list of (slot, filename, env)
+        self.next_slot = {}
+
+    def save(self, env, filename):
+        update_acc(env)
+        q = self.pending.setdefault(id(env), [])
+        slot = self.next_slot.get(id(env), 0)
+        for item in [p for p in q if p[0] == slot]:
+            self._emit(item)
+            q.remove(item)
+        env.stage_state(slot)
+        q.append((slot, filename, env))
+        self.next_slot[id(env)] = 1 - slot
+
+    def _emit(self, item):
+        slot, filename, env = item
+        d = env.read_stage(slot)
+        self.writer(filename, {"id": np.arange(1, env.N + 1), "type": env.type, "position": d["position"],
+                               "velocity": d["velocity"], "acceleration": d["acceleration"], "mass": env.mass,
+                               "volume": env.volume, "damage": d["damage"]})
+
+    def flush(self):
+        for q in self.pending.values():
+            for item in q:  # in the order they were taken
+                self._emit(item)
+            q.clear()
+
+
 def _print_data_file(envs, step, writer, ext):
     for env in envs:
-        save_state(env, writer, f"env_{env.id}_step_{step}.{ext}")
+        name = f"env_{env.id}_step_{step}.{ext}"
+        if isinstance(writer, _StagedWriter):
+            writer.save(env, name)
+        else:
+            save_state(env, writer, name)
 
 
 def run(envs, N, solver, filewrite_freq=10, neigh_update_freq=1, average_prop_freq=1, out_dir="datafile",
-        start_at=0, write_from=0, ext="jld", max_part=30, writer=None, logger=None):
+        start_at=0, write_from=0, ext="jld", max_part=30, writer=None, logger=None, staged_io=True):
     """solvers.jl:97-187 ``run!`` with the reference's cadence: a force
     evaluation at every file write (including the initial two), contact
     neighbour updates every ``neigh_update_freq`` steps, diagnostics every
@@ -120,6 +159,10 @@ def run(envs, N, solver, filewrite_freq=10, neigh_update_freq=1, average_prop_fr
     event between them are issued as one device call."""
     if isinstance(envs, GeneralEnvironment):
         envs = [envs]
+    # with staged_io the snapshots reach the writer through pinned staging
+    # buffers, overlapping the copies with the next steps
+    if writer is not None and staged_io:
+        writer = _StagedWriter(writer)
     _print_data_file(envs, "start_with", writer, ext)
     update_neighs(envs, max_part)
     for env in envs:
@@ -155,6 +198,8 @@ def run(envs, N, solver, filewrite_freq=10, neigh_update_freq=1, average_prop_fr
             update_neighs(envs, max_part)
         i += 1
     _print_data_file(envs, "end_with", writer, ext)
+    if isinstance(writer, _StagedWriter):
+        writer.flush()
 
 
 def simulate(*args, out_dir="datafile", append_date=True, **kwargs):

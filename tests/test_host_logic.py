@@ -29,3 +29,16 @@ def test_serving_stream_is_seeded_and_bounded():
     # mean inter-arrival near 1/50 s
     gaps = np.diff([0.0] + a1)
     assert 0.01 < gaps.mean() < 0.04
+
+
+def test_write_ovito_layout(tmp_path):
+    from peridyn_b200 import io
+
+    y = np.array([[0.0, 1.5e-5], [2.0, -3.25], [1e-3, 4.0]])
+    p = tmp_path / "s.data"
+    io.write_ovito(str(p), id=np.array([1, 2]), position=y, damage=np.array([0.0, 0.5]))
+    lines = p.read_text().splitlines()
+    assert lines[0] == "2 "
+    assert lines[1] == "# damage | id | position"
+    assert lines[2] == "0.0 1 0.0 2.0 0.001 "
+    assert lines[3] == "0.5 2 1.5e-5 -3.25 4.0 "
