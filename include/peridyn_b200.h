@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define PD_ABI_VERSION 1
+#define PD_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PD_API __attribute__((visibility("default")))
@@ -62,8 +62,9 @@ enum {
 };
 
 /* Material kinds: src/materials/bond_based.jl, ordinary_state_based.jl,
- * skip_specific.jl. */
-enum { PD_MAT_BOND_BASED = 0, PD_MAT_ORDINARY_STATE_BASED = 1, PD_MAT_SKIP = 2 };
+ * skip_specific.jl, elasto_plastic.jl (ElastoPlasticSolidSpecific, Von
+ * Mises; serial FP64 mode only). */
+enum { PD_MAT_BOND_BASED = 0, PD_MAT_ORDINARY_STATE_BASED = 1, PD_MAT_SKIP = 2, PD_MAT_ELASTO_PLASTIC = 3 };
 
 /* Arithmetic modes.
  * PD_PREC_FP64_SERIAL: FP64, no fused multiply-add, every particle's
@@ -108,6 +109,8 @@ typedef struct pd_material_desc {
     double horizon;
     double particle_size;           /* GeneralMaterial particle_size              */
     int64_t max_neigh;              /* GeneralMaterial max_neigh                  */
+    const double *plastic_psi;      /* ELASTO_PLASTIC: psi = 75/(8 pi) sigma_e^2 /
+                                       horizon^5 per type pair (elasto_plastic.jl:60-68) */
 } pd_material_desc;
 
 /* ---------------------------------------------------------------------- */
@@ -193,6 +196,9 @@ PD_API pd_status pd_env_get_family(pd_env *env, int64_t block, int64_t *family, 
 PD_API pd_status pd_env_get_weighted_volume(pd_env *env, int64_t block, double *m);
 /* Dilatation theta of an LPS block as of the last force evaluation (n). */
 PD_API pd_status pd_env_get_theta(pd_env *env, int64_t block, double *theta);
+/* Plastic deviatoric strain edp of an elasto-plastic block in the reference
+ * layout (rows x n, column-major, aligned with pd_env_get_family). */
+PD_API pd_status pd_env_get_plastic_strain(pd_env *env, int64_t block, double *edp);
 
 /* ---------------------------------------------------------------------- */
 /* State                                                                   */

@@ -41,6 +41,10 @@ _SIG = {
     "or_force_density_T": (None, [ctypes.c_int, I64, I64, c_dp, c_dp, c_dp, c_i64p, c_u8p, c_i64p, I64, c_dp, c_dp,
                                   c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, ctypes.c_int]),
     "or_isapprox_rigid": (ctypes.c_int, [I64, c_dp, c_dp]),
+    "or_td_norm2": (None, [I64, I64, c_dp, c_dp, c_i64p, c_u8p, c_i64p, I64, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp,
+                           c_dp]),
+    "or_force_density_ep": (None, [I64, I64, c_dp, c_dp, c_dp, c_i64p, c_u8p, c_i64p, I64, c_dp, c_dp, c_dp, c_dp,
+                                   c_dp, c_dp, c_dp, c_dp, c_dp, c_dp]),
     "or_contact12_neighs": (None, [I64, c_dp, I64, c_dp, D, I64, c_i64p]),
     "or_contact12_force": (None, [I64, I64, c_i64p, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, D, D, D]),
     "or_contact11_neighs": (None, [I64, c_dp, I64, c_i64p, c_u8p, D, D, I64, I64, c_i64p]),
@@ -82,7 +86,7 @@ def _u(a):
     return None if a is None else a.ctypes.data_as(c_u8p)
 
 
-PMB, LPS, SKIP = 0, 1, 2
+PMB, LPS, SKIP, EP = 0, 1, 2, 3
 
 
 def cal_family(x, horizon, max_neigh):
@@ -151,6 +155,10 @@ class OracleEnv:
                 B.intact = np.asfortranarray(intact, dtype=np.uint8)
             B.m = weighted_volume(B.x, B.vol, B.family)
             B.theta = np.zeros(B.n)
+            if B.kind == EP:  # elasto_plastic.jl:60-68 init
+                B.psi = np.asfortranarray(spc.psi, dtype=np.float64)
+                B.edp = np.zeros(B.family.shape, order="F")
+                B.td_norm2 = np.zeros(B.n)
             B.deformed = bool(gen.deformed[0])
             self.blocks.append(B)
             ys.append(gen.y)
@@ -219,9 +227,16 @@ class OracleEnv:
         f_ = self.f[:, s]
         assert y_.flags.f_contiguous and f_.flags.f_contiguous
         M = B.family.shape[0]
-        if B.kind == LPS:
+        if B.kind in (LPS, EP):
             lib().or_dilatation(B.n, _d(y_), _d(B.x), _u(B.intact), _i(B.family), M, _d(B.vol), _d(B.m),
                                 _d(B.theta), self.nthreads)
+        if B.kind == EP:  # elasto_plastic.jl:166-172 out_of_loop!, then the bond loop
+            lib().or_td_norm2(B.n, M, _d(y_), _d(B.x), _i(B.family), _u(B.intact), _i(B.type_rel), B.nt,
+                              _d(B.cs), _d(B.vol), _d(B.m), _d(B.theta), _d(B.G), _d(B.edp), _d(B.td_norm2))
+            lib().or_force_density_ep(B.n, M, _d(f_), _d(y_), _d(B.x), _i(B.family), _u(B.intact),
+                                      _i(B.type_rel), B.nt, _d(B.cs), _d(B.density), _d(B.vol), _d(B.m),
+                                      _d(B.theta), _d(B.K), _d(B.G), _d(B.psi), _d(B.td_norm2), _d(B.edp))
+            return
         lib().or_force_density_T(B.kind, B.n, M, _d(f_), _d(y_), _d(B.x), _i(B.family), _u(B.intact),
                                  _i(B.type_rel), B.nt, _d(B.cs), _d(B.density), _d(B.vol), _d(B.c), _d(B.m),
                                  _d(B.theta), _d(B.K), _d(B.G), self.nthreads)

@@ -590,3 +590,101 @@ void or_contact11_force(int64_t n, int64_t rows, const int64_t *neighs,
         }
     }
 }
+
+/* ---------------------------------------------------------------------
+ * Elasto-plastic solid.  Both loops visit i = 1..n and the family of i in
+ * stored order, like loop_over_neighs! (peri.jl:411-445) and
+ * force_density_T! (general_material.jl:296-369).
+ * --------------------------------------------------------------------- */
+void or_td_norm2(int64_t n, int64_t M, const double *y, const double *x, const int64_t *family,
+                 uint8_t *intact, const int64_t *type_rel, int64_t ntypes, const double *cs,
+                 const double *vol, const double *m, const double *theta, const double *G,
+                 const double *edp, double *td_norm2) {
+    for (int64_t i = 0; i < n; ++i) td_norm2[i] = 0.0; /* elasto_plastic.jl:171 fill! */
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t ti = type_rel[i];
+        for (int64_t k = 0; k < M; ++k) {
+            if (!COL(intact, M, k, i)) continue;
+            int64_t j = COL(family, M, k, i) - 1;
+            int64_t tj = type_rel[j];
+            double X1 = x[3 * j] - x[3 * i], X2 = x[3 * j + 1] - x[3 * i + 1], X3 = x[3 * j + 2] - x[3 * i + 2];
+            double Y1 = y[3 * j] - y[3 * i], Y2 = y[3 * j + 1] - y[3 * i + 1], Y3 = y[3 * j + 2] - y[3 * i + 2];
+            double yij = mag3(Y1, Y2, Y3);
+            double xij = mag3(X1, X2, X3);
+            double extension = yij - xij;
+            double s = extension / xij;
+            size_t tp = (size_t)(ti - 1) + (size_t)(tj - 1) * (size_t)ntypes;
+            if (s < cs[tp]) {
+                /* elasto_plastic.jl:276-287 */
+                double wij = 1 / mag3(X1, X2, X3);
+                double wji = 1 / mag3(-X1, -X2, -X3);
+                double Gij = G[tp];
+                double edpij = COL(edp, M, k, i);
+                double a = wij / m[i], b = wji / m[j];
+                double w_m = a + b;
+                double tw = theta[i] * a + theta[j] * b;
+                double theta_ij = tw / w_m;
+                double ed = extension - theta_ij * xij / 3;
+                double td = 15 * Gij * (ed - edpij) * w_m;
+                td_norm2[i] = td_norm2[i] + td * td * vol[j];
+            } else {
+                COL(intact, M, k, i) = 0;
+            }
+        }
+    }
+}
+
+void or_force_density_ep(int64_t n, int64_t M, double *f, const double *y, const double *x,
+                         const int64_t *family, uint8_t *intact, const int64_t *type_rel, int64_t ntypes,
+                         const double *cs, const double *density, const double *vol, const double *m,
+                         const double *theta, const double *K, const double *G, const double *psi,
+                         const double *td_norm2, double *edp) {
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t ti = type_rel[i];
+        double _den_i = density[ti - 1];
+        for (int64_t k = 0; k < M; ++k) {
+            if (!COL(intact, M, k, i)) continue;
+            int64_t j = COL(family, M, k, i) - 1;
+            int64_t tj = type_rel[j];
+            double _den_j = density[tj - 1];
+            double X1 = x[3 * j] - x[3 * i], X2 = x[3 * j + 1] - x[3 * i + 1], X3 = x[3 * j + 2] - x[3 * i + 2];
+            double Y1 = y[3 * j] - y[3 * i], Y2 = y[3 * j + 1] - y[3 * i + 1], Y3 = y[3 * j + 2] - y[3 * i + 2];
+            double yij = mag3(Y1, Y2, Y3);
+            double xij = mag3(X1, X2, X3);
+            double extension = yij - xij;
+            double s = extension / xij;
+            size_t tp = (size_t)(ti - 1) + (size_t)(tj - 1) * (size_t)ntypes;
+            if (s < cs[tp]) {
+                /* elasto_plastic.jl:215-242 */
+                double wij = 1 / mag3(X1, X2, X3);
+                double wji = 1 / mag3(-X1, -X2, -X3);
+                double Kij = K[tp], Gij = G[tp], psij = psi[tp];
+                double C = sqrt(2 * psij / td_norm2[i]);
+                double a = wij / m[i], b = wji / m[j];
+                double tw = theta[i] * a + theta[j] * b;
+                double theta_ij = tw / (a + b);
+                double ed = extension - theta_ij * xij / 3;
+                double ede = ed - COL(edp, M, k, i);
+                double td_trial = 15 * Gij * (a + b) * ede;
+                double td;
+                if (C > 1) {
+                    td = td_trial;
+                } else {
+                    td = C * td_trial;
+                    COL(edp, M, k, i) = COL(edp, M, k, i) + ede * (1 - C);
+                }
+                double tn = (3 * Kij) * xij * tw;
+                double tij = tn + td;
+                double xx = 0.5 * tij / yij;
+                f[3 * i] = f[3 * i] + xx * Y1 * vol[j] / _den_i;
+                f[3 * i + 1] = f[3 * i + 1] + xx * Y2 * vol[j] / _den_i;
+                f[3 * i + 2] = f[3 * i + 2] + xx * Y3 * vol[j] / _den_i;
+                f[3 * j] = f[3 * j] - xx * Y1 * vol[i] / _den_j;
+                f[3 * j + 1] = f[3 * j + 1] - xx * Y2 * vol[i] / _den_j;
+                f[3 * j + 2] = f[3 * j + 2] - xx * Y3 * vol[i] / _den_j;
+            } else {
+                COL(intact, M, k, i) = 0;
+            }
+        }
+    }
+}

@@ -72,6 +72,23 @@ void or_force_density_T(int kind, int64_t n, int64_t M, double *f,
                         const double *m, const double *theta,
                         const double *K, const double *G, int nthreads);
 
+/* Elasto-plastic solid (elasto_plastic.jl), single-threaded.
+ * or_td_norm2: peri.jl:411-445 loop_over_neighs! with td_norm2_ij!
+ *   (elasto_plastic.jl:274-288): td_norm2[i] = sum over intact bonds of
+ *   td^2 V_j; bonds with s >= cs are cleared (as that loop does).
+ * or_force_density_ep: general_material.jl:296-369 with
+ *   force_density_t_ij (elasto_plastic.jl:215-242); edp (M x n) is updated
+ *   in place.  psi: ntypes x ntypes yield values (init, :60-68). */
+void or_td_norm2(int64_t n, int64_t M, const double *y, const double *x, const int64_t *family,
+                 uint8_t *intact, const int64_t *type_rel, int64_t ntypes, const double *cs,
+                 const double *vol, const double *m, const double *theta, const double *G,
+                 const double *edp, double *td_norm2);
+void or_force_density_ep(int64_t n, int64_t M, double *f, const double *y, const double *x,
+                         const int64_t *family, uint8_t *intact, const int64_t *type_rel, int64_t ntypes,
+                         const double *cs, const double *density, const double *vol, const double *m,
+                         const double *theta, const double *K, const double *G, const double *psi,
+                         const double *td_norm2, double *edp);
+
 /* general_material.jl:243-255: the "deformed" gate.  Returns 1 when
  * isapprox(y .- y[:,1] .+ x[:,1], x) holds (rigid translate; skip forces). */
 int or_isapprox_rigid(int64_t n, const double *y, const double *x);

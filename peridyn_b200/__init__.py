@@ -11,9 +11,9 @@ from .contacts import (LinearSpringContactModel, NonLinearSpringContactModel, No
                        NonLinearSpringContactModel12, ShortRangeContactModel)
 from .environment import Env, GeneralEnvironment
 from .serving import Server, serve_stream
-from .materials import (BondBasedMaterial, BondBasedSpecific, GeneralMaterial, OrdinaryStateBasedMaterial,
-                        OrdinaryStateBasedSpecific, PeridynamicsMaterial, SkipMaterial, SkipSpecific,
-                        julia_pow_int, make_matrix)
+from .materials import (BondBasedMaterial, BondBasedSpecific, ElastoPlasticSolidSpecific, GeneralMaterial,
+                        OrdinaryStateBasedMaterial, OrdinaryStateBasedSpecific, PeridynamicsMaterial, SkipMaterial,
+                        SkipSpecific, VonMises, julia_pow_int, make_matrix)
 from .solvers import (DSVelocityVerlet, QSDrag, apply_bc_at0, apply_solver, cal_damage, minimize, printdata, run,
                       save_state, simulate, update_acc, update_neighs, velocity_verlet_step)
 

@@ -29,6 +29,7 @@ PD_ERR_UNSUPPORTED = 9
 PD_MAT_BOND_BASED = 0
 PD_MAT_ORDINARY_STATE_BASED = 1
 PD_MAT_SKIP = 2
+PD_MAT_ELASTO_PLASTIC = 3
 
 PD_PREC_FP64_SERIAL = 0
 PD_PREC_FP64 = 1
@@ -73,6 +74,7 @@ class MaterialDesc(ctypes.Structure):
         ("horizon", ctypes.c_double),
         ("particle_size", ctypes.c_double),
         ("max_neigh", ctypes.c_int64),
+        ("plastic_psi", c_dp),
     ]
 
 
@@ -116,6 +118,7 @@ _SIGNATURES = {
     "pd_env_get_family": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_i64p, c_u8p]),
     "pd_env_get_weighted_volume": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_dp]),
     "pd_env_get_theta": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_dp]),
+    "pd_env_get_plastic_strain": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_dp]),
     "pd_env_get_state": (ctypes.c_int32, [c_vp, c_dp, c_dp, c_dp, c_dp]),
     "pd_env_set_state": (ctypes.c_int32, [c_vp, c_dp, c_dp, c_dp]),
     "pd_env_get_mass": (ctypes.c_int32, [c_vp, c_dp, c_dp, c_dp]),

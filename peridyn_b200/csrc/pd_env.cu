@@ -80,6 +80,9 @@ pd::Geo pd_env::geo() const {
     g.nbr = nbr.p;
     g.fam = fam.p;
     g.deformed = deformed.p;
+    g.td2 = td2.p;
+    g.edp_in = edp[ecur].p;
+    g.edp_out = edp[1 - ecur].p;
     return g;
 }
 
@@ -274,7 +277,7 @@ extern "C" pd_status pd_env_add_block(pd_env *env, int64_t n, const double *x, c
     if (n <= 0 || !x || !y || !v || !volume || !type || !mat)
         return fail(PD_ERR_ARG, "pd_env_add_block: NULL array or n <= 0");
     if (n > (int64_t)1 << 30) return fail(PD_ERR_ARG, "block too large (%lld)", (long long)n);
-    if (mat->kind < PD_MAT_BOND_BASED || mat->kind > PD_MAT_SKIP)
+    if (mat->kind < PD_MAT_BOND_BASED || mat->kind > PD_MAT_ELASTO_PLASTIC)
         return fail(PD_ERR_ARG, "unknown material kind %d", mat->kind);
     if (mat->ntypes < 1 || mat->ntypes > 255) return fail(PD_ERR_ARG, "ntypes must be 1..255");
     if (!mat->density) return fail(PD_ERR_ARG, "density is NULL");
@@ -313,7 +316,12 @@ extern "C" pd_status pd_env_add_block(pd_env *env, int64_t n, const double *x, c
         if (!mat->bond_stiffness) return fail(PD_ERR_ARG, "bond_stiffness is NULL");
         b.c.assign(mat->bond_stiffness, mat->bond_stiffness + nt2);
     }
-    if (mat->kind == PD_MAT_ORDINARY_STATE_BASED) {
+    if (mat->kind == PD_MAT_ELASTO_PLASTIC) {
+        if (!mat->plastic_psi) return fail(PD_ERR_ARG, "plastic_psi is NULL");
+        b.psi.assign(mat->plastic_psi, mat->plastic_psi + nt2);
+        if (!symmetric(b.psi, nt)) return fail(PD_ERR_ARG, "plastic_psi must be symmetric");
+    }
+    if (mat->kind == PD_MAT_ORDINARY_STATE_BASED || mat->kind == PD_MAT_ELASTO_PLASTIC) {
         if (!mat->bulk_modulus || !mat->shear_modulus) return fail(PD_ERR_ARG, "bulk/shear modulus is NULL");
         b.K.assign(mat->bulk_modulus, mat->bulk_modulus + nt2);
         b.G.assign(mat->shear_modulus, mat->shear_modulus + nt2);
@@ -641,9 +649,10 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
                 size_t e = (size_t)i + (size_t)j * b.nt;
                 PairParam pp;
                 pp.cs = b.cs[e];
-                pp.k35 = 3 * b.K[e] - 5 * b.G[e];
+                // ordinary_state_based.jl:183 (3K - 5G); elasto_plastic.jl:239 (3K)
+                pp.k35 = b.kind == PD_MAT_ELASTO_PLASTIC ? 3 * b.K[e] : 3 * b.K[e] - 5 * b.G[e];
                 pp.g15 = 15 * b.G[e];
-                pp.pad = 0.0;
+                pp.psi2 = b.kind == PD_MAT_ELASTO_PLASTIC ? 2 * b.psi[e] : 0.0;
                 pairs.push_back(pp);
             }
         for (int t = 0; t < b.nt; ++t) tdens.push_back(b.dens[t]);
@@ -887,6 +896,17 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
     w_b.clear();
     w_b.shrink_to_fit();
     env->cur = 0;
+    // elasto-plastic state (elasto_plastic.jl:60-68): td_norm2, edp = 0
+    bool any_ep = false;
+    for (auto &b : env->hb) any_ep |= b.kind == PD_MAT_ELASTO_PLASTIC;
+    if (any_ep) {
+        PD_TRY(env->td2.alloc(N));
+        CK(cudaMemsetAsync(env->td2.p, 0, N * sizeof(double), st));
+        for (auto &e : env->edp) {
+            PD_TRY(e.alloc(std::max<int64_t>(env->nnz, 32)));
+            CK(cudaMemsetAsync(e.p, 0, std::max<int64_t>(env->nnz, 32) * sizeof(double), st));
+        }
+    }
     // weighted volume (peri.jl:342-354) and intact0 (environment.jl:169)
     launch_weighted_volume(st, env->geo(), env->mth.p);
     launch_popcount(st, N, env->sinfo.p, env->cnt.p, env->words[0].p, env->intact0.p);
@@ -1108,6 +1128,8 @@ extern "C" pd_status pd_env_reset_bonds(pd_env *env) {
     CK(cudaMemcpyAsync(env->words[0].p, env->words0.p, nw, cudaMemcpyDeviceToDevice, env->st));
     CK(cudaMemcpyAsync(env->words[1].p, env->words0.p, nw, cudaMemcpyDeviceToDevice, env->st));
     env->cur = 0;
+    for (auto &e : env->edp)  // elasto-plastic bond state starts over with the bonds
+        if (e.p) CK(cudaMemsetAsync(e.p, 0, std::max<int64_t>(env->nnz, 32) * sizeof(double), env->st));
     CK(cudaStreamSynchronize(env->st));
     return PD_OK;
 }
@@ -1325,5 +1347,38 @@ extern "C" pd_status pd_env_stage_read(pd_env *env, int32_t slot, double *y, dou
         for (int64_t e = 0; e < NE; ++e) damage[e] = S.host[9 * NE + env->map_h[e]];
     if (time_step) *time_step = S.ts;
     S.pending = false;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_get_plastic_strain(pd_env *env, int64_t block, double *edp) {
+    PD_TRY(need_final(env));
+    if (block < 0 || block >= (int64_t)env->hb.size() || !edp) return fail(PD_ERR_ARG, "bad block or NULL edp");
+    const HostBlock &b = env->hb[block];
+    if (b.kind != PD_MAT_ELASTO_PLASTIC) return fail(PD_ERR_ARG, "block %lld is not elasto-plastic", (long long)block);
+    CK(cudaSetDevice(env->device));
+    const int64_t s0 = b.first_int / 32, s1 = (b.first_int + round_up(b.n, 32)) / 32;
+    const SliceInfo *si = env->sinfo_h.data();
+    const int64_t w0 = si[s0].word, w1 = si[s1].word;
+    std::vector<uint32_t> fm(w1 - w0);
+    std::vector<double> e(32 * (w1 - w0));
+    if (w1 > w0) {
+        CK(cudaMemcpyAsync(fm.data(), env->fam.p + w0, (w1 - w0) * 4, cudaMemcpyDeviceToHost, env->st));
+        CK(cudaMemcpyAsync(e.data(), env->edp[env->ecur].p + 32 * w0, 32 * (w1 - w0) * sizeof(double),
+                           cudaMemcpyDeviceToHost, env->st));
+    }
+    CK(cudaStreamSynchronize(env->st));
+    const int64_t R = b.rows;
+    std::fill(edp, edp + (size_t)R * b.n, 0.0);
+    for (int64_t i = 0; i < b.n; ++i) {
+        const int64_t p = b.first_int + i;
+        const int64_t wb = si[p / 32].word - w0 + (p % 32);
+        int64_t r = 0;
+        for (int32_t k = 0; k < env->cnt_h[p] && r < R; ++k) {
+            const int64_t w = wb + 32 * (k / 32);
+            if (!((fm[w] >> (k % 32)) & 1u)) continue;
+            edp[(size_t)i * R + r] = e[32 * w + (k % 32)];
+            ++r;
+        }
+    }
     return PD_OK;
 }

@@ -77,7 +77,7 @@ struct HostBlock {
     int64_t max_neigh = 100;
     std::vector<double> x, y, v, vol;
     std::vector<int64_t> type;
-    std::vector<double> c, K, G, cs, dens;
+    std::vector<double> c, K, G, cs, dens, psi;
     bool host_family = false;
     int64_t rows = 0;  // reference family rows M'
     std::vector<int64_t> family;
@@ -163,6 +163,10 @@ struct pd_env {
     pd::DBuf<pd::SliceInfo> sinfo;
     pd::DBuf<int32_t> nbr;
     pd::DBuf<uint32_t> words[2], words0, fam;
+    // elasto-plastic state: td_norm2 per particle, edp per bond slot
+    // (double-buffered by force evaluation, edp[ecur] current)
+    pd::DBuf<double> td2, edp[2];
+    int ecur = 0;
     int cur = 0;
     pd::DBuf<double2> mth;
     pd::DBuf<pd::DevBlock> blocks_d;

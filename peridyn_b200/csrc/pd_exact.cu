@@ -158,7 +158,7 @@ __global__ void k_theta_serial(Geo g, const double4 *__restrict__ y,
     int32_t ti = g.tinfo[p];
     if (ti < 0) return;
     const DevBlock &B = g.blocks[ti >> 8];
-    if (B.kind != PD_MAT_ORDINARY_STATE_BASED) return;
+    if (B.kind != PD_MAT_ORDINARY_STATE_BASED && B.kind != PD_MAT_ELASTO_PLASTIC) return;
     double4 xp = g.x4[p], yp = y[p];
     double c_i = 3.0 / mth[p].x;
     int32_t n = g.cnt[p];
@@ -218,6 +218,141 @@ __device__ __forceinline__ bool bond_term(const Geo &g, const DevBlock &B, int t
 }
 
 // ---------------------------------------------------------------------
+// Elasto-plastic solid (elasto_plastic.jl).  Unlike the PMB and LPS laws,
+// the bond term depends on which end visits the bond: particle i's visit
+// to bond slot k uses td_norm2[i] and edp[k, i] and updates edp[k, i].
+// ---------------------------------------------------------------------
+// Slot of neighbour p in q's family (slots hold descending indices).
+__device__ __forceinline__ int32_t find_slot(const Geo &g, int64_t q, int32_t p) {
+    const SliceInfo s = g.si[q >> 5];
+    const bool st = s.mode == kStencil;
+    const int32_t *nb = g.nbr + s.nbr + (st ? 0 : (q & 31));
+    const int32_t target = st ? (int32_t)(p - q) : p;
+    int32_t lo = 0, hi = g.cnt[q];
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        const int32_t v = st ? nb[mid] : nb[32 * mid];
+        if (v > target) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// force_density_t_ij (elasto_plastic.jl:215-242) for the visit of i to j;
+// mi, mj = (m, theta); the plastic update of edp[k, i] goes to *edp_new.
+__device__ __forceinline__ double ep_t(const PairParam &pp, double xij, double ext, double2 mi, double2 mj,
+                                       double td2_i, double edp_old, double *edp_new) {
+    const double wij = 1.0 / xij;  // influence_function(X) == influence_function(-X)
+    const double C = sqrt(pp.psi2 / td2_i);
+    const double a = wij / mi.x, b = wij / mj.x;
+    const double tw = mi.y * a + mj.y * b;
+    const double theta_ij = tw / (a + b);
+    const double ed = ext - theta_ij * xij / 3;
+    const double ede = ed - edp_old;
+    const double td_trial = pp.g15 * (a + b) * ede;
+    double td;
+    if (C > 1) {
+        td = td_trial;
+    } else {
+        td = C * td_trial;
+        if (edp_new) *edp_new = edp_old + ede * (1 - C);
+    }
+    const double tn = pp.k35 * xij * tw;
+    return tn + td;
+}
+
+// The elasto-plastic term seen by p for the bond to q: from p's own visit
+// (own, slot k of p) or from q's visit to p.
+__device__ __forceinline__ bool bond_term_ep(const Geo &g, const DevBlock &B, int tp, int64_t p, double4 xp,
+                                             double4 yp, double2 mp, double rho_p, int32_t q, int32_t k, bool own,
+                                             const double4 *__restrict__ y, const double2 *__restrict__ mth,
+                                             double &t0, double &t1, double &t2) {
+    double4 xq = g.x4[q], yq = y[q];
+    double X1 = xq.x - xp.x, X2 = xq.y - xp.y, X3 = xq.z - xp.z;
+    double Y1 = yq.x - yp.x, Y2 = yq.y - yp.y, Y3 = yq.z - yp.z;
+    double yij = mag3(Y1, Y2, Y3);
+    double xij = mag3(X1, X2, X3);
+    double ext = yij - xij;
+    double s = ext / xij;
+    int tq = B.nt > 1 ? (g.tinfo[q] & 255) : 0;
+    const PairParam &pp = g.pairs[B.pair_base + tp + tq * B.nt];
+    if (!(s < pp.cs)) return false;
+    const double2 mq = mth[q];
+    double t;
+    if (own) {
+        const int64_t e = slot_index(g.si, p, k);
+        t = ep_t(pp, xij, ext, mp, mq, g.td2[p], g.edp_in[e], g.edp_out + e);
+    } else {
+        const int64_t e = slot_index(g.si, q, find_slot(g, q, (int32_t)p));
+        t = ep_t(pp, xij, ext, mq, mp, g.td2[q], g.edp_in[e], nullptr);
+    }
+    double xx = 0.5 * t / yij;
+    t0 = xx * Y1 * xq.w / rho_p;
+    t1 = xx * Y2 * xq.w / rho_p;
+    t2 = xx * Y3 * xq.w / rho_p;
+    return true;
+}
+
+// peri.jl:411-445 loop_over_neighs! with td_norm2_ij! (elasto_plastic.jl:
+// 274-288): td_norm2[p] over p's family in stored order; bonds at or beyond
+// the critical stretch are cleared (that loop breaks them too).  Particles
+// of other blocks only copy their flags.
+__global__ void __launch_bounds__(kThreads)
+    k_td_serial(Geo g, const double4 *__restrict__ y, const double2 *__restrict__ mth,
+                const uint32_t *__restrict__ win, uint32_t *__restrict__ wout, int64_t p0, int64_t p1) {
+    int64_t p = p0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= p1) return;
+    const int32_t ti = g.tinfo[p];
+    const int32_t n = g.cnt[p];
+    const int64_t wb = g.si[p >> 5].word + (p & 31);
+    const bool active = ti >= 0 && g.blocks[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC && g.deformed[ti >> 8] != 0;
+    if (!active) {
+        for (int32_t w = 0; w * 32 < n; ++w) wout[wb + 32 * (int64_t)w] = win[wb + 32 * (int64_t)w];
+        return;
+    }
+    const DevBlock &B = g.blocks[ti >> 8];
+    const int tp = ti & 255;
+    const double4 xp = g.x4[p], yp = y[p];
+    const double2 mp = mth[p];
+    const BondRef br = bond_ref(g.si, g.nbr, win, p);
+    uint32_t *wo = wout + wb;
+    double acc = 0.0;
+    uint32_t w = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        if ((k & 31) == 0) {
+            if (k > 0) wo[32 * (int64_t)((k >> 5) - 1)] = w;
+            w = *br.word(k);
+        }
+        if (!((w >> (k & 31)) & 1u)) continue;
+        const int32_t q = br.q(k);
+        const double4 xq = g.x4[q], yq = y[q];
+        const double X1 = xq.x - xp.x, X2 = xq.y - xp.y, X3 = xq.z - xp.z;
+        const double Y1 = yq.x - yp.x, Y2 = yq.y - yp.y, Y3 = yq.z - yp.z;
+        const double yij = mag3(Y1, Y2, Y3);
+        const double xij = mag3(X1, X2, X3);
+        const double ext = yij - xij;
+        const double s = ext / xij;
+        const int tq = B.nt > 1 ? (g.tinfo[q] & 255) : 0;
+        const PairParam &pp = g.pairs[B.pair_base + tp + tq * B.nt];
+        if (s < pp.cs) {
+            const double2 mq = mth[q];
+            const double wij = 1.0 / xij;
+            const double a = wij / mp.x, b = wij / mq.x;
+            const double w_m = a + b;
+            const double tw = mp.y * a + mq.y * b;
+            const double theta_ij = tw / w_m;
+            const double ed = ext - theta_ij * xij / 3;
+            const double td = pp.g15 * (ed - g.edp_in[slot_index(g.si, p, k)]) * w_m;
+            acc = acc + td * td * xq.w;
+        } else {
+            w &= ~(1u << (k & 31));
+        }
+    }
+    if (n > 0) wo[32 * (int64_t)((n - 1) >> 5)] = w;
+    g.td2[p] = acc;
+}
+
+// ---------------------------------------------------------------------
 // general_material.jl:296-369 in the serial loop's summation order.
 // The reference visits i = 1..N and, for each i, its family in stored
 // (descending) order, adding the term to f_i and subtracting it from f_j.
@@ -239,7 +374,8 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
     const DevBlock &B = g.blocks[ti >> 8];
     int tp = ti & 255;
     double4 xp = g.x4[p], yp = y[p];
-    double2 mp = KIND == PD_MAT_ORDINARY_STATE_BASED ? mth[p] : make_double2(0.0, 0.0);
+    double2 mp = KIND != PD_MAT_BOND_BASED ? mth[p] : make_double2(0.0, 0.0);
+    constexpr bool EP = KIND == PD_MAT_ELASTO_PLASTIC;
     double rho_p = g.tdens[B.type_base + tp];
     int32_t n = g.cnt[p];
     const BondRef br = bond_ref(g.si, g.nbr, win, p);
@@ -259,7 +395,8 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
         if (q > p) break;
         uint32_t w = *br.word(k);
         if (!((w >> (k & 31)) & 1u)) continue;
-        if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
+        if (EP ? bond_term_ep(g, B, tp, p, xp, yp, mp, rho_p, q, k, false, y, mth, t0, t1, t2)
+               : bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
             fy = fy + t1;
             fz = fz + t2;
@@ -273,9 +410,14 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
             if (k > 0) wo[32 * (int64_t)((k >> 5) - 1)] = w;
             w = *br.word(k);
         }
+        if (EP) {  // edp carries over unless this visit yields
+            const int64_t e = slot_index(g.si, p, k);
+            g.edp_out[e] = g.edp_in[e];
+        }
         if (!((w >> (k & 31)) & 1u)) continue;
         int32_t q = br.q(k);
-        if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
+        if (EP ? bond_term_ep(g, B, tp, p, xp, yp, mp, rho_p, q, k, true, y, mth, t0, t1, t2)
+               : bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
             fy = fy + t1;
             fz = fz + t2;
@@ -289,7 +431,8 @@ __device__ void force_serial_particle(const Geo &g, int64_t p, int32_t ti,
         int32_t q = br.q(k);
         uint32_t ww = *br.word(k);
         if (!((ww >> (k & 31)) & 1u)) continue;
-        if (bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
+        if (EP ? bond_term_ep(g, B, tp, p, xp, yp, mp, rho_p, q, k, false, y, mth, t0, t1, t2)
+               : bond_term<KIND>(g, B, tp, xp, yp, mp, rho_p, q, y, mth, t0, t1, t2)) {
             fx = fx + t0;
             fy = fy + t1;
             fz = fz + t2;
@@ -316,11 +459,15 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (!active) {
         for (int32_t w = 0; w * 32 < n; ++w) wout[wb + 32 * (int64_t)w] = win[wb + 32 * (int64_t)w];
+        if (kind == PD_MAT_ELASTO_PLASTIC && g.edp_out)
+            for (int32_t k = 0; k < n; ++k) g.edp_out[slot_index(g.si, p, k)] = g.edp_in[slot_index(g.si, p, k)];
         if (!accumulate) f[p] = make_double4(0.0, 0.0, 0.0, 0.0);
         return;
     }
     if (kind == PD_MAT_BOND_BASED)
         force_serial_particle<PD_MAT_BOND_BASED>(g, p, ti, y, mth, win, wout, f, accumulate);
+    else if (kind == PD_MAT_ELASTO_PLASTIC)
+        force_serial_particle<PD_MAT_ELASTO_PLASTIC>(g, p, ti, y, mth, win, wout, f, accumulate);
     else
         force_serial_particle<PD_MAT_ORDINARY_STATE_BASED>(g, p, ti, y, mth, win, wout, f,
                                                             accumulate);
@@ -633,6 +780,13 @@ void launch_theta_serial(cudaStream_t st, const Geo &g, const double4 *y, const 
                          double2 *mth, int64_t p0, int64_t p1) {
     if (p1 <= p0) return;
     k_theta_serial<<<grid_for(p1 - p0), kThreads, 0, st>>>(g, y, win, mth, p0, p1); pd::note_launch();
+}
+
+void launch_td_serial(cudaStream_t st, const Geo &g, const double4 *y, const double2 *mth,
+                      const uint32_t *win, uint32_t *wout, int64_t p0, int64_t p1) {
+    if (p1 <= p0) return;
+    k_td_serial<<<grid_for(p1 - p0), kThreads, 0, st>>>(g, y, mth, win, wout, p0, p1);
+    pd::note_launch();
 }
 
 void launch_force_serial(cudaStream_t st, const Geo &g, const double4 *y, const double2 *mth,

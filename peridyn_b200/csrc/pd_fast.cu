@@ -1539,6 +1539,9 @@ pd_status export_fast(pd_env *env, Fast<R> &F) {
 }
 
 pd_status ensure_fast(pd_env *env) {
+    for (const auto &b : env->hb)
+        if (b.kind == PD_MAT_ELASTO_PLASTIC)
+            return fail(PD_ERR_UNSUPPORTED, "the elasto-plastic solid runs in PD_PREC_FP64_SERIAL only");
     if (env->hbc.size() > (size_t)kMaxFastBC)
         return fail(PD_ERR_UNSUPPORTED, "the throughput modes support at most %d boundary conditions", kMaxFastBC);
     if (!env->fast) {

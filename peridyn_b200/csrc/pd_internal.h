@@ -93,9 +93,9 @@ __device__ __forceinline__ BondRef bond_ref(const SliceInfo *si, const int32_t *
 
 struct PairParam {
     double cs;    // critical stretch
-    double k35;   // 3K - 5G   (LPS)
-    double g15;   // 15G       (LPS)
-    double pad;
+    double k35;   // 3K - 5G (LPS); 3K (elasto-plastic)
+    double g15;   // 15G
+    double psi2;  // 2 psi (elasto-plastic yield value)
 };
 
 // Everything a bond kernel reads (passed by value).
@@ -111,7 +111,17 @@ struct Geo {
     const int32_t *nbr;        // bond index data (see SliceInfo)
     const uint32_t *fam;       // family-member bits (same layout as intact)
     const int32_t *deformed;   // per block
+    // elasto-plastic blocks: td_norm2 per particle, plastic deviatoric
+    // strain per bond slot (read from edp_in, written to edp_out)
+    double *td2;
+    const double *edp_in;
+    double *edp_out;
 };
+
+// Per-slot double index of bond slot k of particle p (elasto-plastic edp).
+__device__ __forceinline__ int64_t slot_index(const SliceInfo *si, int64_t p, int32_t k) {
+    return ((si[p >> 5].word + 32 * (int64_t)(k >> 5) + (p & 31)) << 5) + (k & 31);
+}
 
 struct BCDev {
     int32_t kind;
@@ -159,6 +169,9 @@ void launch_theta_serial(cudaStream_t st, const Geo &g, const double4 *y, const 
 void launch_force_serial(cudaStream_t st, const Geo &g, const double4 *y, const double2 *mth,
                          const uint32_t *win, uint32_t *wout, double4 *f, int accumulate,
                          int64_t p0, int64_t p1);
+// elasto_plastic.jl:166-172 out_of_loop! td_norm2 pass (breaks bonds too)
+void launch_td_serial(cudaStream_t st, const Geo &g, const double4 *y, const double2 *mth,
+                      const uint32_t *win, uint32_t *wout, int64_t p0, int64_t p1);
 
 // Elementwise velocity-Verlet pieces (exact FP64 arithmetic).
 void launch_kick_drift(cudaStream_t st, int64_t N, double c, double dt, const double4 *f,

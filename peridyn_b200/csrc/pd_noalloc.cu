@@ -86,6 +86,8 @@ extern "C" pd_status pd_force_density_device_static(pd_env *env, int64_t block, 
         cudaGetLastError();
         return fail(PD_ERR_ARG, "f/y must be device pointers");
     }
+    if (hb.kind == PD_MAT_ELASTO_PLASTIC)
+        return fail(PD_ERR_UNSUPPORTED, "the device-pointer entry point does not evaluate elasto-plastic blocks");
     double4 *scratch = nullptr;
     PD_TRY(scratch_for(env->device, &scratch));
     cudaStream_t st = stream ? (cudaStream_t)stream : env->st;

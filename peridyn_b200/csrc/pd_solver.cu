@@ -205,15 +205,30 @@ pd_status update_acc_serial(pd_env *env) {
         launch_gate_multi(st, env->gate_items.p, ni, gx, env->x4.p, env->y.p, env->gate_part.p, env->deformed.p);
     }
     // out_of_loop!: dilatation for state-based blocks
-    bool any_lps = false;
-    for (const auto &hb : env->hb) any_lps |= hb.kind == PD_MAT_ORDINARY_STATE_BASED;
+    bool any_lps = false, any_ep = false;
+    for (const auto &hb : env->hb) {
+        any_lps |= hb.kind == PD_MAT_ORDINARY_STATE_BASED || hb.kind == PD_MAT_ELASTO_PLASTIC;
+        any_ep |= hb.kind == PD_MAT_ELASTO_PLASTIC;
+    }
     if (any_lps) launch_theta_serial(st, g, env->y.p, env->words[env->cur].p, env->mth.p, 0, env->N);
-    // fill!(f, 0) + force_density_T! for every block
-    prof_begin(env, st);
-    launch_force_serial(st, g, env->y.p, env->mth.p, env->words[env->cur].p, env->words[1 - env->cur].p,
-                        env->f.p, 0, 0, env->N);
-    prof_end(env, st);
-    env->cur = 1 - env->cur;
+    if (any_ep) {
+        // elasto_plastic.jl:170-171: td_norm2 pass (breaks bonds), then the
+        // bond loop on its flags, back into words[cur]; edp is double-buffered
+        launch_td_serial(st, g, env->y.p, env->mth.p, env->words[env->cur].p, env->words[1 - env->cur].p, 0,
+                         env->N);
+        prof_begin(env, st);
+        launch_force_serial(st, g, env->y.p, env->mth.p, env->words[1 - env->cur].p, env->words[env->cur].p,
+                            env->f.p, 0, 0, env->N);
+        prof_end(env, st);
+        env->ecur = 1 - env->ecur;
+    } else {
+        // fill!(f, 0) + force_density_T! for every block
+        prof_begin(env, st);
+        launch_force_serial(st, g, env->y.p, env->mth.p, env->words[env->cur].p, env->words[1 - env->cur].p,
+                            env->f.p, 0, 0, env->N);
+        prof_end(env, st);
+        env->cur = 1 - env->cur;
+    }
     CK(cudaGetLastError());
     // short_range_contact!
     PD_TRY(contacts_force(env));
@@ -365,6 +380,8 @@ extern "C" pd_status pd_force_density_device(pd_env *env, int64_t block, double 
     }
     cudaStream_t st = stream ? (cudaStream_t)stream : env->st;
     const HostBlock &hb = env->hb[block];
+    if (hb.kind == PD_MAT_ELASTO_PLASTIC)
+        return fail(PD_ERR_UNSUPPORTED, "the device-pointer entry point does not evaluate elasto-plastic blocks");
     if (!env->tmp_y.p) PD_TRY(env->tmp_y.alloc(env->N));
     if (!env->tmp_f.p) PD_TRY(env->tmp_f.alloc(env->N));
     const int64_t *map = env->map.p + hb.first_env;

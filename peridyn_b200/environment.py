@@ -142,6 +142,16 @@ class GeneralEnvironment:
         h, self._h = self._h, None
         return h
 
+    def plastic_strain(self, block):
+        """edp of an elasto-plastic block (rows x n, aligned with its family)."""
+        L = _abi.lib()
+        rows = ctypes.c_int64()
+        _abi.check(L.pd_env_family_rows(self._h, block, ctypes.byref(rows)))
+        n = self.material_blocks[block].general.n
+        out = np.zeros((rows.value, n), order="F")
+        _abi.check(L.pd_env_get_plastic_strain(self._h, block, _abi.dptr(out)))
+        return out
+
     def kernel_shape(self):
         """(warps per slice, unroll) the throughput path runs with."""
         w, u = ctypes.c_int32(), ctypes.c_int32()

@@ -187,6 +187,48 @@ class OrdinaryStateBasedSpecific(SpecificMaterial):
         return self
 
 
+class VonMises:
+    """elasto_plastic.jl:453-479 Von Mises criterion."""
+
+    @staticmethod
+    def effective_stress2(s1, s2, s3):
+        # ((s1 - s2)^2 + (s2 - s3)^2 + (s1 - s3)^2) / 2, element-wise
+        a, b, c = s1 - s2, s2 - s3, s1 - s3
+        return (a * a + b * b + c * c) / 2
+
+
+class ElastoPlasticSolidSpecific(SpecificMaterial):
+    """elasto_plastic.jl:31-116: ``ElastoPlasticSolidSpecific(K, G, cs,
+    density, sigma_y; criteria=VonMises())``.  ``init`` sets the yield value
+    psi = 75/(8 pi) * sigma_e^2 / horizon^5 per type pair, the plastic
+    deviatoric strain edp (per bond) and td_norm2 to zero (:60-68)."""
+
+    kind = _abi.PD_MAT_ELASTO_PLASTIC
+
+    def __init__(self, bulk_modulus, shear_modulus, critical_stretch, density, yield_stress, criteria=None):
+        self.bulk_modulus = make_matrix(bulk_modulus) if np.ndim(bulk_modulus) == 2 else make_matrix(_as_vec(bulk_modulus))
+        self.shear_modulus = make_matrix(shear_modulus) if np.ndim(shear_modulus) == 2 else make_matrix(_as_vec(shear_modulus))
+        self.critical_stretch = (make_matrix(critical_stretch) if np.ndim(critical_stretch) == 2
+                                 else make_matrix(_as_vec(critical_stretch)))
+        self.density = _as_vec(density)
+        self.yield_stress = (make_matrix(yield_stress) if np.ndim(yield_stress) == 2
+                             else make_matrix(_as_vec(yield_stress)))
+        self.criteria = VonMises() if criteria is None else criteria
+        if not hasattr(self.criteria, "effective_stress2"):
+            raise NotImplementedError(f"effective_stress not implemented for {type(self.criteria).__name__}")
+        self.psi = np.zeros_like(self.yield_stress)
+        self.theta = np.zeros(0)
+
+    def init(self, gen):
+        d = gen.horizon
+        # sigma = [1, 0, 0] * sigma_y (elasto_plastic.jl:62-65)
+        sy = self.yield_stress
+        se2 = self.criteria.effective_stress2(sy * 1.0, sy * 0.0, sy * 0.0)
+        self.psi = np.asfortranarray((75 / (8 * math.pi)) * se2 / julia_pow_int(d, 5))
+        self.theta = np.zeros(gen.n)
+        return self
+
+
 class SkipSpecific(SpecificMaterial):
     """skip_specific.jl:39-49: no material forces (rigid/passive block)."""
 
@@ -244,9 +286,11 @@ class PeridynamicsMaterial:
             d.critical_stretch = mat(spc.critical_stretch)
         if spc.kind == _abi.PD_MAT_BOND_BASED:
             d.bond_stiffness = mat(spc.bond_stiffness)
-        if spc.kind == _abi.PD_MAT_ORDINARY_STATE_BASED:
+        if spc.kind in (_abi.PD_MAT_ORDINARY_STATE_BASED, _abi.PD_MAT_ELASTO_PLASTIC):
             d.bulk_modulus = mat(spc.bulk_modulus)
             d.shear_modulus = mat(spc.shear_modulus)
+        if spc.kind == _abi.PD_MAT_ELASTO_PLASTIC:
+            d.plastic_psi = mat(spc.psi)
         d.horizon = self.general.horizon
         d.particle_size = self.general.particle_size
         d.max_neigh = self.general.max_neigh

@@ -42,3 +42,22 @@ def bar_with_bcs(kind, nx=20, ny=6, nz=6, steps=60):
         bc = pb.ContainerBC(x[0] > cen[0], limits=lim)
     w["bcs"] = [fix, bc]
     return w
+
+
+def ep_cube(sigma_y, n=10, peak=60.0, cs=0.02, seed=7, ntypes=1):
+    """Elasto-plastic (Von Mises) cube with the pmb_cube pulse; a second
+    type on the x > mean half when ntypes == 2."""
+    x, vol = lattice.cuboid(n, n - 1, n - 2, 1.0e-3, jitter=1.0e-5, seed=seed)
+    t = np.ones(x.shape[1], dtype=np.int64)
+    if ntypes == 2:
+        t = np.where(x[0] < x[0].mean(), 1, 2).astype(np.int64)
+    gen = pb.GeneralMaterial(x.copy(order="F"), lattice.gaussian_pulse(x, peak, 3.0e-3), x, vol, t, 3.015e-3,
+                             max_neigh=200)
+    # per type-pair values in make_matrix order (n(n+1)/2 entries for n types)
+    npairs = ntypes * (ntypes + 1) // 2
+    K = [46.7e9, 43.0e9, 40.0e9][:npairs]
+    G = [28.0e9, 26.0e9, 25.0e9][:npairs]
+    sy = [sigma_y, 1.5 * sigma_y, 2.0 * sigma_y][:npairs]
+    spc = pb.ElastoPlasticSolidSpecific(K, G, [cs] * npairs, [2700.0, 2500.0][:ntypes], sy)
+    mat = pb.PeridynamicsMaterial(gen, spc, name="ep_cube")
+    return {"materials": [mat], "contacts": [], "bcs": [], "dt": 2.0e-8, "steps": 60}

@@ -23,7 +23,7 @@ def test_library_exports_header_symbols():
 
 def test_abi_version_and_status_strings():
     L = _abi.lib()
-    assert L.pd_abi_version() == 1
+    assert L.pd_abi_version() == 2
     assert L.pd_status_string(0) == b"ok"
     assert L.pd_status_string(_abi.PD_ERR_FAMILY_OVERFLOW).startswith(b"family")
 

@@ -8,7 +8,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import _abi, configs, lattice
-from tests.cases import bar_with_bcs, random_cloud
+from tests.cases import bar_with_bcs, ep_cube, random_cloud
 
 pytestmark = pytest.mark.gpu
 
@@ -350,4 +350,32 @@ def test_scaling_and_container_bcs_bit_exact(oracle, kind):
     it_g = pb.minimize(env, pb.QSDrag(1e-7, 10.0, max_iter=5))
     assert it_o == it_g
     _assert_state_equal(env, ora, kind + " after QSDrag")
+    env.close()
+
+
+@pytest.mark.parametrize("builder", [lambda: ep_cube(5e6), lambda: ep_cube(2e6, ntypes=2),
+                                     lambda: ep_cube(5e6, peak=300.0, cs=0.003)])
+def test_elasto_plastic_bit_exact(oracle, builder, layout):
+    # td_norm2 pass, asymmetric bond terms (each end's own edp and td_norm2)
+    w = builder()
+    env, ora = _pair(oracle, w)
+    _check_layout(env, layout)
+    for _ in range(40):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=40)
+    _assert_state_equal(env, ora)
+    _assert_bonds_equal(env, ora)
+    B = ora.blocks[0]
+    assert np.abs(B.edp).max() > 0.0
+    assert np.array_equal(env.plastic_strain(0), B.edp)
+    assert np.array_equal(env.theta(0), B.theta)
+    env.close()
+
+
+def test_elasto_plastic_needs_serial_mode():
+    w = ep_cube(5e6, n=6)
+    env = pb.Env(1, w["materials"], [], [], w["dt"], precision="fp32c")
+    with pytest.raises(pb.PDError) as e:
+        pb.velocity_verlet_step(env, nsteps=2)
+    assert e.value.status == _abi.PD_ERR_UNSUPPORTED
     env.close()

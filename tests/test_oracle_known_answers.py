@@ -265,3 +265,35 @@ def test_container_bc_zeroes_escaping_velocities(oracle):
         assert np.all(ora.v[:, idx[out]] == 0.0)
         outside_seen |= bool(out.any())
     assert outside_seen
+
+
+def test_elasto_plastic_elastic_limit_is_lps(oracle):
+    # With a yield stress too high to be reached, C = sqrt(2 psi / td_norm2)
+    # stays > 1 and t = 3K |xi| tw + 15G (a + b) ed, which is the LPS law
+    # (ordinary_state_based.jl:176-187) rearranged: same forces to rounding.
+    import peridyn_b200 as pb
+    from tests.cases import ep_cube
+
+    w = ep_cube(1e30, n=8)
+    gen = w["materials"][0].general
+    lps = pb.PeridynamicsMaterial(gen, pb.OrdinaryStateBasedSpecific([46.7e9], [28.0e9], [0.02], [2700.0]))
+    a = oracle.OracleEnv(w["materials"], [], [], w["dt"])
+    b = oracle.OracleEnv([lps], [], [], w["dt"])
+    for _ in range(25):
+        a.vv_step()
+        b.vv_step()
+    assert np.all(a.blocks[0].edp == 0.0)
+    assert np.linalg.norm(a.y - b.y) <= 1e-12 * np.linalg.norm(b.y)
+    assert np.linalg.norm(a.f - b.f) <= 1e-9 * np.linalg.norm(b.f)
+
+
+def test_elasto_plastic_yields(oracle):
+    from tests.cases import ep_cube
+
+    w = ep_cube(5e6, n=8)
+    a = oracle.OracleEnv(w["materials"], [], [], w["dt"])
+    for _ in range(25):
+        a.vv_step()
+    B = a.blocks[0]
+    assert np.abs(B.edp).max() > 0.0
+    assert np.all(B.edp[B.family == 0] == 0.0)
