@@ -101,6 +101,8 @@ struct FBC {
     double4 *last;
     int64_t sn;          // ScaleFixWait scalebool particles
     const int32_t *sidx;
+    int64_t rank_lo;     // rank[p - rank_lo]: position of particle p in idx / last
+    const int32_t *rank;
 };
 
 template <class R>
@@ -132,15 +134,6 @@ struct StepArgs {
     FBC bc[kMaxFastBC];
 };
 
-__device__ __forceinline__ int64_t lower_bound_i32(const int32_t *a, int64_t n, int32_t key) {
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-        int64_t mid = (lo + hi) >> 1;
-        if (a[mid] < key) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
 
 __device__ __forceinline__ double &cmp(double4 &a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 
@@ -394,7 +387,7 @@ __device__ __forceinline__ void bc_position(const StepArgs<R> &a, int64_t p, uin
         if (!((bits >> k) & 1)) continue;
         const FBC &b = a.bc[k];
         if (b.kind == PD_BC_CONTAINER) continue;
-        const int64_t r = lower_bound_i32(b.idx, b.n, (int32_t)p);
+        const int64_t r = b.rank[p - b.rank_lo];
         double4 last = b.last[r];
         const double step = a.dt * (((a.dir_pos >> k) & 1) ? -1.0 : 1.0);
         for (int d = 0; d < 3; ++d) {
@@ -893,6 +886,8 @@ struct Fast {
     DBuf<FBlock<R>> fb;
     DBuf<FPair<R>> fp;
     DBuf<uint8_t> bcbits;
+    DBuf<int32_t> bcrank;            // per BC, dense over its index range
+    std::vector<int64_t> bcrank_off, bcrank_lo;
     DBuf<double> gpart;
     DBuf<GateItem> gitems;
     std::vector<GateItem> gitems_h;
@@ -1024,6 +1019,8 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
         b.last = env->bcs[k].last.p;
         b.sn = env->bcs[k].sn;
         b.sidx = env->bcs[k].sidx.p;
+        b.rank_lo = k < F.bcrank_lo.size() ? F.bcrank_lo[k] : 0;
+        b.rank = F.bcrank.p ? F.bcrank.p + (k < F.bcrank_off.size() ? F.bcrank_off[k] : 0) : nullptr;
     }
     a.ts = env->ts;
     return a;
@@ -1082,6 +1079,27 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         for (size_t k = 0; k < env->hbc.size(); ++k)
             for (int64_t e : env->hbc[k].env_idx) bits[env->map_h[e]] |= (uint8_t)(1u << k);
         CK(cudaMemcpyAsync(F.bcbits.p, bits.data(), N, cudaMemcpyHostToDevice, env->st));
+        // rank tables: BC k's particle p sits at rank[k][p - lo[k]] of its
+        // ascending index list (no search in the step kernel)
+        std::vector<int32_t> rank;
+        F.bcrank_off.clear();
+        F.bcrank_lo.clear();
+        for (size_t k = 0; k < env->hbc.size(); ++k) {
+            const auto &ei = env->hbc[k].env_idx;
+            F.bcrank_off.push_back((int64_t)rank.size());
+            if (ei.empty()) {
+                F.bcrank_lo.push_back(0);
+                continue;
+            }
+            const int64_t lo = env->map_h[ei.front()], hi = env->map_h[ei.back()];
+            F.bcrank_lo.push_back(lo);
+            const size_t base = rank.size();
+            rank.resize(base + (size_t)(hi - lo + 1), -1);
+            for (size_t r = 0; r < ei.size(); ++r) rank[base + (size_t)(env->map_h[ei[r]] - lo)] = (int32_t)r;
+        }
+        PD_TRY(F.bcrank.alloc(std::max<size_t>(rank.size(), 1)));
+        if (!rank.empty())
+            CK(cudaMemcpyAsync(F.bcrank.p, rank.data(), rank.size() * 4, cudaMemcpyHostToDevice, env->st));
         CK(cudaStreamSynchronize(env->st));
     }
     F.cur = 0;
