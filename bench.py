@@ -37,6 +37,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from peridyn_b200 import replicas  # noqa: E402  (host logic only; no library load)
+
 METRIC = "bond-force updates/s"
 UNIT = "bond-updates/s"
 
@@ -248,10 +250,7 @@ def time_precision(work, precision, sim_steps, device, flush, dist):
             t_total += e0.elapsed_time(e1) / 1e3
             bonds += 0.5 * (b0 + env.num_bonds()) * sim_steps
     env.close()
-    if dist is not None:
-        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
+    t_total, bonds = replicas.reduce_timing(t_total, bonds, dist, "cuda")
     return {"precision": precision, "value": bonds / t_total, "unit": UNIT, "ms_per_step": 1e3 * t_total / 2,
             "steps": 2, "warmup": 1}
 
@@ -277,7 +276,10 @@ def run_serving(args, rank, world, local):
     # each rank serves its own stream (seeded by rank): independent jobs, no collective on the data path
     out = {}
     for precision in ("fp32c", "fp64"):
-        jobs, arrivals = configs.serving_jobs(args.jobs, seed=5 + 1000 * rank, precision=precision)
+        # one global stream of jobs x world, dealt to the ranks by footprint
+        jobs, arrivals = configs.serving_jobs(args.jobs * world, seed=5, precision=precision)
+        mine = replicas.shard_by_footprint([w["materials"][0].general.n for w in jobs], world)[rank]
+        jobs, arrivals = [jobs[i] for i in mine], [arrivals[i] for i in mine]
         warm, warm_arr = configs.serving_jobs(4, seed=99, n_lo=5e3, n_hi=2e4, steps_lo=100, steps_hi=200,
                                               precision=precision)
         with pb.Server(device=local) as srv:
@@ -288,15 +290,8 @@ def run_serving(args, rank, world, local):
                     dist.barrier()
                 recs, summary = pb.serve_stream(srv, jobs, arrivals)
                 runs.append(summary)
-        wall = max(r["wall_s"] for r in runs)
-        bonds = sum(r["bond_updates"] for r in runs) / len(runs)
-        if dist is not None:
-            t = torch.tensor([wall, bonds], device="cuda", dtype=torch.float64)
-            w_ = t[:1].clone()
-            dist.all_reduce(w_, op=dist.ReduceOp.MAX)
-            b_ = t[1:].clone()
-            dist.all_reduce(b_, op=dist.ReduceOp.SUM)
-            wall, bonds = float(w_.item()), float(b_.item())
+        wall, bonds = replicas.reduce_timing(max(r["wall_s"] for r in runs),
+                                             sum(r["bond_updates"] for r in runs) / len(runs), dist, "cuda")
         out[precision] = {"value": bonds / wall, "wall_s": wall,
                           "latency_ms": runs[-1]["latency_ms"], "jobs": runs[-1]["jobs"]}
     if rank == 0:
@@ -447,16 +442,7 @@ def main():
     prof_n = ctypes_i64()
     _abi.check(L.pd_env_profile_read(env._h, ctypes.byref(prof_ms), ctypes.byref(prof_n)))
     _abi.check(L.pd_env_profile(env._h, 0))
-    t_total = float(sum(times))
-    if dist is not None:
-        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_total = float(t.item())
-        nb = torch.tensor([sum(bonds)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(nb, op=dist.ReduceOp.SUM)
-        total_bonds = float(nb.item())
-    else:
-        total_bonds = float(sum(bonds))
+    t_total, total_bonds = replicas.reduce_timing(sum(times), sum(bonds), dist, "cuda")
     value = total_bonds / t_total
     # end-to-end through the public API with host buffers
     h2d = hy.numel() * 8 + hv.numel() * 8
@@ -488,11 +474,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_times.append(e0.elapsed_time(e1) / 1e3)
-    e2e_t = float(sum(e2e_times))
-    if dist is not None:
-        t = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t, _ = replicas.reduce_timing(sum(e2e_times), 0.0, dist, "cuda")
     e2e_value = total_bonds / e2e_t
     # the state now holds one complete run from the initial state
     accuracy = None
