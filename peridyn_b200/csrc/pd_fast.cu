@@ -149,6 +149,7 @@ struct Split {
     static constexpr int NW = BT / 32;                // warps per block
     static constexpr int SPB = NW / WPS;              // slices per block
     static constexpr int MINB = 1024 / BT;            // resident blocks per SM aimed for (<= 64 registers)
+    static constexpr int MINB_THETA = 1280 / BT;      // the dilatation walk fits 48 registers
 };
 
 // The index loads of a bond walk depend on nothing, but each thread only
@@ -599,7 +600,7 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
 template <class R, int WPS, int U>
-__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_theta(StepArgs<R> a) {
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB_THETA : 1) k_theta(StepArgs<R> a) {
     using V4 = typename Tr<R>::V4;
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB, CS = Split<WPS>::CS;
     __shared__ R sh[WPS > 1 ? NW : 1][1][32];
