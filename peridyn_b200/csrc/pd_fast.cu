@@ -59,10 +59,18 @@ struct Tr<float> {
     }
     // One 256-bit load of a particle record (x, volume | u, -); the record
     // buffer is not written while a kernel reads it.
+    // NC = false: a coherent load, for the persistent kernel, which reads
+    // records other blocks wrote earlier in the same launch
+    template <bool NC = true>
     static __device__ __forceinline__ void load_rec(const float4 *r, float4 &x, float4 &u) {
-        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-            : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
-            : "l"(r));
+        if (NC)
+            asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
+                : "l"(r));
+        else
+            asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
+                         : "l"(r));
     }
 };
 template <>
@@ -73,9 +81,17 @@ struct Tr<double> {
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
     static __device__ __forceinline__ double sqrt_(double a) { return sqrt(a); }
     static __device__ __forceinline__ double rcp(double a) { return 1.0 / a; }
+    template <bool NC = true>
     static __device__ __forceinline__ void load_rec(const double4 *r, double4 &x, double4 &u) {
-        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w) : "l"(r));
-        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r + 1));
+        if (NC) {
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w) : "l"(r));
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r + 1));
+        } else {
+            asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x.x), "=d"(x.y), "=d"(x.z), "=d"(x.w)
+                         : "l"(r));
+            asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w)
+                         : "l"(r + 1));
+        }
     }
 };
 
@@ -196,6 +212,7 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
     old = __shfl_sync(0xffffffffu, old, 0);
     if (old != WPS - 1) return false;
     __threadfence_block();
+    if (lane == 0) arrive[sl] = 0;  // every warp of the slice has arrived: ready for reuse
     const int w0 = wid - w;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
@@ -258,7 +275,7 @@ struct Kin<float> {
     }
 };
 
-template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI>
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
                                           typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz) {
@@ -283,7 +300,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
+            Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
             // stretch s = num / dl;  |Y|^2 = |xi|^2 + num
@@ -316,7 +333,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
     }
 }
 
-template <class R, int KIND, bool kBreak, int WPS, int U>
+template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
                                             typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
                                             R &fz) {
@@ -331,17 +348,17 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
     }
     if (B.nt > 1) {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, true>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
                                                            fy, fz);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, true>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
+            bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
                                                             Ap, Bp, fx, fy, fz);
     } else {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, false>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
                                                             fy, fz);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
+            bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
                                                              up, Ap, Bp, fx, fy, fz);
     }
 }
@@ -451,20 +468,16 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 template <class R, int MODE>
 __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
 
-template <class R, int WPS, int U, int MODE>
-__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_step(StepArgs<R> a) {
+// One step of one slice (its WPS warps): bond gather, fixed-order
+// combination, integration.  Shared by k_step and the persistent kernel.
+template <class R, int WPS, int U, int MODE, bool NC>
+__device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], int *arrive) {
     using V4 = typename Tr<R>::V4;
-    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
-    __shared__ R sh[WPS > 1 ? NW : 1][3][32];
-    __shared__ int arrive[SPB];
+    constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    if (WPS > 1) {
-        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
-        __syncthreads();
-    }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
-    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
+    if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     constexpr bool kBreak = MODE != 5 && MODE != 6;
     R f[3] = {0, 0, 0};
@@ -473,12 +486,12 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             V4 xp, up;
-            Tr<R>::load_rec(a.xu + 2 * p, xp, up);
+            Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
             if (B.kind == PD_MAT_BOND_BASED)
-                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
+                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
             else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U>(a, p, w, B, tp, xp, up, f[0], f[1],
-                                                                          f[2]);
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1],
+                                                                              f[2]);
         }
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 3>(sh, arrive, wid, lane, f)) return;
@@ -490,6 +503,18 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     }
     const R ir = a.irho[p];
     integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
+}
+
+template <class R, int WPS, int U, int MODE>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_step(StepArgs<R> a) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][3][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    step_body<R, WPS, U, MODE, true>(a, sh, arrive);
 }
 
 // MODE 3/4: integration of forces already in f (after contact forces).
@@ -568,7 +593,7 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     store_u(a, p, u0, u1, u2);
 }
 
-template <class R, int WPS, int U, bool ST>
+template <class R, int WPS, int U, bool ST, bool NC = true>
 __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
                                         const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up) {
     using V4 = typename Tr<R>::V4;
@@ -586,7 +611,7 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            Tr<R>::load_rec(a.xu + 2 * (int64_t)q, xq, uq);
+            Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num;
             const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
@@ -599,39 +624,111 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
-template <class R, int WPS, int U>
-__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB_THETA : 1) k_theta(StepArgs<R> a) {
+template <class R, int WPS, int U, bool NC>
+__device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32], int *arrive) {
     using V4 = typename Tr<R>::V4;
-    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB, CS = Split<WPS>::CS;
-    __shared__ R sh[WPS > 1 ? NW : 1][1][32];
-    __shared__ int arrive[SPB];
+    constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    if (WPS > 1) {
-        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
-        __syncthreads();
-    }
     const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
-    if (p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
+    if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
     R acc = 0;
     if (lps) {
         V4 xp, up;
-        Tr<R>::load_rec(a.xu + 2 * p, xp, up);
+        Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
         const int32_t n = a.cnt[p];
         const SliceInfo d = a.si[p >> 5];
         const uint32_t *wp = a.words + d.word + (p & 31);
         if (d.mode == kStencil)
-            acc = theta_walk<R, WPS, U, true>(a, p, w, n, a.nbr + d.nbr, wp, xp, up);
+            acc = theta_walk<R, WPS, U, true, NC>(a, p, w, n, a.nbr + d.nbr, wp, xp, up);
         else
-            acc = theta_walk<R, WPS, U, false>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, xp, up);
+            acc = theta_walk<R, WPS, U, false, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, xp, up);
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 1>(sh, arrive, wid, lane, &acc)) return;
     if (!lps) return;
     typename Tr<R>::V2 mb = a.mab[p];
     mb.x = R(3) * acc * mb.y * mb.y;  // theta/m = (3/m) acc / m
     a.mab[p] = mb;
+}
+
+template <class R, int WPS, int U>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB_THETA : 1) k_theta(StepArgs<R> a) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][1][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    theta_body<R, WPS, U, true>(a, sh, arrive);
+}
+
+// ---------------------------------------------------------------------
+// Persistent chunk: nsteps full steps (dilatation phase, force + integration
+// phase) in one cooperative launch, phases separated by a grid barrier, so
+// small problems pay no per-kernel launch and ramp-up.  Records written in
+// one phase are read by other blocks in the next, hence coherent loads.
+// ---------------------------------------------------------------------
+struct GridBar {
+    unsigned count, gen;
+    int err, pad;
+};
+constexpr unsigned kBarrierSpins = 1u << 25;  // x >= 64 ns: gives up after ~2 s
+
+// Grid-wide barrier of a cooperative launch; false (and the error flag set)
+// when a block waited past kBarrierSpins.
+__device__ __forceinline__ bool grid_barrier(GridBar *gb, unsigned nblocks) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = &gb->gen;
+        volatile int *verr = &gb->err;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&gb->count, 1u) == nblocks - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            for (unsigned it = 0; *vgen == g && !*verr; ++it) {
+                if (it > kBarrierSpins) {
+                    atomicExch(&gb->err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    __threadfence();
+    return *(volatile int *)&gb->err == 0;
+}
+
+template <class R, int WPS, int U, bool LPS>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1)
+    k_persist(StepArgs<R> a, typename Tr<R>::V4 *b0, typename Tr<R>::V4 *b1, int nsteps, GridBar *gb) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][3][32];
+    __shared__ R sh1[WPS > 1 ? NW : 1][1][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    const int64_t ts0 = a.ts;
+    for (int s = 0; s < nsteps; ++s) {
+        a.xu = (s & 1) ? b1 : b0;
+        a.xn = (s & 1) ? b0 : b1;
+        a.ts = ts0 + s;
+        if (LPS) {
+            theta_body<R, WPS, U, false>(a, sh1, arrive);
+            if (!grid_barrier(gb, gridDim.x)) return;
+        }
+        step_body<R, WPS, U, 1, false>(a, sh, arrive);
+        if (s + 1 < nsteps && !grid_barrier(gb, gridDim.x)) return;
+    }
 }
 
 // Deformed gate on y = x + u (general_material.jl:243-255).
@@ -895,6 +992,8 @@ struct Fast {
     DBuf<V4> tune;        // autotuner output scratch
     DBuf<double> tune_d;
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
+    DBuf<GridBar> gbar;   // persistent-chunk barrier state
+    bool persisted = false;
     int cur = 0;
     int wps = 0;          // warps per 32-particle slice (autotuned)
     // CUDA graphs of kGraphSteps velocity-Verlet steps, keyed by the first
@@ -1446,6 +1545,67 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
     return PD_OK;
 }
 
+// Steps from the current time_step before the next BC direction flip (at most maxn).
+int64_t flip_free_run(const pd_env *env, int64_t maxn) {
+    int64_t n = 0;
+    for (; n < maxn; ++n)
+        for (const auto &h : env->hbc)
+            if (h.kind == PD_BC_TOFRO && (env->ts + n > h.applyafter) && std::fmod((double)(env->ts + n), h.freq) == 0.0)
+                return n;
+    return n;
+}
+
+// Launch nsteps full steps as one persistent cooperative kernel when the
+// whole grid (at the largest warps-per-slice that fits) can be resident;
+// *done = false leaves the steps to the caller.
+template <class R, int WPS, int U, bool LPS>
+pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
+    constexpr int BT = Split<WPS>::BT, SPB = Split<WPS>::SPB;
+    void (*kern)(StepArgs<R>, typename Tr<R>::V4 *, typename Tr<R>::V4 *, int, GridBar *) = k_persist<R, WPS, U, LPS>;
+    const int64_t blocks = ((env->N + 31) / 32 + SPB - 1) / SPB;
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, 0));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, env->device));
+    if (blocks > (int64_t)per_sm * sms) {
+        *done = false;
+        return PD_OK;
+    }
+    if (!F.gbar.p) {
+        PD_TRY(F.gbar.alloc(1));
+        CK(cudaMemsetAsync(F.gbar.p, 0, sizeof(GridBar), env->st));
+    }
+    StepArgs<R> a = args(env, F);
+    a.dir_vel = a.dir_pos = dir_bits(env);
+    a.ts = env->ts + 1;
+    typename Tr<R>::V4 *b0 = F.xu[F.cur].p, *b1 = F.xu[1 - F.cur].p;
+    GridBar *gb = F.gbar.p;
+    void *kargs[] = {&a, &b0, &b1, &nsteps, &gb};
+    CK(cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)blocks), dim3(BT), kargs, 0, env->st));
+    add_launches(1);
+    for (int k = 0; k < nsteps; ++k) advance_bc_clock(env);
+    if (nsteps & 1) F.cur = 1 - F.cur;
+    F.persisted = true;
+    *done = true;
+    return PD_OK;
+}
+
+// The persistent kernel runs the environment's kernel shape (F.wps), so a
+// run gives the same numbers whichever launch path each step takes.
+template <class R, bool LPS>
+pd_status persist_any(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
+    constexpr int LO = Unroll<R>::LO, HI = Unroll<R>::HI;
+    switch (F.wps) {
+        case 10 + LO: return persist_try<R, 1, LO, LPS>(env, F, nsteps, done);
+        case 10 + HI: return persist_try<R, 1, HI, LPS>(env, F, nsteps, done);
+        case 20 + LO: return persist_try<R, 2, LO, LPS>(env, F, nsteps, done);
+        case 20 + HI: return persist_try<R, 2, HI, LPS>(env, F, nsteps, done);
+        case 40 + LO: return persist_try<R, 4, LO, LPS>(env, F, nsteps, done);
+        case 40 + HI: return persist_try<R, 4, HI, LPS>(env, F, nsteps, done);
+        case 80 + LO: return persist_try<R, 8, LO, LPS>(env, F, nsteps, done);
+        default: return persist_try<R, 8, HI, LPS>(env, F, nsteps, done);
+    }
+}
+
 template <class R>
 pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true) {
     cudaStream_t st = env->st;
@@ -1465,8 +1625,30 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
     // kGraphSteps steps while the BC directions stay constant; the rest
     // (contacts, direction flips, the last step, profiling) launch directly.
     const bool graphs = !contacts && !env->prof && !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
+    // With PD_PERSIST=1, once every block has deformed (no gate), flip-free
+    // runs go to one persistent cooperative launch when the grid of the
+    // chosen shape fits on the device.  Off by default: on B200 the graph
+    // replays measured faster (40 k-particle LPS bar at 2 warps/slice: 44.7
+    // against 49.1 us per step; 17.6 k-particle PMB cube: 15.6 against
+    // 17.5 us), the grid barriers costing more than graph kernel boundaries.
+    const char *pe = std::getenv("PD_PERSIST");
+    const bool persist = graphs && pe && std::strcmp(pe, "1") == 0;
+    bool persist_fits = true;
     PD_TRY(gate_prepare(env, F));
     for (int64_t s = 0; s < nsteps;) {
+        if (persist && persist_fits && F.gitems_h.empty() && nsteps - 1 - s >= 8) {
+            const int64_t m = flip_free_run(env, std::min<int64_t>(nsteps - 1 - s, 1 << 20));
+            if (m >= 8) {
+                bool done = false;
+                if (lps) PD_TRY((persist_any<R, true>(env, F, (int)m, &done)));
+                else PD_TRY((persist_any<R, false>(env, F, (int)m, &done)));
+                if (done) {
+                    s += m;
+                    continue;
+                }
+                persist_fits = false;
+            }
+        }
         if (graphs && nsteps - 1 - s >= kGraphSteps && flip_free_steps(env, kGraphSteps)) {
             PD_TRY(poll_gate_flags(env, F));
             PD_TRY(replay_graph(env, F, lps));
@@ -1639,6 +1821,24 @@ void fast_release(pd_env *env) {
     env->fast_valid = false;
 }
 
+// A persistent chunk whose grid barrier gave up (blocks not co-resident)
+// leaves its error flag set: report it and clear it.
+pd_status persist_check(pd_env *env) {
+    FastHolder *h = holder(env);
+    auto chk = [&](auto &F) -> pd_status {
+        if (!F.persisted) return PD_OK;
+        F.persisted = false;
+        GridBar gb;
+        CK(cudaMemcpy(&gb, F.gbar.p, sizeof(gb), cudaMemcpyDeviceToHost));
+        if (gb.err) {
+            CK(cudaMemset(F.gbar.p, 0, sizeof(GridBar)));
+            return fail(PD_ERR_TIMEOUT, "persistent step kernel: grid barrier timed out");
+        }
+        return PD_OK;
+    };
+    return h->prec == PD_PREC_FP32C ? chk(h->f32) : chk(h->f64);
+}
+
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps) {
     if (nsteps == 0) return PD_OK;
     PD_TRY(ensure_fast(env));
@@ -1648,7 +1848,7 @@ pd_status fast_vv_steps(pd_env *env, int64_t nsteps) {
     h->dirty = true;
     PD_TRY(refresh_deformed_flags(env));
     CK(cudaStreamSynchronize(env->st));
-    return PD_OK;
+    return persist_check(env);
 }
 
 pd_status fast_update_acc(pd_env *env) {

@@ -217,3 +217,27 @@ def test_scaling_and_container_bcs_fast(oracle, precision, kind):
     assert ev <= TOL[precision], f"velocity rel-L2 {ev:.3e}"
     assert mism == 0
     env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_persistent_chunks_match_graph_replays(precision, monkeypatch):
+    # PD_PERSIST=1: flip-free runs of a deformed problem in one cooperative
+    # launch with grid barriers; same shape, so the same numbers
+    w = configs.lps_bar(nx=30, ny=8, nz=8)
+
+    def run(persist):
+        if persist:
+            monkeypatch.setenv("PD_PERSIST", "1")
+        else:
+            monkeypatch.delenv("PD_PERSIST", raising=False)
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+        env.set_kernel_shape(2, 2 if precision == "fp32c" else 1)
+        pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=40)   # deforms: the gate drops out
+        pb.velocity_verlet_step(env, nsteps=120)  # persistent when enabled
+        out = env.get_state()
+        env.close()
+        return out
+
+    for a, b in zip(run(False), run(True)):
+        assert np.array_equal(a, b)
