@@ -54,6 +54,8 @@ def build_workload(name, args):
         return configs.batched_cubes(nspec=args.nspec)
     if name == "disk_impact":
         return configs.disk_impact()
+    if name == "elasto_plastic":
+        return configs.ep_bar()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -177,6 +179,14 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_threads(work):
+    """Host threads the oracle uses for this workload: all cores, except
+    the elasto-plastic restatement, which is single-threaded."""
+    if any(m.specific.kind == 3 for m in work["materials"]):
+        return 1
+    return os.cpu_count() or 1
 
 
 def cpu_sample(work, seconds, nthreads):
@@ -314,7 +324,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     work = build_workload(args.workload, args)
-    nthreads = os.cpu_count() or 1
+    nthreads = cpu_threads(work)
     per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
     vals = []
     samples = []
@@ -330,7 +340,8 @@ def run_reference(args, rank, world):
             "config": {"workload": work["workload"], "precision": "fp64", "particles": None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                              "sample": f"{samples[0][0]} velocity-Verlet steps per bench step of "
-                                       f"{work['workload']} (OpenMP, atomic scatter)"},
+                                       f"{work['workload']} "
+                                       + ("(OpenMP, atomic scatter)" if nthreads > 1 else "(single thread)")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -342,7 +353,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="lps_bar",
-                    choices=["lps_bar", "pmb_cube", "batched", "disk_impact", "serving"])
+                    choices=["lps_bar", "pmb_cube", "batched", "disk_impact", "elasto_plastic", "serving"])
     ap.add_argument("--jobs", type=int, default=48, help="serving: jobs per stream")
     ap.add_argument("--precision", default="fp32c", choices=["fp64_serial", "fp64", "fp32c"])
     ap.add_argument("--no-fp64-compare", action="store_true",
@@ -384,7 +395,7 @@ def main():
     stream_ptr = ctypes_void()
     _abi.check(L.pd_env_stream(env._h, ctypes.byref(stream_ptr)))
     stream = torch.cuda.ExternalStream(stream_ptr.value, device=torch.device("cuda", local))
-    lps = any(m.specific.kind == 1 for m in work["materials"])
+    lps = any(m.specific.kind in (1, 3) for m in work["materials"])
     y0, v0, _, _ = env.get_state()
     # pinned host copies for the end-to-end arm
     hy = torch.from_numpy(np.ascontiguousarray(y0.T)).pin_memory()
@@ -531,10 +542,12 @@ def main():
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:
-        rate, n, dt = cpu_sample(work, args.cpu_sample_s, os.cpu_count() or 1)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+        nth = cpu_threads(work)
+        rate, n, dt = cpu_sample(work, args.cpu_sample_s, nth)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
                                 "sample": f"{n} velocity-Verlet steps of {work['workload']} in {dt:.1f} s "
-                                          f"(OpenMP over particles, atomic scatter)"}
+                                          + ("(OpenMP over particles, atomic scatter)" if nth > 1 else
+                                             "(single thread)")}
     env.close()
     print(json.dumps(line), flush=True)
     if dist is not None:

@@ -156,3 +156,19 @@ def serving_jobs(njobs, seed=5, rate=50.0, n_lo=5.0e3, n_hi=5.0e5, steps_lo=500,
         t += -math.log(1.0 - uk[5]) / rate
         arrivals.append(t)
     return jobs, arrivals
+
+
+def ep_bar(nx=100, ny=20, nz=20, yield_stress=2e6, steps=2000):
+    """The lps_bar tensile bar (Fix + Move BCs) as an elasto-plastic (Von
+    Mises) solid with the given yield stress; serial FP64 mode."""
+    from .materials import ElastoPlasticSolidSpecific
+
+    w = lps_bar(nx=nx, ny=ny, nz=nz, steps=steps)
+    mat = w["materials"][0]
+    E, nu = 70e9, 0.25
+    K = E / 3 / (1 - 2 * nu)
+    G = E / 2 / (1 + nu)
+    spc = ElastoPlasticSolidSpecific([K], [G], [0.01], [2700.0], [yield_stress])
+    w["materials"] = [PeridynamicsMaterial(mat.general, spc, name="ep_bar")]
+    w["workload"] = f"ep_bar_{nx}x{ny}x{nz}"
+    return w
