@@ -87,8 +87,13 @@ enum {
 };
 
 /* Contact models: contacts.jl ContactModel12 (two blocks) / ContactModel11
- * (self contact of one block); force law nonlinearspring.jl:124-145. */
-enum { PD_CONTACT_12 = 0, PD_CONTACT_11 = 1 };
+ * (self contact of one block); force law nonlinearspring.jl:124-145.
+ * PD_CONTACT_11 reproduces the reference's neighbour search, whose merge
+ * walk (contacts.jl:554-557) assumes ascending families and so finds at most
+ * the first family member; PD_CONTACT_11_ORDERED (extension) takes every
+ * family member whose bond is broken, in an adjacent search cell and within
+ * equi_dist, in family order, up to max_neighs. */
+enum { PD_CONTACT_12 = 0, PD_CONTACT_11 = 1, PD_CONTACT_11_ORDERED = 2 };
 
 typedef struct pd_env pd_env;
 

@@ -48,6 +48,7 @@ _SIG = {
     "or_contact12_neighs": (None, [I64, c_dp, I64, c_dp, D, I64, c_i64p]),
     "or_contact12_force": (None, [I64, I64, c_i64p, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, c_dp, D, D, D]),
     "or_contact11_neighs": (None, [I64, c_dp, I64, c_i64p, c_u8p, D, D, I64, I64, c_i64p]),
+    "or_contact11_neighs_ordered": (None, [I64, c_dp, I64, c_i64p, c_u8p, D, D, I64, I64, c_i64p]),
     "or_contact11_force": (None, [I64, I64, c_i64p, c_dp, c_dp, c_dp, c_dp, D, D, D]),
 }
 
@@ -295,8 +296,10 @@ class OracleEnv:
             else:
                 B = C.b1
                 x = np.asfortranarray(self.y[:, s1])
-                lib().or_contact11_neighs(B.n, _d(x), B.family.shape[0], _i(B.family), _u(B.intact), cm.distance,
-                                          cm.equi_dist, int(max_part), C.rows, _i(C.neighs))
+                search = lib().or_contact11_neighs_ordered if getattr(cm, "ordered", False) else \
+                    lib().or_contact11_neighs
+                search(B.n, _d(x), B.family.shape[0], _i(B.family), _u(B.intact), cm.distance, cm.equi_dist,
+                       int(max_part), C.rows, _i(C.neighs))
 
     # --------------------------------------------------------------- BCs
     def apply_bc_at0(self):

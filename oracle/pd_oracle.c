@@ -565,6 +565,43 @@ void or_contact11_neighs(int64_t n, const double *x, int64_t M,
     free(cell_of);
 }
 
+/* Ordered variant of contacts.jl:539-573: what the merge walk there sets out
+ * to find when families are not ascending.  Every family member j of a
+ * particle i whose bond is broken, whose get_cells cell (peri.jl:500-520) is
+ * one of the 27 around i's, and with |y_i - y_j|^2 < equi_dist^2 is listed,
+ * in stored family order, up to rows; the rest of the column is 0. */
+void or_contact11_neighs_ordered(int64_t n, const double *x, int64_t M,
+                                 const int64_t *family, const uint8_t *intact,
+                                 double search_distance, double equi_dist,
+                                 int64_t max_part, int64_t rows, int64_t *neighbors) {
+    memset(neighbors, 0, sizeof(int64_t) * (size_t)rows * (size_t)n);
+    if (n == 0) return;
+    int64_t *cell_of = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+    cells_t c;
+    get_cells(n, x, search_distance, max_part, &c, cell_of);
+    const double equi_dist2 = equi_dist * equi_dist;
+    const int64_t N0 = c.N[0], N1 = c.N[1];
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t ci = cell_of[i];
+        const int64_t ii[3] = {ci % N0, (ci / N0) % N1, ci / (N0 * N1)};
+        int64_t ind = 0;
+        for (int64_t k = 0; k < M && ind < rows; ++k) {
+            const int64_t j1 = COL(family, M, k, i);
+            if (j1 <= 0 || COL(intact, M, k, i)) continue;
+            const int64_t j = j1 - 1, cj = cell_of[j];
+            const int64_t jj[3] = {cj % N0, (cj / N0) % N1, cj / (N0 * N1)};
+            int adj = 1;
+            for (int d = 0; d < 3; ++d) adj &= llabs(ii[d] - jj[d]) <= 1;
+            const double d1 = x[3 * i] - x[3 * j], d2 = x[3 * i + 1] - x[3 * j + 1],
+                         d3 = x[3 * i + 2] - x[3 * j + 2];
+            const double dr2 = (d1 * d1 + d2 * d2) + d3 * d3;
+            if (adj && dr2 < equi_dist2) COL(neighbors, rows, ind++, i) = j1;
+        }
+    }
+    free_cells(&c);
+    free(cell_of);
+}
+
 /* contacts.jl:357-381 short_range_contact! (11, CPU) */
 void or_contact11_force(int64_t n, int64_t rows, const int64_t *neighs,
                         const double *x1, double *f1, const double *vol1,

@@ -115,6 +115,13 @@ void or_contact11_neighs(int64_t n, const double *x, int64_t M,
                          double search_distance, double equi_dist,
                          int64_t max_part, int64_t rows, int64_t *neighbors);
 
+/* Ordered variant of contacts.jl:539-573: every broken-bond family member
+ * in an adjacent cell and within equi_dist, in family order, up to rows. */
+void or_contact11_neighs_ordered(int64_t n, const double *x, int64_t M,
+                                 const int64_t *family, const uint8_t *intact,
+                                 double search_distance, double equi_dist,
+                                 int64_t max_part, int64_t rows, int64_t *neighbors);
+
 /* contacts.jl:357-381 short_range_contact! (ContactModel11, CPU). */
 void or_contact11_force(int64_t n, int64_t rows, const int64_t *neighs,
                         const double *x1, double *f1, const double *vol1,

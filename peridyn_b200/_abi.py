@@ -44,6 +44,7 @@ PD_BC_CONTAINER = 4
 
 PD_CONTACT_12 = 0
 PD_CONTACT_11 = 1
+PD_CONTACT_11_ORDERED = 2
 
 c_dp = ctypes.POINTER(ctypes.c_double)
 c_i64p = ctypes.POINTER(ctypes.c_int64)

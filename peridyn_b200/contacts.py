@@ -30,11 +30,19 @@ class NonLinearSpringContactModel12(ContactModel):
 
 
 class NonLinearSpringContactModel11(ContactModel):
-    """nonlinearspring.jl:32-44 with ContactModel11_gcal (contacts.jl:105-124)."""
+    """nonlinearspring.jl:32-44 with ContactModel11_gcal (contacts.jl:105-124).
 
-    kind = _abi.PD_CONTACT_11
+    ``ordered=False`` keeps the reference's neighbour search
+    (contacts.jl:539-573), whose merge walk assumes ascending families and so
+    finds at most the first family member.  ``ordered=True`` (an extension)
+    lists every family member whose bond is broken, in a search cell adjacent
+    to the particle's and within ``equi_dist``, in family order, up to
+    ``max_neighs`` of them.
+    """
 
-    def __init__(self, exponent, stifness, mat1, distanceD=1.0, distanceX=5, max_neighs=50):
+    def __init__(self, exponent, stifness, mat1, distanceD=1.0, distanceX=5, max_neighs=50, ordered=False):
+        self.ordered = bool(ordered)
+        self.kind = _abi.PD_CONTACT_11_ORDERED if self.ordered else _abi.PD_CONTACT_11
         self.exponent = float(exponent)
         self.stifness = float(stifness)
         self.type = mat1.type
@@ -48,15 +56,20 @@ class NonLinearSpringContactModel11(ContactModel):
         self.max_neighs = min(int(max_neighs), mat1.general.n)
 
 
-def NonLinearSpringContactModel(exponent, stifness, mat1, mat2=None, distanceD=1.0, distanceX=None, max_neighs=50):
+def NonLinearSpringContactModel(exponent, stifness, mat1, mat2=None, distanceD=1.0, distanceX=None, max_neighs=50,
+                                ordered=False):
     """nonlinearspring.jl:63-111: two blocks -> 12 (distanceX=3.0),
-    one block -> 11 (distanceX=5)."""
+    one block -> 11 (distanceX=5); ``ordered`` selects the ordered
+    self-contact search (one block only)."""
     if mat2 is not None:
+        if ordered:
+            raise ValueError("ordered neighbour search applies to self contact (one block) only")
         return NonLinearSpringContactModel12(exponent, stifness, mat1, mat2, distanceD=distanceD,
                                              distanceX=3.0 if distanceX is None else distanceX,
                                              max_neighs=max_neighs)
     return NonLinearSpringContactModel11(exponent, stifness, mat1, distanceD=distanceD,
-                                         distanceX=5 if distanceX is None else distanceX, max_neighs=max_neighs)
+                                         distanceX=5 if distanceX is None else distanceX, max_neighs=max_neighs,
+                                         ordered=ordered)
 
 
 def LinearSpringContactModel(stifness, mat1, mat2=None, **kwargs):

@@ -446,6 +446,37 @@ __global__ void k_c11_neighs(int64_t first, int64_t n, const double4 *__restrict
     nb11[li] = res;
 }
 
+// Every family member with a broken bond, in an adjacent search cell and
+// within equi_dist, in family (slot) order, up to rows.
+__global__ void k_c11_neighs_ordered(int64_t first, int64_t n, const double4 *__restrict__ y,
+                                     const SliceInfo *__restrict__ si, const int32_t *__restrict__ cnt,
+                                     const int32_t *__restrict__ nbr, const uint32_t *__restrict__ words,
+                                     const uint32_t *__restrict__ fam, RefCells rc, double equi2, int64_t rows,
+                                     int32_t *__restrict__ nb) {
+    int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (li >= n) return;
+    int64_t p = first + li;
+    const BondRef fr = bond_ref(si, nbr, fam, p);
+    const int64_t wb = fr.w - fam;
+    const int32_t c = cnt[p];
+    const double4 a = y[p];
+    int64_t r = 0;
+    for (int32_t k = 0; k < c && r < rows; ++k) {
+        const uint32_t bit = 1u << (k & 31);
+        const int64_t wi = wb + 32 * (int64_t)(k >> 5);
+        if (!(fam[wi] & bit) || (words[wi] & bit)) continue;  // not a member, or intact
+        const int32_t q = fr.q(k);
+        const double4 b = y[q];
+        const bool adj = abs(ref_cell(rc, a.x, 0) - ref_cell(rc, b.x, 0)) <= 1 &&
+                         abs(ref_cell(rc, a.y, 1) - ref_cell(rc, b.y, 1)) <= 1 &&
+                         abs(ref_cell(rc, a.z, 2) - ref_cell(rc, b.z, 2)) <= 1;
+        const double d1 = a.x - b.x, d2 = a.y - b.y, d3 = a.z - b.z;
+        const double dr2 = ((d1 * d1 + d2 * d2) + d3 * d3);
+        if (adj && dr2 < equi2) nb[r++ * n + li] = q;
+    }
+    for (; r < rows; ++r) nb[r * n + li] = -1;
+}
+
 __global__ void k_c11_rev_count(int64_t first, int64_t n, const int32_t *__restrict__ nb11, int32_t *__restrict__ rcnt) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -468,7 +499,7 @@ __global__ void k_c11_rev_fill(int64_t first, int64_t n, const int32_t *__restri
 //   i < p listing p:  f_p -= F(y_i - y_p) .* (V_p / rho_p)
 //   own neighbour q:  f_p += F(y_p - y_q) .* (V_q / rho_p)
 //   i > p listing p:  f_p -= F(y_i - y_p) .* (V_p / rho_p)
-__global__ void k_c11_force(int64_t first, int64_t n, const int32_t *__restrict__ nb11,
+__global__ void k_c11_force(int64_t first, int64_t n, int64_t nbrows, const int32_t *__restrict__ nb11,
                             const int32_t *__restrict__ roff, const int32_t *__restrict__ rev,
                             const double4 *__restrict__ y, const double4 *__restrict__ x4,
                             const double *__restrict__ dens, CLaw law, double4 *__restrict__ f) {
@@ -476,8 +507,7 @@ __global__ void k_c11_force(int64_t first, int64_t n, const int32_t *__restrict_
     if (li >= n) return;
     int64_t p = first + li;
     int32_t o = roff[li], e = roff[li + 1];
-    int32_t q = nb11[li];
-    if (o == e && q < 0) return;
+    if (o == e && nb11[li] < 0) return;
     double4 yp = y[p], fp = f[p];
     double den_p = dens[p], vol_p = x4[p].w;
     double F1, F2, F3;
@@ -490,7 +520,9 @@ __global__ void k_c11_force(int64_t first, int64_t n, const int32_t *__restrict_
         fp.y = fp.y - F2 * s;
         fp.z = fp.z - F3 * s;
     }
-    if (q >= 0) {
+    for (int64_t k = 0; k < nbrows; ++k) {  // p's own neighbours, in row order
+        const int32_t q = nb11[k * n + li];
+        if (q < 0) break;
         double4 yq = y[q];
         contact_fn(law, yp.x - yq.x, yp.y - yq.y, yp.z - yq.z, F1, F2, F3);
         double s = x4[q].w / den_p;
@@ -625,11 +657,21 @@ pd_status update11(pd_env *env, const HostContact &hc, DevContact &dc, int64_t m
     for (int d = 0; d < 3; ++d) rc.mn[d] = m[d];
     rc.h = hc.distance;
     rc.maxpart = (double)max_part;
-    k_c11_neighs<<<gridn(dc.n1), kT, 0, st>>>(dc.first1, dc.n1, env->y.p, env->sinfo.p, env->cnt.p, env->nbr.p,
-                                              env->words[env->cur].p, env->fam.p, rc, hc.equi_dist * hc.equi_dist, dc.nb.p); pd::note_launch();
+    if (hc.kind == PD_CONTACT_11_ORDERED) {
+        k_c11_neighs_ordered<<<gridn(dc.n1), kT, 0, st>>>(dc.first1, dc.n1, env->y.p, env->sinfo.p, env->cnt.p,
+                                                          env->nbr.p, env->words[env->cur].p, env->fam.p, rc,
+                                                          hc.equi_dist * hc.equi_dist, dc.nbrows, dc.nb.p);
+        pd::note_launch();
+    } else {
+        k_c11_neighs<<<gridn(dc.n1), kT, 0, st>>>(dc.first1, dc.n1, env->y.p, env->sinfo.p, env->cnt.p, env->nbr.p,
+                                                  env->words[env->cur].p, env->fam.p, rc, hc.equi_dist * hc.equi_dist,
+                                                  dc.nb.p);
+        pd::note_launch();
+    }
     CK(cudaGetLastError());
     dc.has_neighs = true;
-    PD_TRY(build_reverse(env, dc, dc.n1, dc.first1, dc.n1, dc.first1, dc.nb.p, 1, true));
+    PD_TRY(build_reverse(env, dc, dc.n1, dc.first1, dc.n1, dc.first1, dc.nb.p, dc.nbrows,
+                         hc.kind != PD_CONTACT_11_ORDERED));
     CK(cudaStreamSynchronize(st));
     return PD_OK;
 }
@@ -662,6 +704,7 @@ pd_status contacts_finalize(pd_env *env) {
             dc.n2 = b2.n;
             dc.first2 = b2.first_int;
             dc.rows = std::min<int64_t>(hc.max_neighs, b2.n);  // ContactModel12_gcal
+            dc.nbrows = dc.rows;
             PD_TRY(dc.nb.alloc((size_t)dc.n1 * dc.rows));
             CK(cudaMemsetAsync(dc.nb.p, 0xff, (size_t)dc.n1 * dc.rows * 4, env->st));
             PD_TRY(dc.rev_off.alloc(dc.n2 + 1));
@@ -671,8 +714,9 @@ pd_status contacts_finalize(pd_env *env) {
             dc.n2 = b1.n;
             dc.first2 = b1.first_int;
             dc.rows = hc.max_neighs;  // ContactModel11_gcal: zeros(max_neighs, N)
-            PD_TRY(dc.nb.alloc((size_t)dc.n1));
-            CK(cudaMemsetAsync(dc.nb.p, 0xff, (size_t)dc.n1 * 4, env->st));
+            dc.nbrows = hc.kind == PD_CONTACT_11_ORDERED ? dc.rows : 1;
+            PD_TRY(dc.nb.alloc((size_t)dc.n1 * dc.nbrows));
+            CK(cudaMemsetAsync(dc.nb.p, 0xff, (size_t)dc.n1 * dc.nbrows * 4, env->st));
             PD_TRY(dc.rev_off.alloc(dc.n1 + 1));
             PD_TRY(dc.rev_cnt.alloc(dc.n1 + 1));
             CK(cudaMemsetAsync(dc.rev_off.p, 0, (dc.n1 + 1) * 4, env->st));
@@ -705,7 +749,7 @@ pd_status contacts_force(pd_env *env) {
             k_c12_force2<<<gridn(dc.n2), kT, 0, env->st>>>(dc.first2, dc.n2, dc.rev_off.p, dc.rev.p, env->y.p,
                                                            env->x4.p, env->dens.p, law, env->f.p); pd::note_launch();
         } else {
-            k_c11_force<<<gridn(dc.n1), kT, 0, env->st>>>(dc.first1, dc.n1, dc.nb.p, dc.rev_off.p, dc.rev.p, env->y.p,
+            k_c11_force<<<gridn(dc.n1), kT, 0, env->st>>>(dc.first1, dc.n1, dc.nbrows, dc.nb.p, dc.rev_off.p, dc.rev.p, env->y.p,
                                                           env->x4.p, env->dens.p, law, env->f.p); pd::note_launch();
         }
         CK(cudaGetLastError());
@@ -735,11 +779,14 @@ extern "C" pd_status pd_env_get_contact_neighs(pd_env *env, int64_t contact, int
                 neighs[(size_t)i * dc.rows + r] = j < 0 ? 0 : (int64_t)(j - dc.first2 + 1);
             }
     } else {
-        std::vector<int32_t> h(dc.n1);
+        std::vector<int32_t> h((size_t)dc.n1 * dc.nbrows);
         CK(cudaMemcpyAsync(h.data(), dc.nb.p, h.size() * 4, cudaMemcpyDeviceToHost, env->st));
         CK(cudaStreamSynchronize(env->st));
         for (int64_t i = 0; i < dc.n1; ++i)
-            neighs[(size_t)i * dc.rows] = h[i] < 0 ? 0 : (int64_t)(h[i] - dc.first1 + 1);
+            for (int64_t r = 0; r < dc.nbrows; ++r) {
+                const int32_t j = h[r * dc.n1 + i];
+                neighs[(size_t)i * dc.rows + r] = j < 0 ? 0 : (int64_t)(j - dc.first1 + 1);
+            }
     }
     return PD_OK;
 }

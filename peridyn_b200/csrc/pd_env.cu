@@ -452,7 +452,8 @@ extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block
                                         double distance, int64_t max_neighs, int64_t *out_contact) {
     PD_TRY(check_env(env));
     if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
-    if (kind != PD_CONTACT_12 && kind != PD_CONTACT_11) return fail(PD_ERR_ARG, "unknown contact kind %d", kind);
+    if (kind != PD_CONTACT_12 && kind != PD_CONTACT_11 && kind != PD_CONTACT_11_ORDERED)
+        return fail(PD_ERR_ARG, "unknown contact kind %d", kind);
     int64_t nb = (int64_t)env->hb.size();
     if (block1 < 0 || block1 >= nb) return fail(PD_ERR_ARG, "no block %lld", (long long)block1);
     if (kind == PD_CONTACT_12 && (block2 < 0 || block2 >= nb || block2 == block1))

@@ -123,7 +123,8 @@ struct DevContact {
     int64_t n1 = 0, n2 = 0;       // particles of pair[1] / pair[2] (block sizes)
     int64_t first1 = 0, first2 = 0;  // internal first index of the two blocks
     int64_t rows = 0;
-    DBuf<int32_t> nb;       // n1 x rows, internal indices of set-2 particles, -1 pad
+    int64_t nbrows = 0;     // rows stored in nb (1 for the reference contact-11 search)
+    DBuf<int32_t> nb;       // nbrows x n1 (row r of particle i at r*n1+i), internal indices, -1 pad
     DBuf<int32_t> rev_off;  // n2+1 reverse-list offsets
     DBuf<int32_t> rev;      // reverse lists (internal indices of set-1 particles, ascending)
     DBuf<int32_t> rev_cnt;  // n2 scratch

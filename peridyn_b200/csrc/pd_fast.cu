@@ -936,13 +936,13 @@ __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_
 }
 
 template <class R>
-__global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, const int32_t *nb11, const int32_t *roff,
-                       const int32_t *rev, const double *dens, CLawF law) {
+__global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, int64_t nbrows, const int32_t *nb11,
+                       const int32_t *roff, const int32_t *rev, const double *dens, CLawF law) {
     const int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (li >= n) return;
     const int64_t p = first + li;
-    const int32_t o = roff[li], e = roff[li + 1], q = nb11[li];
-    if (o == e && q < 0) return;
+    const int32_t o = roff[li], e = roff[li + 1];
+    if (o == e && nb11[li] < 0) return;
     double yp0, yp1, yp2, a0 = 0, a1 = 0, a2 = 0, F0, F1, F2;
     ypos(a, p, yp0, yp1, yp2);
     const double den = dens[p], vol = a.x64[p].w;
@@ -954,7 +954,9 @@ __global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, const int32_t *n
         a1 -= F1 * (vol / den);
         a2 -= F2 * (vol / den);
     }
-    if (q >= 0) {
+    for (int64_t k = 0; k < nbrows; ++k) {
+        const int32_t q = nb11[k * n + li];
+        if (q < 0) break;
         double yq0, yq1, yq2;
         ypos(a, q, yq0, yq1, yq2);
         cfn(law, yp0 - yq0, yp1 - yq1, yp2 - yq2, F0, F1, F2);
@@ -1300,7 +1302,7 @@ pd_status contacts_fast(pd_env *env, StepArgs<R> &a) {
             note_launch();
             note_launch();
         } else {
-            k_fc11<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nb.p, dc.rev_off.p, dc.rev.p,
+            k_fc11<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nbrows, dc.nb.p, dc.rev_off.p, dc.rev.p,
                                                              env->dens.p, law);
             note_launch();
         }

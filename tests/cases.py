@@ -61,3 +61,32 @@ def ep_cube(sigma_y, n=10, peak=60.0, cs=0.02, seed=7, ntypes=1):
     spc = pb.ElastoPlasticSolidSpecific(K, G, [cs] * npairs, [2700.0, 2500.0][:ntypes], sy)
     mat = pb.PeridynamicsMaterial(gen, spc, name="ep_cube")
     return {"materials": [mat], "contacts": [], "bcs": [], "dt": 2.0e-8, "steps": 60}
+
+
+def self_contact_block(oracle, ordered=False, max_neighs=20, seed=8):
+    """A block with a random third of its bonds broken (symmetrically),
+    compressed to 0.7x so broken pairs come within the contact distance of a
+    linear-spring self contact.  Returns the workload and the families
+    (computed by the oracle) both sides are given."""
+    x, vol = lattice.cuboid(8, 8, 6, 1e-3, jitter=3e-5, seed=2)
+    fam, intact = oracle.cal_family(x, 3.015e-3, 200)
+    rng = np.random.default_rng(seed)
+    n = x.shape[1]
+    brk = set()
+    for i in range(n):
+        for k in range(fam.shape[0]):
+            j = fam[k, i]
+            if j > 0 and j - 1 > i and rng.random() < 0.35:
+                brk.add((i, j - 1))
+    intact = intact.copy()
+    for i in range(n):
+        for k in range(fam.shape[0]):
+            j = fam[k, i] - 1
+            if j >= 0 and ((i, j) in brk or (j, i) in brk):
+                intact[k, i] = False
+    y = np.asfortranarray(0.7 * x + rng.normal(0, 5e-5, size=x.shape))
+    gen = pb.GeneralMaterial(y, np.zeros_like(x, order="F"), x, vol, np.ones(n, dtype=np.int64), 3.015e-3,
+                             max_neigh=200)
+    mat = pb.PeridynamicsMaterial(gen, pb.BondBasedSpecific([10e9], [0.5], [2000.0]))
+    cm = pb.LinearSpringContactModel(1e18, mat, distanceX=5, max_neighs=max_neighs, ordered=ordered)
+    return {"materials": [mat], "contacts": [cm], "bcs": [], "dt": 1e-9}, [(fam, intact)]

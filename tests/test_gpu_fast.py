@@ -9,7 +9,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import configs, lattice
-from tests.cases import bar_with_bcs, random_cloud
+from tests.cases import bar_with_bcs, random_cloud, self_contact_block
 
 pytestmark = pytest.mark.gpu
 
@@ -128,6 +128,24 @@ def test_contact_impact_fast(oracle, precision):
     eu, ev, mism = _errors(env, ora)
     assert eu <= (1e-9 if precision == "fp64" else 2e-4), eu
     assert mism == 0
+    env.close()
+
+
+@pytest.mark.parametrize("ordered", [False, True])
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_self_contact_fast(oracle, precision, ordered):
+    w, families = self_contact_block(oracle, ordered=ordered)
+    env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision, families=families)
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"], families=families)
+    for _ in range(8):
+        ora.update_neighs()
+        pb.update_neighs(env)
+        assert np.array_equal(env.contact_neighs(0), ora.contacts[0].neighs)
+        ora.vv_step()
+        pb.velocity_verlet_step(env)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= TOL[precision], eu
+    assert ev <= (1e-9 if precision == "fp64" else 1e-3), ev
     env.close()
 
 

@@ -8,7 +8,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import _abi, configs, lattice
-from tests.cases import bar_with_bcs, ep_cube, random_cloud
+from tests.cases import bar_with_bcs, ep_cube, random_cloud, self_contact_block
 
 pytestmark = pytest.mark.gpu
 
@@ -258,42 +258,25 @@ def test_contact12_neighbours_and_forces_bit_exact(oracle):
     env.close()
 
 
-def test_contact11_self_contact_bit_exact(oracle, layout):
-    x, vol = lattice.cuboid(8, 8, 6, 1e-3, jitter=3e-5, seed=2)
-    fam, intact = oracle.cal_family(x, 3.015e-3, 200)
-    rng = np.random.default_rng(8)
-    # break a random third of the bonds (symmetrically) and compress the
-    # block so broken pairs come within the contact distance
-    n = x.shape[1]
-    brk = set()
-    for i in range(n):
-        for k in range(fam.shape[0]):
-            j = fam[k, i]
-            if j > 0 and j - 1 > i and rng.random() < 0.35:
-                brk.add((i, j - 1))
-    intact = intact.copy()
-    for i in range(n):
-        for k in range(fam.shape[0]):
-            j = fam[k, i] - 1
-            if j >= 0 and ((i, j) in brk or (j, i) in brk):
-                intact[k, i] = False
-    y = np.asfortranarray(0.7 * x + rng.normal(0, 5e-5, size=x.shape))
-    gen = pb.GeneralMaterial(y, np.zeros_like(x, order="F"), x, vol, np.ones(n, dtype=np.int64), 3.015e-3,
-                             max_neigh=200)
-    mat = pb.PeridynamicsMaterial(gen, pb.BondBasedSpecific([10e9], [0.5], [2000.0]))
-    cm = pb.LinearSpringContactModel(1e18, mat, distanceX=5, max_neighs=20)
-    w = {"materials": [mat], "contacts": [cm], "bcs": [], "dt": 1e-9}
-    env, ora = _pair(oracle, w, families=[(fam, intact)])
+@pytest.mark.parametrize("ordered", [False, True])
+def test_contact11_self_contact_bit_exact(oracle, layout, ordered):
+    """Both self-contact searches: the reference's merge walk (at most the
+    first family member) and the ordered search (every qualifying member,
+    so several rows per particle and reverse lists with several sources)."""
+    w, families = self_contact_block(oracle, ordered=ordered)
+    env, ora = _pair(oracle, w, families=families)
     _check_layout(env, layout)
-    hits = 0
+    hits = multi = 0
     for _ in range(8):
         ora.update_neighs()
         pb.update_neighs(env)
         assert np.array_equal(env.contact_neighs(0), ora.contacts[0].neighs)
         hits += int((ora.contacts[0].neighs > 0).sum())
+        multi += int((ora.contacts[0].neighs[1] > 0).sum())
         ora.vv_step()
         pb.velocity_verlet_step(env)
     assert hits > 0
+    assert (multi > 0) == ordered
     _assert_state_equal(env, ora)
     env.close()
 

@@ -194,6 +194,48 @@ def test_contact11_merge_walk_only_matches_first_member(oracle):
             assert nb[0, i] == expect
 
 
+def test_contact11_ordered_search_bruteforce(oracle):
+    """The ordered self-contact search lists every broken-bond family member
+    in an adjacent get_cells cell and within equi_dist, in family order; its
+    first entry agrees with the reference's merge walk wherever that finds
+    one."""
+    rng = np.random.default_rng(4)
+    x, vol = lattice.cuboid(7, 7, 4, 1.0, jitter=0.05, seed=5)
+    fam, intact = oracle.cal_family(x, 3.015, 200)
+    intact = np.asfortranarray(intact & (rng.random(intact.shape) > 0.3), dtype=np.uint8)
+    y = np.asfortranarray(x + rng.normal(0, 0.1, size=x.shape))
+    n = x.shape[1]
+    h, max_part, rows = 2.5, 30, 12
+    mn, mx = y.min(axis=1), y.max(axis=1)
+    N = np.clip(np.floor((mx - mn) / h), 1, max_part)
+    cell = np.clip(np.floor((y - mn[:, None]) / h), 1, max_part)
+    assert np.all(cell <= N[:, None])
+    for equi in (1.0, 1.5, 3.5):
+        ref = np.zeros((rows, n), dtype=np.int64, order="F")
+        nb = np.zeros((rows, n), dtype=np.int64, order="F")
+        args = (n, oracle._d(y), fam.shape[0], oracle._i(fam), oracle._u(intact), h, equi, max_part, rows)
+        oracle.lib().or_contact11_neighs(*args, oracle._i(ref))
+        oracle.lib().or_contact11_neighs_ordered(*args, oracle._i(nb))
+        longest = 0
+        for i in range(n):
+            expect = []
+            for k in range(fam.shape[0]):
+                j = fam[k, i] - 1
+                if j < 0 or intact[k, i] or np.any(np.abs(cell[:, i] - cell[:, j]) > 1):
+                    continue
+                d = y[:, i] - y[:, j]
+                if (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2] < equi * equi:
+                    expect.append(j + 1)
+            expect = expect[:rows]
+            longest = max(longest, len(expect))
+            assert list(nb[:len(expect), i]) == expect
+            assert np.all(nb[len(expect):, i] == 0)
+            if ref[0, i]:
+                assert nb[0, i] == ref[0, i]
+        if equi > 3:
+            assert longest > 1
+
+
 def test_contact12_neighs_bruteforce(oracle):
     rng = np.random.default_rng(11)
     x1 = np.asfortranarray(rng.uniform(0, 4, size=(3, 300)))
