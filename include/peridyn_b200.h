@@ -308,6 +308,17 @@ PD_API pd_status pd_env_set_kernel_shape(pd_env *env, int32_t warps_per_slice, i
 /* The shape the throughput path runs with (after autotuning); (0, 0)
  * before the first throughput-mode step or in the serial mode. */
 PD_API pd_status pd_env_kernel_shape(pd_env *env, int32_t *warps_per_slice, int32_t *unroll);
+/* Record staging of the FP32C kernels (extension): a stencil slice's
+ * neighbour records -- a few ranges of consecutive records -- are copied
+ * into shared memory by bulk asynchronous copies before its bonds are
+ * walked, with 4 or 8 warps per slice.  mode 0 (default): never; 1: staged
+ * shapes only (with a fixed kernel shape: its staged form); 2: the
+ * autotuner times staged and unstaged shapes.  Results are identical
+ * either way. */
+PD_API pd_status pd_env_set_record_staging(pd_env *env, int32_t mode);
+/* staged = 1 when the running FP32C shape stages; slices with a staging
+ * plan and the largest plan in records (any pointer may be NULL). */
+PD_API pd_status pd_env_record_staging(pd_env *env, int32_t *staged, int64_t *slices, int64_t *max_records);
 
 /* ---------------------------------------------------------------------- */
 /* Serving (extension): a request loop that admits simulation jobs by HBM  */

@@ -149,6 +149,8 @@ _SIGNATURES = {
     "pd_env_stage_read": (ctypes.c_int32, [c_vp, ctypes.c_int32, c_dp, c_dp, c_dp, c_dp, c_i64p]),
     "pd_env_set_kernel_shape": (ctypes.c_int32, [c_vp, ctypes.c_int32, ctypes.c_int32]),
     "pd_env_kernel_shape": (ctypes.c_int32, [c_vp, c_i32p, c_i32p]),
+    "pd_env_set_record_staging": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
+    "pd_env_record_staging": (ctypes.c_int32, [c_vp, c_i32p, c_i64p, c_i64p]),
     "pd_server_create": (ctypes.c_int32, [ctypes.POINTER(c_vp), ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
                                           ctypes.c_int64]),
     "pd_server_submit": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_int64, c_i64p]),

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pd_env_impl.h"
+#include "pd_stage_plan.h"
 
 using namespace pd;
 
@@ -576,6 +577,36 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
         }
     });
     cnt.swap(cnt_rt);
+    // pass 3 (per stencil slice): record staging plans
+    std::vector<std::vector<int32_t>> plans(S);
+    std::vector<int32_t> spos(nbr.size(), 0);
+    parallel_for(S, [&](int64_t s0, int64_t s1) {
+        std::vector<int32_t> rs, pos;
+        for (int64_t s = s0; s < s1; ++s) {
+            const SliceInfo &d = si[s];
+            if (d.mode != kStencil) continue;
+            const int64_t T = stage_plan(s * kSlice, N, uni[s], rs, pos);
+            if (T == 0 || T > kStageMaxRecords) continue;
+            std::copy(pos.begin(), pos.end(), spos.begin() + d.nbr);
+            std::vector<int32_t> &pl = plans[s];
+            pl.reserve(2 + rs.size());
+            pl.push_back((int32_t)(rs.size() / 2));
+            pl.push_back((int32_t)T);
+            pl.insert(pl.end(), rs.begin(), rs.end());
+        }
+    });
+    std::vector<int32_t> splan_off(S + 1, -1), splan;
+    int64_t nplan = 0, pmax = 0;
+    for (int64_t s = 0; s < S; ++s) {
+        if (plans[s].empty()) continue;
+        splan_off[s] = (int32_t)splan.size();
+        splan.insert(splan.end(), plans[s].begin(), plans[s].end());
+        pmax = std::max<int64_t>(pmax, plans[s][1]);
+        ++nplan;
+    }
+    if (splan.empty()) splan.push_back(0);
+    env->splan_slices = nplan;
+    env->splan_max = pmax;
     env->sinfo_h = si;
     env->cnt_h = cnt;
     env->nnz = (int64_t)kSlice * nwords;
@@ -596,6 +627,12 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     CK(cudaMemcpyAsync(env->words0.p, words.data(), nw * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(env->fam.p, fam.data(), nw * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    PD_TRY(env->splan_off.alloc(S + 1));
+    PD_TRY(env->splan.alloc((int64_t)splan.size()));
+    PD_TRY(env->spos.alloc((int64_t)spos.size()));
+    CK(cudaMemcpyAsync(env->splan_off.p, splan_off.data(), (S + 1) * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->splan.p, splan.data(), splan.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->spos.p, spos.data(), spos.size() * 4, cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     return PD_OK;
 }

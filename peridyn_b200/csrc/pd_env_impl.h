@@ -156,6 +156,13 @@ struct pd_env {
     int64_t nnz = 0;       // bond slots (bits per bit array)
     int64_t nbr_len = 0;   // entries of nbr[]
     int64_t stencil_slices = 0;
+    // Record staging plans of stencil slices (throughput path): the
+    // 32-record windows [p0 + o, p0 + o + 32) of a slice's offsets o merged
+    // into ranges of consecutive records.  splan_off[s] = start of slice s's
+    // plan in splan (-1: not staged); a plan is {ranges, records, then
+    // (first record, count) per range}.  spos[i] = staged position of lane
+    // 0's record of the stencil slot stored at nbr[i].
+    int64_t splan_slices = 0, splan_max = 0;
 
     pd::DBuf<int64_t> map;
     pd::DBuf<double4> x4, y, v, f, p;
@@ -163,6 +170,7 @@ struct pd_env {
     pd::DBuf<int32_t> tinfo, cnt, intact0, deformed;
     pd::DBuf<pd::SliceInfo> sinfo;
     pd::DBuf<int32_t> nbr;
+    pd::DBuf<int32_t> splan_off, splan, spos;
     pd::DBuf<uint32_t> words[2], words0, fam;
     // elasto-plastic state: td_norm2 per particle, edp per bond slot
     // (double-buffered by force evaluation, edp[ecur] current)
@@ -208,6 +216,7 @@ struct pd_env {
     bool fast_valid = false;
     void *fast = nullptr;
     int shape = 0;  // fixed kernel shape 10 * warps_per_slice + unroll, 0 = autotune
+    int staging = 0;  // record staging: 0 = none, 1 = staged shapes, 2 = the autotuner decides
 
     pd::Geo geo() const;
     void release_device();

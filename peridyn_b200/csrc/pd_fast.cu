@@ -136,6 +136,16 @@ struct StepArgs {
     typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
     const int32_t *tinfo, *cnt, *nbr;
     const SliceInfo *si;
+    // record staging plans (FP32C staged kernels): see pd_env
+    const int32_t *splan_off, *splan, *spos;
+    int32_t *serr;        // set when a staging copy did not land in time
+    int32_t stage_bytes;  // dynamic shared memory of the staged kernels
+    // Slice order of the one-slice-per-block kernels: with swz_g = G > 0,
+    // block b = r + G c walks slice r K + c (K = swz_k), so blocks that are
+    // dispatched G apart -- the ones sharing an SM -- walk consecutive
+    // slices and share their neighbour records in L1.  0: block b walks
+    // slice b.
+    int32_t swz_g, swz_k;
     uint32_t *words;
     const FBlock<R> *fb;
     const FPair<R> *fp;
@@ -154,17 +164,19 @@ struct StepArgs {
 __device__ __forceinline__ double &cmp(double4 &a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 
 // Work split of a 32-particle slice over WPS warps: warp w handles the
-// chunks c = w, w + WPS, ... of CS consecutive bonds of every particle of
-// the slice (CS = 32 -- one intact word -- for WPS <= 4, 16 for WPS = 8).
-// Partial sums are combined in a fixed order, so results do not depend on
-// scheduling.
+// contiguous slot range [w*per, (w+1)*per) of every particle of the slice,
+// per = ceil(len / WPS) with len the slice's slot count, so a family of 92
+// slots splits 23/23/23/23 over four warps.  Partial sums are combined in a
+// fixed order, so results do not depend on scheduling.
 template <int WPS>
 struct Split {
-    static constexpr int CS = WPS <= 4 ? 32 : 16;
     static constexpr int BT = WPS <= 4 ? 128 : 256;  // threads per block
     static constexpr int NW = BT / 32;                // warps per block
     static constexpr int SPB = NW / WPS;              // slices per block
     static constexpr int MINB = 1024 / BT;            // resident blocks per SM aimed for (<= 64 registers)
+    // Two slots in flight fit 56 registers: 9 blocks of 128 threads per SM,
+    // so 4 warps per slice cover 1332 slices in one wave instead of 1184.
+    static constexpr int MINB_U2 = 1152 / BT;
     static constexpr int MINB_THETA = 1280 / BT;      // the dilatation walk fits 48 registers
 };
 
@@ -174,15 +186,34 @@ struct Split {
 // will walk (one line per lane), so the walk's loads hit L2 instead of
 // waiting on HBM one chunk at a time.  Stencil slices read no indices.
 template <int WPS>
+__device__ __forceinline__ void warp_range(int32_t len, int w, int32_t &k0, int32_t &k1) {
+    const int32_t per = WPS == 1 ? len : (len + WPS - 1) / WPS;
+    k0 = min(w * per, len);
+    k1 = min(k0 + per, len);
+}
+
+template <int WPS>
 __device__ __forceinline__ void prefetch_slice_indices(const int32_t *nbr, const SliceInfo *si, int64_t s, int w,
                                                        int lane) {
-    constexpr int CS = Split<WPS>::CS;
     const SliceInfo d = si[s];
     if (d.mode != kExplicit) return;
-    for (int32_t c0 = w * CS; c0 < d.len; c0 += WPS * CS) {
-        const int32_t k = c0 + lane;
-        if (lane < CS && k < d.len) asm volatile("prefetch.global.L2 [%0];" ::"l"(nbr + d.nbr + 32 * (int64_t)k));
-    }
+    int32_t k0, k1;
+    warp_range<WPS>(d.len, w, k0, k1);
+    for (int32_t k = k0 + lane; k < k1; k += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(nbr + d.nbr + 32 * (int64_t)k));
+}
+
+// Bits of the slots [w0, w0 + kend) of one intact word (kend <= 32 - (w0 & 31)),
+// bit j <-> slot w0 + j.
+__device__ __forceinline__ uint32_t range_bits(uint32_t word, int32_t w0, int32_t kend) {
+    const uint32_t b = word >> (w0 & 31);
+    return kend >= 32 ? b : (b & ((1u << kend) - 1u));
+}
+
+template <int SPB, class A>
+__device__ __forceinline__ int64_t slice_of_block(const A &a) {
+    const int64_t b = blockIdx.x;
+    if (SPB != 1 || a.swz_g == 0) return b;
+    return (b % a.swz_g) * a.swz_k + b / a.swz_g;
 }
 
 // Neighbour of slot j of a chunk: explicit slices store one index per
@@ -275,32 +306,42 @@ struct Kin<float> {
     }
 };
 
-template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true>
-__device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
+// STG: the neighbour records come from the block's staged copy in shared
+// memory (stg, lane 0's record of slot k at sp[k]) instead of global memory.
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false>
+__device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
-                                          typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz) {
+                                          typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz,
+                                          const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr) {
     using V4 = typename Tr<R>::V4;
-    constexpr int CS = Split<WPS>::CS;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
     float2 fxy = make_float2(0.f, 0.f);  // FP32: packed (fx, fy)
-    for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
+    for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
+        // the part of [k0, k1) in one intact word
+        wend = min(k1, (w0 | 31) + 1);
         uint32_t *wptr = wp + 32 * (w0 >> 5);
-        const uint32_t word = *wptr;
-        const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+        const int32_t kend = wend - w0;
+        const uint32_t bits = range_bits(*wptr, w0, kend);
         if (!bits) continue;
         // Dense, branch-free walk over the chunk: intact bonds dominate, so
         // every slot is evaluated and its term selected by its bit; the
         // unrolled iterations' index and neighbour loads overlap.  Empty
         // stencil slots point at an in-range record and carry a 0 bit.
-        const int32_t kend = min(CS, n - w0);
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
+        const int32_t *spp = STG ? sp + w0 : nullptr;
         uint32_t okm = 0, bit = 1u;  // okm: slots within the critical stretch
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
+            if constexpr (STG) {
+                const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
+                xq = stg[2 * r];
+                uq = stg[2 * r + 1];
+            } else {
+                Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
+            }
             const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
             // stretch s = num / dl;  |Y|^2 = |xi|^2 + num
@@ -323,9 +364,9 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
             if constexpr (sizeof(R) == 4) k.accumulate(coef, fxy, fz);
             else k.accumulate(coef, fx, fy, fz);
         }
-        // bonds break rarely; two warps may own the halves of one word
+        // bonds break rarely; two warps may own parts of one word
         const uint32_t brk = bits & ~okm;
-        if (kBreak && brk) atomicAnd(wptr, ~(CS == 32 ? brk : (brk << (w0 & 31))));
+        if (kBreak && brk) atomicAnd(wptr, ~(brk << (w0 & 31)));
     }
     if constexpr (sizeof(R) == 4) {
         fx += fxy.x;
@@ -333,12 +374,14 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int w
     }
 }
 
-template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true>
+template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
                                             typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
-                                            R &fz) {
-    const int32_t n = a.cnt[p];
+                                            R &fz, const typename Tr<R>::V4 *stg = nullptr) {
     const SliceInfo d = a.si[p >> 5];
+    int32_t k0, k1;
+    warp_range<WPS>(d.len, w, k0, k1);
+    k1 = min(k1, a.cnt[p]);
     uint32_t *wp = a.words + d.word + (p & 31);
     R Ap = 0, Bp = 0;
     if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
@@ -346,19 +389,31 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         Ap = m.x;
         Bp = m.y;
     }
+    if constexpr (STG) {
+        if (stg) {  // a staged slice is a stencil slice
+            const int32_t *sp = a.spos + d.nbr;
+            if (B.nt > 1)
+                bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                                                                     up, Ap, Bp, fx, fy, fz, stg, sp);
+            else
+                bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                                                                      up, Ap, Bp, fx, fy, fz, stg, sp);
+            return;
+        }
+    }
     if (B.nt > 1) {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
                                                            fy, fz);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
+            bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
                                                             Ap, Bp, fx, fy, fz);
     } else {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, w, n, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
                                                             fy, fz);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
+            bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
                                                              up, Ap, Bp, fx, fy, fz);
     }
 }
@@ -464,22 +519,22 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 // MODE 3: integration only (forces already in f, e.g. after contacts).
 // MODE 4: integration only, last of the chunk.
 // MODE 5: force only into a scratch array, no bond breaking.
-// MODE 6: MODE 1 without bond breaking, on scratch outputs (autotuning).
 template <class R, int MODE>
 __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
 
 // One step of one slice (its WPS warps): bond gather, fixed-order
 // combination, integration.  Shared by k_step and the persistent kernel.
-template <class R, int WPS, int U, int MODE, bool NC>
-__device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], int *arrive) {
+template <class R, int WPS, int U, int MODE, bool NC, bool STG = false>
+__device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], int *arrive,
+                                          const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
     constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
     if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
-    constexpr bool kBreak = MODE != 5 && MODE != 6;
+    constexpr bool kBreak = MODE != 5;
     R f[3] = {0, 0, 0};
     if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
@@ -488,17 +543,18 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], 
             V4 xp, up;
             Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
             if (B.kind == PD_MAT_BOND_BASED)
-                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1], f[2]);
+                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0], f[1], f[2],
+                                                                           stg);
             else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1],
-                                                                              f[2]);
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0],
+                                                                                     f[1], f[2], stg);
         }
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 3>(sh, arrive, wid, lane, f)) return;
     const R fx = f[0], fy = f[1], fz = f[2];
     if (p >= a.N) return;
     if (ti < 0) {
-        if (MODE == 1 || MODE == 6) a.xn[2 * p + 1] = V4{};
+        if (MODE == 1) a.xn[2 * p + 1] = V4{};
         return;
     }
     const R ir = a.irho[p];
@@ -506,7 +562,8 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], 
 }
 
 template <class R, int WPS, int U, int MODE>
-__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1) k_step(StepArgs<R> a) {
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? Split<WPS>::MINB_U2 : Split<WPS>::MINB)
+    k_step(StepArgs<R> a) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
     __shared__ int arrive[SPB];
@@ -593,25 +650,32 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     store_u(a, p, u0, u1, u2);
 }
 
-template <class R, int WPS, int U, bool ST, bool NC = true>
-__device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, int32_t n, const int32_t *nb,
-                                        const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up) {
+template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false>
+__device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
+                                        const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up,
+                                        const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr) {
     using V4 = typename Tr<R>::V4;
-    constexpr int CS = Split<WPS>::CS;
     R acc = 0;
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
-    for (int32_t w0 = w * CS; w0 < n; w0 += WPS * CS) {
-        const uint32_t word = wp[32 * (w0 >> 5)];
-        const uint32_t bits = CS == 32 ? word : ((word >> (w0 & 31)) & 0xffffu);
+    for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
+        wend = min(k1, (w0 | 31) + 1);
+        const int32_t kend = wend - w0;
+        const uint32_t bits = range_bits(wp[32 * (w0 >> 5)], w0, kend);
         if (!bits) continue;
-        const int32_t kend = min(CS, n - w0);
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
+        const int32_t *spp = STG ? sp + w0 : nullptr;
         uint32_t bit = 1u;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
-            const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
+            if constexpr (STG) {
+                const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
+                xq = stg[2 * r];
+                uq = stg[2 * r + 1];
+            } else {
+                const int32_t q = slot_neighbour<ST>(np, j, p);
+                Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
+            }
             const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num;
             const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
@@ -624,13 +688,14 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int w, 
 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
-template <class R, int WPS, int U, bool NC>
-__device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32], int *arrive) {
+template <class R, int WPS, int U, bool NC, bool STG = false>
+__device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32], int *arrive,
+                                           const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
     constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    const int64_t p = ((int64_t)blockIdx.x * SPB + wid / WPS) * 32 + lane;
+    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
     if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
@@ -638,13 +703,18 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32],
     if (lps) {
         V4 xp, up;
         Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
-        const int32_t n = a.cnt[p];
         const SliceInfo d = a.si[p >> 5];
+        int32_t k0, k1;
+        warp_range<WPS>(d.len, w, k0, k1);
+        k1 = min(k1, a.cnt[p]);
         const uint32_t *wp = a.words + d.word + (p & 31);
-        if (d.mode == kStencil)
-            acc = theta_walk<R, WPS, U, true, NC>(a, p, w, n, a.nbr + d.nbr, wp, xp, up);
+        if (STG && stg)
+            acc = theta_walk<R, WPS, U, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
+                                                        a.spos + d.nbr);
+        else if (d.mode == kStencil)
+            acc = theta_walk<R, WPS, U, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up);
         else
-            acc = theta_walk<R, WPS, U, false, NC>(a, p, w, n, a.nbr + d.nbr + (p & 31), wp, xp, up);
+            acc = theta_walk<R, WPS, U, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, xp, up);
     }
     if (WPS > 1 && !last_arrival_sum<WPS, 1>(sh, arrive, wid, lane, &acc)) return;
     if (!lps) return;
@@ -663,6 +733,90 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     theta_body<R, WPS, U, true>(a, sh, arrive);
+}
+
+// ---------------------------------------------------------------------
+// Staged kernels (FP32C, 4 or 8 warps per slice, one slice per block).
+// The neighbour records of a stencil slice are a few ranges of
+// consecutive records (the 32-record windows of its offsets, merged); one
+// thread copies them into shared memory with bulk asynchronous copies that
+// complete on an mbarrier, and the walks then read shared memory instead
+// of waiting on L1/L2 one slot at a time.  Same arithmetic and order as the
+// global-load kernels, so the results are identical.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+constexpr uint32_t kStageSpins = 1u << 22;  // bounded wait on the staging copies
+
+// Returns the staged records of slice s in shared memory, or nullptr when
+// the slice has no plan (its walks load from global memory) or when the
+// copies did not complete within kStageSpins polls (error flag set; the
+// block falls back to global loads).  Called by every thread of the block.
+__device__ __forceinline__ const float4 *stage_slice(const StepArgs<float> &a, int64_t s, float4 *srec,
+                                                     uint64_t *bar) {
+    const int32_t so = a.splan_off[s];
+    if (so < 0) return nullptr;
+    const int32_t nr = a.splan[so], T = a.splan[so + 1];
+    const uint32_t b = smem_u32(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"((uint32_t)T * 32u)
+                     : "memory");
+        int32_t base = 0;
+        for (int32_t m = 0; m < nr; ++m) {
+            const int32_t r0 = a.splan[so + 2 + 2 * m], len = a.splan[so + 3 + 2 * m];
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(srec + 2 * base)),
+                "l"(a.xu + 2 * (int64_t)r0), "r"((uint32_t)len * 32u), "r"(b)
+                : "memory");
+            base += len;
+        }
+    }
+    for (uint32_t it = 0; it < kStageSpins; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], 0;\n selp.u32 %0, 1, 0, P;\n}"
+            : "=r"(done)
+            : "r"(b)
+            : "memory");
+        if (done) return srec;
+    }
+    if (threadIdx.x == 0) atomicExch(a.serr, 1);
+    return nullptr;
+}
+
+template <int WPS, int U, int MODE>
+__global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB) k_step_st(StepArgs<float> a) {
+    static_assert(Split<WPS>::SPB == 1, "one slice per block");
+    extern __shared__ __align__(128) float4 srec[];
+    __shared__ float sh[WPS][3][32];
+    __shared__ int arrive[1];
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) arrive[0] = 0;
+    const float4 *stg = stage_slice(a, blockIdx.x, srec, &bar);
+    __syncthreads();
+    step_body<float, WPS, U, MODE, true, true>(a, sh, arrive, stg);
+}
+
+template <int WPS, int U>
+__global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB_THETA) k_theta_st(StepArgs<float> a) {
+    static_assert(Split<WPS>::SPB == 1, "one slice per block");
+    extern __shared__ __align__(128) float4 srec[];
+    __shared__ float sh[WPS][1][32];
+    __shared__ int arrive[1];
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) arrive[0] = 0;
+    const float4 *stg = stage_slice(a, blockIdx.x, srec, &bar);
+    __syncthreads();
+    theta_body<float, WPS, U, true, true>(a, sh, arrive, stg);
 }
 
 // ---------------------------------------------------------------------
@@ -995,6 +1149,7 @@ struct Fast {
     DBuf<double> tune_d;
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     DBuf<GridBar> gbar;   // persistent-chunk barrier state
+    DBuf<int32_t> serr;   // staged kernels: a staging copy timed out
     bool persisted = false;
     int cur = 0;
     int wps = 0;          // warps per 32-particle slice (autotuned)
@@ -1032,17 +1187,78 @@ struct Unroll {
 template <class R, int MODE, int U>
 void launch_step_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
+    const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);  // one slice per block
     switch (wps) {
         case 1: k_step<R, 1, U, MODE><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
         case 2: k_step<R, 2, U, MODE><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_step<R, 4, U, MODE><<<(unsigned)slices, 128, 0, st>>>(a); break;
-        default: k_step<R, 8, U, MODE><<<(unsigned)slices, 256, 0, st>>>(a); break;
+        case 4: k_step<R, 4, U, MODE><<<g1, 128, 0, st>>>(a); break;
+        default: k_step<R, 8, U, MODE><<<g1, 256, 0, st>>>(a); break;
     }
     note_launch();
 }
 
+// Staged shapes (cfg >= 100, FP32C): one block of WPS warps per slice,
+// a.stage_bytes of dynamic shared memory.
+template <int MODE>
+void launch_step_st(cudaStream_t st, int cfg, StepArgs<float> a) {
+    a.swz_g = 0;  // block b stages and walks slice b
+    const unsigned slices = (unsigned)((a.N + 31) / 32);
+    const size_t sm = (size_t)a.stage_bytes;
+    switch (cfg % 100) {
+        case 42: k_step_st<4, 2, MODE><<<slices, 128, sm, st>>>(a); break;
+        case 44: k_step_st<4, 4, MODE><<<slices, 128, sm, st>>>(a); break;
+        case 82: k_step_st<8, 2, MODE><<<slices, 256, sm, st>>>(a); break;
+        default: k_step_st<8, 4, MODE><<<slices, 256, sm, st>>>(a); break;
+    }
+    note_launch();
+}
+
+inline void launch_theta_st(cudaStream_t st, int cfg, StepArgs<float> a) {
+    a.swz_g = 0;  // block b stages and walks slice b
+    const unsigned slices = (unsigned)((a.N + 31) / 32);
+    const size_t sm = (size_t)a.stage_bytes;
+    switch (cfg % 100) {
+        case 42: k_theta_st<4, 2><<<slices, 128, sm, st>>>(a); break;
+        case 44: k_theta_st<4, 4><<<slices, 128, sm, st>>>(a); break;
+        case 82: k_theta_st<8, 2><<<slices, 256, sm, st>>>(a); break;
+        default: k_theta_st<8, 4><<<slices, 256, sm, st>>>(a); break;
+    }
+    note_launch();
+}
+
+// The staged kernels may use up to kStageMaxRecords records of dynamic
+// shared memory; raise their limit once per process.
+inline cudaError_t staged_kernel_attrs() {
+    static cudaError_t status = [] {
+        const int bytes = (int)(kStageMaxRecords * 32);
+        cudaError_t e = cudaSuccess;
+        auto set = [&](const void *k) {
+            const cudaError_t r = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (r != cudaSuccess && e == cudaSuccess) e = r;
+        };
+#define PD_STAGED_ATTRS(W, U)                                                                               \
+    set((const void *)k_step_st<W, U, 0>);                                                                  \
+    set((const void *)k_step_st<W, U, 1>);                                                                  \
+    set((const void *)k_step_st<W, U, 2>);                                                                  \
+    set((const void *)k_theta_st<W, U>);
+        PD_STAGED_ATTRS(4, 2)
+        PD_STAGED_ATTRS(4, 4)
+        PD_STAGED_ATTRS(8, 2)
+        PD_STAGED_ATTRS(8, 4)
+#undef PD_STAGED_ATTRS
+        return e;
+    }();
+    return status;
+}
+
 template <class R, int MODE>
 void launch_step(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    if constexpr (sizeof(R) == 4) {
+        if (cfg >= 100) {
+            launch_step_st<MODE>(st, cfg, a);
+            return;
+        }
+    }
     if (cfg % 10 == Unroll<R>::LO) launch_step_u<R, MODE, Unroll<R>::LO>(st, cfg / 10, a);
     else launch_step_u<R, MODE, Unroll<R>::HI>(st, cfg / 10, a);
 }
@@ -1050,17 +1266,24 @@ void launch_step(cudaStream_t st, int cfg, const StepArgs<R> &a) {
 template <class R, int U>
 void launch_theta_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
+    const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);  // one slice per block
     switch (wps) {
         case 1: k_theta<R, 1, U><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
         case 2: k_theta<R, 2, U><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_theta<R, 4, U><<<(unsigned)slices, 128, 0, st>>>(a); break;
-        default: k_theta<R, 8, U><<<(unsigned)slices, 256, 0, st>>>(a); break;
+        case 4: k_theta<R, 4, U><<<g1, 128, 0, st>>>(a); break;
+        default: k_theta<R, 8, U><<<g1, 256, 0, st>>>(a); break;
     }
     note_launch();
 }
 
 template <class R>
 void launch_theta(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    if constexpr (sizeof(R) == 4) {
+        if (cfg >= 100) {
+            launch_theta_st(st, cfg, a);
+            return;
+        }
+    }
     if (cfg % 10 == Unroll<R>::LO) launch_theta_u<R, Unroll<R>::LO>(st, cfg / 10, a);
     else launch_theta_u<R, Unroll<R>::HI>(st, cfg / 10, a);
 }
@@ -1094,6 +1317,22 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.cnt = env->cnt.p;
     a.nbr = env->nbr.p;
     a.si = env->sinfo.p;
+    a.splan_off = env->splan_off.p;
+    a.splan = env->splan.p;
+    a.spos = env->spos.p;
+    a.serr = F.serr.p;
+    a.stage_bytes = (int32_t)(env->splan_max * 32);
+    const char *sw = std::getenv("PD_SWIZZLE");
+    if (!(sw && std::strcmp(sw, "0") == 0)) {  // on unless PD_SWIZZLE=0
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t S = (env->N + 31) / 32;
+        if (sms > 0 && S > sms) {
+            a.swz_g = sms;
+            a.swz_k = (int32_t)((S + sms - 1) / sms);
+        }
+    }
     a.words = env->words[env->cur].p;
     a.fb = F.fb.p;
     a.fp = F.fp.p;
@@ -1175,6 +1414,10 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         }
         PD_TRY(F.fb.alloc(fb.size()));
         PD_TRY(F.fp.alloc(fp.size()));
+        if (!F.serr.p) {
+            PD_TRY(F.serr.alloc(1));
+            CK(cudaMemsetAsync(F.serr.p, 0, sizeof(int32_t), env->st));
+        }
         CK(cudaMemcpyAsync(F.fb.p, fb.data(), fb.size() * sizeof(FBlock<R>), cudaMemcpyHostToDevice, env->st));
         CK(cudaMemcpyAsync(F.fp.p, fp.data(), fp.size() * sizeof(FPair<R>), cudaMemcpyHostToDevice, env->st));
         std::vector<uint8_t> bits(N, 0);
@@ -1328,12 +1571,16 @@ std::map<std::tuple<int64_t, int64_t, int, bool>, int> g_tune_cache;
 template <class R>
 pd_status autotune(pd_env *env, Fast<R> &F) {
     if (F.wps) return PD_OK;
-    if (env->shape) {  // pd_env_set_kernel_shape
-        F.wps = env->shape;
+    // staged shapes: FP32C, 4 or 8 warps per slice, when some slice has a plan
+    const bool can_stage = sizeof(R) == 4 && env->splan_slices > 0;
+    if (can_stage) CK(staged_kernel_attrs());
+    auto staged_ok = [&](int w) { return can_stage && (w == 4 || w == 8); };
+    if (env->shape) {  // pd_env_set_kernel_shape (+ pd_env_set_record_staging)
+        F.wps = env->shape + (env->staging == 1 && staged_ok(env->shape / 10) ? 100 : 0);
         return PD_OK;
     }
     const bool lps = any_lps(env);
-    const auto key = std::make_tuple(env->N, env->nnz, env->precision, lps);
+    const auto key = std::make_tuple(env->N, env->nnz, env->precision * 4 + env->staging + 1, lps);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -1342,17 +1589,18 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
             return PD_OK;
         }
     }
-    if (const char *fixed = std::getenv("PD_KERNEL_SHAPE")) {  // "WPS,U" overrides the tuner
-        int w = 0, u = 0;
-        if (std::sscanf(fixed, "%d,%d", &w, &u) == 2 && (w == 1 || w == 2 || w == 4 || w == 8) &&
-            (u == Unroll<R>::LO || u == Unroll<R>::HI)) {
-            F.wps = 10 * w + u;
+    if (const char *fixed = std::getenv("PD_KERNEL_SHAPE")) {  // "WPS,U[,staged]" overrides the tuner
+        int w = 0, u = 0, sg = 0;
+        const int n = std::sscanf(fixed, "%d,%d,%d", &w, &u, &sg);
+        if (n >= 2 && (w == 1 || w == 2 || w == 4 || w == 8) && (u == Unroll<R>::LO || u == Unroll<R>::HI)) {
+            F.wps = 10 * w + u + (n == 3 && sg == 1 && staged_ok(w) ? 100 : 0);
             return PD_OK;
         }
     }
-    // The timed kernel is the full step (force + integration, MODE 6 = MODE 1
-    // without bond breaking) writing every output into scratch arrays, so
-    // the environment's state is left untouched.
+    // The timed kernels are the full step (dilatation; force, integration,
+    // BCs and bond breaking, MODE 1) writing every output -- velocities,
+    // records, bond words, BC positions -- into scratch copies, so the
+    // environment's state is left untouched.
     const int64_t N = env->N;
     PD_TRY(F.tune.alloc(5 * N));
     PD_TRY(F.tune_d.alloc(3 * N));
@@ -1369,8 +1617,24 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     a.ax = F.tune_d.p;
     a.ay = F.tune_d.p + N;
     a.az = F.tune_d.p + 2 * N;
-    a.nbc = 0;
     a.deformed = F.ones.p;
+    const int64_t nwords = std::max<int64_t>(env->nnz / 32, 1);
+    DBuf<uint32_t> twords;
+    PD_TRY(twords.alloc(nwords));
+    CK(cudaMemcpyAsync(twords.p, a.words, nwords * 4, cudaMemcpyDeviceToDevice, env->st));
+    a.words = twords.p;
+    int64_t nlast = 0;
+    for (int k = 0; k < a.nbc; ++k)
+        if (a.bc[k].last) nlast += a.bc[k].n;
+    DBuf<double4> tlast;
+    PD_TRY(tlast.alloc(std::max<int64_t>(nlast, 1)));
+    for (int k = 0, off = 0; k < a.nbc; ++k) {
+        if (!a.bc[k].last) continue;
+        CK(cudaMemcpyAsync(tlast.p + off, a.bc[k].last, a.bc[k].n * sizeof(double4), cudaMemcpyDeviceToDevice,
+                           env->st));
+        a.bc[k].last = tlast.p + off;
+        off += (int)a.bc[k].n;
+    }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1378,25 +1642,48 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     int best_w = 40 + Unroll<R>::LO;
     std::vector<int> shapes;
     for (int wps : {1, 2, 4, 8})
-        for (int u : {Unroll<R>::LO, Unroll<R>::HI}) shapes.push_back(10 * wps + u);
-    // two sweeps over the shapes, 8 timed steps each, best of the two per
-    // shape: short kernels are noisy one launch at a time
-    std::vector<float> t(shapes.size(), 1e30f);
-    for (int sweep = 0; sweep < 2; ++sweep)
-        for (size_t i = 0; i < shapes.size(); ++i) {
-            const int w = shapes[i];
-            if (lps) launch_theta(env->st, w, a);
-            launch_step<R, 6>(env->st, w, a);
-            cudaEventRecord(e0, env->st);
-            for (int r = 0; r < 8; ++r) {
-                if (lps) launch_theta(env->st, w, a);
-                launch_step<R, 6>(env->st, w, a);
+        for (int u : {Unroll<R>::LO, Unroll<R>::HI}) {
+            if (env->staging != 1 || !staged_ok(wps)) shapes.push_back(10 * wps + u);
+            if (env->staging >= 1 && staged_ok(wps)) shapes.push_back(100 + 10 * wps + u);
+        }
+    // Each shape runs as the stepping loop does: a captured graph of
+    // kTuneSteps steps, replayed once to warm up and then timed in three
+    // sweeps over the shapes, best of the three per shape.
+    constexpr int kTuneSteps = 12;
+    std::vector<cudaGraphExec_t> ex(shapes.size(), nullptr);
+    auto release = [&] {
+        for (auto &g : ex)
+            if (g) cudaGraphExecDestroy(g);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    };
+    for (size_t i = 0; i < shapes.size(); ++i) {
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(env->st, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            for (int r = 0; r < kTuneSteps; ++r) {
+                if (lps) launch_theta(env->st, shapes[i], a);
+                launch_step<R, 1>(env->st, shapes[i], a);
             }
+            err = cudaStreamEndCapture(env->st, &graph);
+        }
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&ex[i], graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (err == cudaSuccess) err = cudaGraphLaunch(ex[i], env->st);
+        if (err != cudaSuccess) {
+            release();
+            return cuda_fail(err, "autotune", __FILE__, __LINE__);
+        }
+    }
+    std::vector<float> t(shapes.size(), 1e30f);
+    for (int sweep = 0; sweep < 3; ++sweep)
+        for (size_t i = 0; i < shapes.size(); ++i) {
+            cudaEventRecord(e0, env->st);
+            cudaGraphLaunch(ex[i], env->st);
             cudaEventRecord(e1, env->st);
             cudaError_t err = cudaEventSynchronize(e1);
             if (err != cudaSuccess) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
+                release();
                 return cuda_fail(err, "autotune", __FILE__, __LINE__);
             }
             float ms = 0.f;
@@ -1408,8 +1695,14 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
             best = t[i];
             best_w = shapes[i];
         }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (std::getenv("PD_TUNE_LOG")) {
+        std::fprintf(stderr, "pd autotune N=%lld:", (long long)env->N);
+        for (size_t i = 0; i < shapes.size(); ++i)
+            std::fprintf(stderr, " %s%d,%d=%.2fus", shapes[i] >= 100 ? "s" : "", shapes[i] % 100 / 10, shapes[i] % 10,
+                         1e3f * t[i] / kTuneSteps);
+        std::fprintf(stderr, " -> %d\n", best_w);
+    }
+    release();
     CK(cudaGetLastError());
     F.tune.reset();
     F.tune_d.reset();
@@ -1577,6 +1870,7 @@ pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
         CK(cudaMemsetAsync(F.gbar.p, 0, sizeof(GridBar), env->st));
     }
     StepArgs<R> a = args(env, F);
+    a.swz_g = 0;  // the cooperative grid covers the slices in order
     a.dir_vel = a.dir_pos = dir_bits(env);
     a.ts = env->ts + 1;
     typename Tr<R>::V4 *b0 = F.xu[F.cur].p, *b1 = F.xu[1 - F.cur].p;
@@ -1596,7 +1890,7 @@ pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
 template <class R, bool LPS>
 pd_status persist_any(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
     constexpr int LO = Unroll<R>::LO, HI = Unroll<R>::HI;
-    switch (F.wps) {
+    switch (F.wps % 100) {  // the persistent kernel reads global memory (no staging)
         case 10 + LO: return persist_try<R, 1, LO, LPS>(env, F, nsteps, done);
         case 10 + HI: return persist_try<R, 1, HI, LPS>(env, F, nsteps, done);
         case 20 + LO: return persist_try<R, 2, LO, LPS>(env, F, nsteps, done);
@@ -1841,6 +2135,20 @@ pd_status persist_check(pd_env *env) {
     return h->prec == PD_PREC_FP32C ? chk(h->f32) : chk(h->f64);
 }
 
+// A staged kernel whose staging copies timed out fell back to global loads
+// (results unaffected) and raised the flag: report it.
+pd_status stage_check(pd_env *env) {
+    FastHolder *h = holder(env);
+    if (h->prec != PD_PREC_FP32C || h->f32.wps < 100 || !h->f32.serr.p) return PD_OK;
+    int32_t e = 0;
+    CK(cudaMemcpy(&e, h->f32.serr.p, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(h->f32.serr.p, 0, sizeof(e)));
+        return fail(PD_ERR_TIMEOUT, "staged step kernel: a record staging copy did not complete in time");
+    }
+    return PD_OK;
+}
+
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps) {
     if (nsteps == 0) return PD_OK;
     PD_TRY(ensure_fast(env));
@@ -1850,6 +2158,7 @@ pd_status fast_vv_steps(pd_env *env, int64_t nsteps) {
     h->dirty = true;
     PD_TRY(refresh_deformed_flags(env));
     CK(cudaStreamSynchronize(env->st));
+    PD_TRY(stage_check(env));
     return persist_check(env);
 }
 
@@ -1886,7 +2195,28 @@ extern "C" pd_status pd_env_kernel_shape(pd_env *env, int32_t *warps_per_slice, 
     if (!env || !warps_per_slice || !unroll) return pd::fail(PD_ERR_ARG, "NULL argument");
     int cfg = 0;
     if (env->fast) cfg = env->precision == PD_PREC_FP32C ? pd::holder(env)->f32.wps : pd::holder(env)->f64.wps;
-    *warps_per_slice = cfg / 10;
+    *warps_per_slice = cfg % 100 / 10;
     *unroll = cfg % 10;
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_set_record_staging(pd_env *env, int32_t mode) {
+    if (!env) return pd::fail(PD_ERR_ARG, "environment handle is NULL");
+    if (mode < 0 || mode > 2) return pd::fail(PD_ERR_ARG, "record staging mode %d: use 0, 1 or 2", mode);
+    env->staging = mode;
+    if (env->fast) {
+        pd::holder(env)->f32.wps = 0;
+        pd::holder(env)->f64.wps = 0;
+    }
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_record_staging(pd_env *env, int32_t *staged, int64_t *slices, int64_t *max_records) {
+    if (!env) return pd::fail(PD_ERR_ARG, "environment handle is NULL");
+    int cfg = 0;
+    if (env->fast && env->precision == PD_PREC_FP32C) cfg = pd::holder(env)->f32.wps;
+    if (staged) *staged = cfg >= 100;
+    if (slices) *slices = env->splan_slices;
+    if (max_records) *max_records = env->splan_max;
     return PD_OK;
 }

@@ -31,6 +31,9 @@
 namespace pd {
 
 constexpr int kSlice = 32;
+// Largest record staging plan of a slice (FP32C records of 32 bytes: 64 KB
+// of shared memory per block).
+constexpr int64_t kStageMaxRecords = 2048;
 
 // Counts every kernel launch the library issues (pd_kernel_launches);
 // graph replays add their kernel nodes.

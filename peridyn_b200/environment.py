@@ -162,6 +162,18 @@ class GeneralEnvironment:
         """Fix the throughput-mode kernel shape; (0, 0) = autotune."""
         _abi.check(_abi.lib().pd_env_set_kernel_shape(self._h, int(warps_per_slice), int(unroll)))
 
+    def set_record_staging(self, mode=0):
+        """FP32C record staging into shared memory: 0 = never (default),
+        1 = staged shapes, 2 = the autotuner decides."""
+        _abi.check(_abi.lib().pd_env_set_record_staging(self._h, int(mode)))
+
+    def record_staging(self):
+        """{'staged': running shape stages, 'slices': slices with a plan,
+        'max_records': largest plan}."""
+        st, sl, mx = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        _abi.check(_abi.lib().pd_env_record_staging(self._h, ctypes.byref(st), ctypes.byref(sl), ctypes.byref(mx)))
+        return {"staged": bool(st.value), "slices": int(sl.value), "max_records": int(mx.value)}
+
     # ------------------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None):

@@ -259,3 +259,89 @@ def test_persistent_chunks_match_graph_replays(precision, monkeypatch):
 
     for a, b in zip(run(False), run(True)):
         assert np.array_equal(a, b)
+
+
+def _two_type_block():
+    x, vol = lattice.cuboid(16, 9, 8, 1.0e-3, jitter=2e-5, seed=9)
+    t = np.where(x[0] < x[0].mean(), 1, 2).astype(np.int64)
+    gen = pb.GeneralMaterial(x.copy(order="F"), lattice.gaussian_pulse(x, 40.0, 2e-3), x, vol, t, 3.015e-3,
+                             max_neigh=200)
+    spc = pb.OrdinaryStateBasedSpecific([20e9, 25e9, 30e9], [9e9, 10e9, 12e9], [0.004, 0.003, 0.005],
+                                        [2000.0, 2500.0])
+    return {"materials": [pb.PeridynamicsMaterial(gen, spc)], "contacts": [], "bcs": [], "dt": 2e-8}
+
+
+@pytest.mark.parametrize("shape", [(4, 2), (4, 4), (8, 2), (8, 4)])
+@pytest.mark.parametrize("builder", [
+    lambda: configs.lps_bar(nx=30, ny=8, nz=8),
+    lambda: configs.pmb_cube(n=14, peak=60.0),
+    _two_type_block,
+    lambda: configs.batched_cubes(nspec=5, edge_lo=6, edge_hi=11),
+])
+def test_record_staging_is_bit_identical(builder, shape):
+    """The staged kernels (neighbour records copied to shared memory by bulk
+    asynchronous copies) do the same arithmetic in the same order as the
+    global-load kernels: identical states and broken-bond sets."""
+    w = builder()
+
+    def run(staging):
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision="fp32c")
+        env.set_kernel_shape(*shape)
+        env.set_record_staging(staging)
+        if w["bcs"]:
+            pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=120)
+        st = env.record_staging()
+        out = env.get_state(), [env._family(b)[1] for b in range(len(w["materials"]))]
+        env.close()
+        return out, st
+
+    (s1, i1), st1 = run(0)
+    (s2, i2), st2 = run(1)
+    assert not st1["staged"]
+    assert st2["staged"] and st2["slices"] > 0 and 0 < st2["max_records"] <= 2048
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    for a, b in zip(i1, i2):
+        assert np.array_equal(a, b)
+    assert sum(int((~i).sum()) for i in i1) >= 0
+
+
+def test_record_staging_autotuned_bar_matches_oracle(oracle):
+    w = configs.lps_bar(nx=40, ny=10, nz=10)
+    env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision="fp32c")
+    env.set_record_staging(2)
+    ora = oracle.OracleEnv(w["materials"], w["contacts"], w["bcs"], w["dt"])
+    ora.apply_bc_at0()
+    pb.apply_bc_at0(env, 0)
+    for _ in range(200):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=200)
+    eu, ev, mism = _errors(env, ora)
+    assert eu <= TOL["fp32c"], eu
+    assert env.record_staging()["slices"] > 0
+    env.close()
+
+
+@pytest.mark.parametrize("shape", [(4, 2), (8, 4)])
+def test_slice_swizzle_is_bit_identical(shape, monkeypatch):
+    # one-slice-per-block kernels walk slices in SM-grouped order by
+    # default; the order of blocks changes no arithmetic
+    w = configs.lps_bar(nx=60, ny=10, nz=10)
+
+    def run():
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision="fp32c")
+        env.set_kernel_shape(*shape)
+        pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=100)
+        out = env.get_state(), env._family(0)[1]
+        env.close()
+        return out
+
+    monkeypatch.setenv("PD_SWIZZLE", "0")
+    s1, i1 = run()
+    monkeypatch.delenv("PD_SWIZZLE")
+    s2, i2 = run()
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    assert np.array_equal(i1, i2)
