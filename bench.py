@@ -64,8 +64,10 @@ def build_workload(name, args):
 # int32 per (slot, particle) in explicit slices, one per slot in stencil
 # slices) and per particle the state the kernel streams (listed per
 # precision below).
-def bond_bytes(layout):
-    return layout["slots"] / 8.0 + 4.0 * layout["index_entries"]
+def bond_bytes(layout, ep=False):
+    # elasto-plastic: per slot the plastic strain read and written (8 + 8)
+    # plus, in the throughput modes, the reverse slot's index and strain (4 + 8)
+    return layout["slots"] / 8.0 + 4.0 * layout["index_entries"] + (28.0 * layout["slots"] if ep else 0.0)
 
 
 def particle_bytes(precision, lps):
@@ -396,6 +398,7 @@ def main():
     _abi.check(L.pd_env_stream(env._h, ctypes.byref(stream_ptr)))
     stream = torch.cuda.ExternalStream(stream_ptr.value, device=torch.device("cuda", local))
     lps = any(m.specific.kind in (1, 3) for m in work["materials"])
+    ep = any(m.specific.kind == 3 for m in work["materials"])
     y0, v0, _, _ = env.get_state()
     # pinned host copies for the end-to-end arm
     hy = torch.from_numpy(np.ascontiguousarray(y0.T)).pin_memory()
@@ -495,7 +498,7 @@ def main():
     n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
     layout = env.layout()
     shape = env.kernel_shape()
-    bytes_launch = bond_bytes(layout) + n_int * particle_bytes(args.precision, lps)
+    bytes_launch = bond_bytes(layout, ep) + n_int * particle_bytes(args.precision, lps)
     avg_ms = prof_ms.value / max(1, prof_n.value)
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
     peaks = {}

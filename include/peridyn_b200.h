@@ -63,7 +63,8 @@ enum {
 
 /* Material kinds: src/materials/bond_based.jl, ordinary_state_based.jl,
  * skip_specific.jl, elasto_plastic.jl (ElastoPlasticSolidSpecific, Von
- * Mises; serial FP64 mode only). */
+ * Mises; all three precisions; the device-pointer entry points take the
+ * other kinds only). */
 enum { PD_MAT_BOND_BASED = 0, PD_MAT_ORDINARY_STATE_BASED = 1, PD_MAT_SKIP = 2, PD_MAT_ELASTO_PLASTIC = 3 };
 
 /* Arithmetic modes.

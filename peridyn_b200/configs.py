@@ -160,7 +160,7 @@ def serving_jobs(njobs, seed=5, rate=50.0, n_lo=5.0e3, n_hi=5.0e5, steps_lo=500,
 
 def ep_bar(nx=100, ny=20, nz=20, yield_stress=2e6, steps=2000):
     """The lps_bar tensile bar (Fix + Move BCs) as an elasto-plastic (Von
-    Mises) solid with the given yield stress; serial FP64 mode."""
+    Mises) solid with the given yield stress."""
     from .materials import ElastoPlasticSolidSpecific
 
     w = lps_bar(nx=nx, ny=ny, nz=nz, steps=steps)

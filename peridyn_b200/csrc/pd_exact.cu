@@ -222,20 +222,9 @@ __device__ __forceinline__ bool bond_term(const Geo &g, const DevBlock &B, int t
 // the bond term depends on which end visits the bond: particle i's visit
 // to bond slot k uses td_norm2[i] and edp[k, i] and updates edp[k, i].
 // ---------------------------------------------------------------------
-// Slot of neighbour p in q's family (slots hold descending indices).
+// Slot of neighbour p in q's family.
 __device__ __forceinline__ int32_t find_slot(const Geo &g, int64_t q, int32_t p) {
-    const SliceInfo s = g.si[q >> 5];
-    const bool st = s.mode == kStencil;
-    const int32_t *nb = g.nbr + s.nbr + (st ? 0 : (q & 31));
-    const int32_t target = st ? (int32_t)(p - q) : p;
-    int32_t lo = 0, hi = g.cnt[q];
-    while (lo < hi) {
-        const int32_t mid = (lo + hi) >> 1;
-        const int32_t v = st ? nb[mid] : nb[32 * mid];
-        if (v > target) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
+    return slot_of(g.si, g.nbr, g.cnt, q, p);
 }
 
 // force_density_t_ij (elasto_plastic.jl:215-242) for the visit of i to j;

@@ -102,7 +102,8 @@ struct FBlock {
 };
 template <class R>
 struct FPair {
-    R cs, k35, g15, pad;
+    R cs, k35, g15;
+    R psi;  // elasto-plastic: sqrt(2 psi), so that C = psi / sqrt(td_norm2)
 };
 
 constexpr int kMaxFastBC = 8;
@@ -139,6 +140,14 @@ struct StepArgs {
     // record staging plans (FP32C staged kernels): see pd_env
     const int32_t *splan_off, *splan, *spos;
     int32_t *serr;        // set when a staging copy did not land in time
+    // elasto-plastic blocks: plastic strain per bond slot (read edp_in,
+    // written edp_out), 1/sqrt(td_norm2) per particle, and per slot the
+    // slot of the reverse bond in the neighbour's family
+    const double *edp_in;
+    double *edp_out;
+    R *rtd;
+    const int32_t *partner;
+    int32_t ep;  // the environment has elasto-plastic blocks
     int32_t stage_bytes;  // dynamic shared memory of the staged kernels
     // Slice order of the one-slice-per-block kernels: with swz_g = G > 0,
     // block b = r + G c walks slice r K + c (K = swz_k), so blocks that are
@@ -312,7 +321,8 @@ template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, b
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
                                           typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz,
-                                          const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr) {
+                                          const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
+                                          R rtdp = R(0)) {
     using V4 = typename Tr<R>::V4;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -323,13 +333,21 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
         uint32_t *wptr = wp + 32 * (w0 >> 5);
         const int32_t kend = wend - w0;
         const uint32_t bits = range_bits(*wptr, w0, kend);
-        if (!bits) continue;
+        if (!bits) {
+            if (KIND == PD_MAT_ELASTO_PLASTIC) {  // carry the strain of broken bonds
+                const int64_t e0 = ((int64_t)(wptr - a.words) << 5) + (w0 & 31);
+                for (int32_t j = 0; j < kend; ++j) a.edp_out[e0 + j] = a.edp_in[e0 + j];
+            }
+            continue;
+        }
         // Dense, branch-free walk over the chunk: intact bonds dominate, so
         // every slot is evaluated and its term selected by its bit; the
         // unrolled iterations' index and neighbour loads overlap.  Empty
         // stencil slots point at an in-range record and carry a 0 bit.
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         const int32_t *spp = STG ? sp + w0 : nullptr;
+        // elasto-plastic: per-slot state index of the chunk's first slot
+        const int64_t ebase = KIND == PD_MAT_ELASTO_PLASTIC ? ((int64_t)(wptr - a.words) << 5) + (w0 & 31) : 0;
         uint32_t okm = 0, bit = 1u;  // okm: slots within the critical stretch
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
@@ -356,9 +374,31 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
             R tn;
             if (KIND == PD_MAT_BOND_BASED) {
                 tn = num;
-            } else {
+            } else if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
                 typename Tr<R>::V2 mq = a.mab[q];
                 tn = pp.k35 * (Ap + mq.x) * dl + pp.g15 * num * (Bp + mq.y);
+            } else {
+                // force_density_t_ij (elasto_plastic.jl:215-242) of both
+                // visits: p's (its slot e, its td_norm2) and q's (the
+                // reverse slot, q's td_norm2); f_p gets (t_pq + t_qp) / 2.
+                // With A = theta/m, B = 1/m: theta_ij = (A_p + A_q) /
+                // (B_p + B_q), tn = 3K (A_p + A_q), td_trial = 15G w
+                // (B_p + B_q) (ed - edp).
+                typename Tr<R>::V2 mq = a.mab[q];
+                const R As = Ap + mq.x, Bs = Bp + mq.y;
+                const R ext = num * Tr<R>::rcp(ly + lx);
+                const R ed = ext - As * Tr<R>::rcp(Bs) * lx * R(1.0 / 3.0);
+                const R gB = pp.g15 * Tr<R>::rcp(lx) * Bs;
+                const int64_t e = ebase + j;
+                const int32_t pe = a.partner[e];
+                const double eo = a.edp_in[e];
+                const R ede_p = ed - (R)eo, ede_q = ed - (R)a.edp_in[pe];
+                const R Cp = pp.psi * rtdp, Cq = pp.psi * a.rtd[q];
+                const bool pl = Cp <= R(1);  // p's visit yields
+                const R td_p = gB * ede_p * (pl ? Cp : R(1));
+                const R td_q = gB * ede_q * (Cq <= R(1) ? Cq : R(1));
+                tn = (pp.k35 * As + R(0.5) * (td_p + td_q)) * dl;
+                a.edp_out[e] = (live && ok && pl) ? (double)((R)eo + ede_p * (R(1) - Cp)) : eo;
             }
             const R coef = (live && ok) ? tn * xq.w * Tr<R>::rcp(dl * ly) : R(0);
             if constexpr (sizeof(R) == 4) k.accumulate(coef, fxy, fz);
@@ -383,12 +423,13 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
     warp_range<WPS>(d.len, w, k0, k1);
     k1 = min(k1, a.cnt[p]);
     uint32_t *wp = a.words + d.word + (p & 31);
-    R Ap = 0, Bp = 0;
-    if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
+    R Ap = 0, Bp = 0, rtdp = 0;
+    if (KIND != PD_MAT_BOND_BASED) {
         typename Tr<R>::V2 m = a.mab[p];
         Ap = m.x;
         Bp = m.y;
     }
+    if (KIND == PD_MAT_ELASTO_PLASTIC) rtdp = a.rtd[p];
     if constexpr (STG) {
         if (stg) {  // a staged slice is a stencil slice
             const int32_t *sp = a.spos + d.nbr;
@@ -404,17 +445,17 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
     if (B.nt > 1) {
         if (d.mode == kStencil)
             bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
-                                                           fy, fz);
+                                                           fy, fz, nullptr, nullptr, rtdp);
         else
             bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
-                                                            Ap, Bp, fx, fy, fz);
+                                                            Ap, Bp, fx, fy, fz, nullptr, nullptr, rtdp);
     } else {
         if (d.mode == kStencil)
             bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
-                                                            fy, fz);
+                                                            fy, fz, nullptr, nullptr, rtdp);
         else
             bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
-                                                             up, Ap, Bp, fx, fy, fz);
+                                                             up, Ap, Bp, fx, fy, fz, nullptr, nullptr, rtdp);
     }
 }
 
@@ -524,7 +565,7 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
 
 // One step of one slice (its WPS warps): bond gather, fixed-order
 // combination, integration.  Shared by k_step and the persistent kernel.
-template <class R, int WPS, int U, int MODE, bool NC, bool STG = false>
+template <class R, int WPS, int U, int MODE, bool NC, bool STG = false, bool EPK = false>
 __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], int *arrive,
                                           const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
@@ -542,10 +583,14 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], 
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             V4 xp, up;
             Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
-            if (B.kind == PD_MAT_BOND_BASED)
+            if (B.kind == PD_MAT_BOND_BASED) {
                 bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0], f[1], f[2],
                                                                            stg);
-            else
+            } else if (EPK && B.kind == PD_MAT_ELASTO_PLASTIC) {
+                if constexpr (EPK)
+                    bond_gather<R, PD_MAT_ELASTO_PLASTIC, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1],
+                                                                              f[2]);
+            } else
                 bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0],
                                                                                      f[1], f[2], stg);
         }
@@ -561,7 +606,7 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], 
     integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
 }
 
-template <class R, int WPS, int U, int MODE>
+template <class R, int WPS, int U, int MODE, bool EPK = false>
 __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? Split<WPS>::MINB_U2 : Split<WPS>::MINB)
     k_step(StepArgs<R> a) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
@@ -571,7 +616,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? 
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    step_body<R, WPS, U, MODE, true>(a, sh, arrive);
+    step_body<R, WPS, U, MODE, true, false, EPK>(a, sh, arrive);
 }
 
 // MODE 3/4: integration of forces already in f (after contact forces).
@@ -698,7 +743,8 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32],
     const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
     if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
-    const bool lps = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED;
+    const bool lps = ti >= 0 && (a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED ||
+                                 a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC);
     R acc = 0;
     if (lps) {
         V4 xp, up;
@@ -733,6 +779,135 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     theta_body<R, WPS, U, true>(a, sh, arrive);
+}
+
+// ---------------------------------------------------------------------
+// Elasto-plastic td_norm2 pass (elasto_plastic.jl:274-288 through
+// loop_over_neighs!, peri.jl:411-445): td_norm2_p = sum over intact bonds
+// within the critical stretch of td_trial^2 V_q, with p's own plastic
+// strain; bonds at or beyond the critical stretch break here (the force
+// walk that follows finds none).  The sum runs in FP64 in both precisions
+// (td_trial^2 exceeds the FP32 range in SI units); stored as
+// 1/sqrt(td_norm2) in the working precision.
+// ---------------------------------------------------------------------
+template <class R, int U, bool ST, bool MULTI>
+__device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1,
+                                          const int32_t *nb, uint32_t *wp, const FBlock<R> &B, int tp,
+                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp) {
+    using V4 = typename Tr<R>::V4;
+    FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
+    const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
+    double acc = 0.0;
+    for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
+        wend = min(k1, (w0 | 31) + 1);
+        uint32_t *wptr = wp + 32 * (w0 >> 5);
+        const int32_t kend = wend - w0;
+        const uint32_t bits = range_bits(*wptr, w0, kend);
+        if (!bits) continue;
+        const int32_t *np = nb + (ST ? 1 : 32) * w0;
+        const int64_t ebase = ((int64_t)(wptr - a.words) << 5) + (w0 & 31);
+        uint32_t okm = 0, bit = 1u;
+#pragma unroll U
+        for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
+            const int32_t q = slot_neighbour<ST>(np, j, p);
+            V4 xq, uq;
+            Tr<R>::template load_rec<true>(a.xu + 2 * (int64_t)q, xq, uq);
+            const Kin<R> k(xq, uq, nx, nu);
+            const R num = k.num, xx2 = k.xx2;
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+            const R dl = ly * lx + xx2;
+            const bool live = (bits & bit) != 0u;
+            if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
+            const bool ok = num < pp.cs * dl;
+            okm |= ok ? bit : 0u;
+            const typename Tr<R>::V2 mq = a.mab[q];
+            const R As = Ap + mq.x, Bs = Bp + mq.y;
+            const R ed = num * Tr<R>::rcp(ly + lx) - As * Tr<R>::rcp(Bs) * lx * R(1.0 / 3.0);
+            const R tdt = pp.g15 * Tr<R>::rcp(lx) * Bs * (ed - (R)a.edp_in[ebase + j]);
+            const double t2 = (double)tdt * (double)tdt * (double)xq.w;
+            acc += (live && ok) ? t2 : 0.0;
+        }
+        const uint32_t brk = bits & ~okm;
+        if (brk) atomicAnd(wptr, ~(brk << (w0 & 31)));
+    }
+    return acc;
+}
+
+template <class R, int WPS, int U>
+__device__ __forceinline__ void td_body(const StepArgs<R> &a, double (*sh)[1][32], int *arrive) {
+    using V4 = typename Tr<R>::V4;
+    constexpr int SPB = Split<WPS>::SPB;
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = wid % WPS;
+    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
+    const int32_t ti = p < a.N ? a.tinfo[p] : -1;
+    const bool ep = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC && a.deformed[ti >> 8];
+    double acc = 0.0;
+    if (ep) {
+        const FBlock<R> B = a.fb[ti >> 8];
+        const int tp = ti & 255;
+        V4 xp, up;
+        Tr<R>::template load_rec<true>(a.xu + 2 * p, xp, up);
+        const SliceInfo d = a.si[p >> 5];
+        int32_t k0, k1;
+        warp_range<WPS>(d.len, w, k0, k1);
+        k1 = min(k1, a.cnt[p]);
+        uint32_t *wp = a.words + d.word + (p & 31);
+        const typename Tr<R>::V2 m = a.mab[p];
+        const bool st = d.mode == kStencil;
+        const int32_t *nb = a.nbr + d.nbr + (st ? 0 : (p & 31));
+        if (B.nt > 1) {
+            acc = st ? td_walk<R, U, true, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y)
+                     : td_walk<R, U, false, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y);
+        } else {
+            acc = st ? td_walk<R, U, true, false>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y)
+                     : td_walk<R, U, false, false>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y);
+        }
+    }
+    if (WPS > 1 && !last_arrival_sum<WPS, 1>(sh, arrive, wid, lane, &acc)) return;
+    if (!ep) return;
+    a.rtd[p] = acc > 0.0 ? (R)(1.0 / sqrt(acc)) : (R)INFINITY;
+}
+
+template <class R, int WPS, int U>
+__global__ void __launch_bounds__(Split<WPS>::BT) k_td(StepArgs<R> a) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ double sh[WPS > 1 ? NW : 1][1][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    td_body<R, WPS, U>(a, sh, arrive);
+}
+
+// Per bond slot e of an elasto-plastic particle, the slot of the reverse
+// bond in the neighbour's family (partner[e]); other slots point at
+// themselves so that every read stays in range.
+template <class R>
+__global__ void __launch_bounds__(kT) k_partner(StepArgs<R> a, const uint32_t *fam, int32_t *partner) {
+    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
+    if (p >= a.N) return;
+    const SliceInfo d = a.si[p >> 5];
+    const int32_t n = a.cnt[p];
+    const int32_t ti = a.tinfo[p];
+    const bool ep = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC;
+    const bool st = d.mode == kStencil;
+    const int32_t *nb = a.nbr + d.nbr + (st ? 0 : (p & 31));
+    for (int32_t k = 0; k < d.len; ++k) {
+        const int64_t e = slot_index(a.si, p, k);
+        const bool member = ep && k < n && ((fam[e >> 5] >> (k & 31)) & 1u);
+        if (!member) {
+            partner[e] = (int32_t)e;
+            continue;
+        }
+        const int32_t q = st ? (int32_t)p + nb[k] : nb[32 * k];
+        const int32_t kq = slot_of(a.si, a.nbr, a.cnt, q, p);
+        const SliceInfo dq = a.si[q >> 5];
+        const bool found = kq < a.cnt[q] && (dq.mode == kStencil ? (int64_t)q + a.nbr[dq.nbr + kq] == p
+                                                                 : a.nbr[dq.nbr + (q & 31) + 32 * (int64_t)kq] == p);
+        partner[e] = found ? (int32_t)slot_index(a.si, q, kq) : (int32_t)e;
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -1150,6 +1325,8 @@ struct Fast {
     DBuf<int32_t> ones;   // all blocks "deformed" while tuning
     DBuf<GridBar> gbar;   // persistent-chunk barrier state
     DBuf<int32_t> serr;   // staged kernels: a staging copy timed out
+    DBuf<R> rtd;          // elasto-plastic: 1/sqrt(td_norm2) per particle
+    DBuf<int32_t> partner;  // elasto-plastic: reverse-bond slot per slot
     bool persisted = false;
     int cur = 0;
     int wps = 0;          // warps per 32-particle slice (autotuned)
@@ -1184,15 +1361,30 @@ struct Unroll {
     static constexpr int HI = sizeof(R) == 4 ? 4 : 2;
 };
 
-template <class R, int MODE, int U>
+template <class R, int MODE, int U, bool EPK = false>
 void launch_step_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
     const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);  // one slice per block
     switch (wps) {
-        case 1: k_step<R, 1, U, MODE><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_step<R, 2, U, MODE><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_step<R, 4, U, MODE><<<g1, 128, 0, st>>>(a); break;
-        default: k_step<R, 8, U, MODE><<<g1, 256, 0, st>>>(a); break;
+        case 1: k_step<R, 1, U, MODE, EPK><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_step<R, 2, U, MODE, EPK><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_step<R, 4, U, MODE, EPK><<<g1, 128, 0, st>>>(a); break;
+        default: k_step<R, 8, U, MODE, EPK><<<g1, 256, 0, st>>>(a); break;
+    }
+    note_launch();
+}
+
+// Elasto-plastic td_norm2 pass (one unroll: U = LO).
+template <class R>
+void launch_td(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    constexpr int U = Unroll<R>::LO;
+    const int64_t slices = (a.N + 31) / 32;
+    const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);
+    switch (cfg % 100 / 10) {
+        case 1: k_td<R, 1, U><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
+        case 2: k_td<R, 2, U><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
+        case 4: k_td<R, 4, U><<<g1, 128, 0, st>>>(a); break;
+        default: k_td<R, 8, U><<<g1, 256, 0, st>>>(a); break;
     }
     note_launch();
 }
@@ -1253,6 +1445,10 @@ inline cudaError_t staged_kernel_attrs() {
 
 template <class R, int MODE>
 void launch_step(cudaStream_t st, int cfg, const StepArgs<R> &a) {
+    if (a.ep) {  // elasto-plastic kernels: one unroll, no staging
+        launch_step_u<R, MODE, Unroll<R>::LO, true>(st, cfg % 100 / 10, a);
+        return;
+    }
     if constexpr (sizeof(R) == 4) {
         if (cfg >= 100) {
             launch_step_st<MODE>(st, cfg, a);
@@ -1322,6 +1518,15 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.spos = env->spos.p;
     a.serr = F.serr.p;
     a.stage_bytes = (int32_t)(env->splan_max * 32);
+    a.ep = 0;
+    for (const auto &b : env->hb)
+        if (b.kind == PD_MAT_ELASTO_PLASTIC) a.ep = 1;
+    if (a.ep) {
+        a.edp_in = env->edp[env->ecur].p;
+        a.edp_out = env->edp[1 - env->ecur].p;
+        a.rtd = F.rtd.p;
+        a.partner = F.partner.p;
+    }
     const char *sw = std::getenv("PD_SWIZZLE");
     if (!(sw && std::strcmp(sw, "0") == 0)) {  // on unless PD_SWIZZLE=0
         int dev = 0, sms = 0;
@@ -1407,8 +1612,10 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
                     size_t e = (size_t)i + (size_t)j * b.nt;
                     FPair<R> pp{};
                     pp.cs = (R)b.cs[e];
-                    pp.k35 = (R)(3 * b.K[e] - 5 * b.G[e]);
+                    const bool ep = b.kind == PD_MAT_ELASTO_PLASTIC;
+                    pp.k35 = (R)(ep ? 3 * b.K[e] : 3 * b.K[e] - 5 * b.G[e]);
                     pp.g15 = (R)(15 * b.G[e]);
+                    pp.psi = ep ? (R)std::sqrt(2 * b.psi[e]) : R(0);
                     fp.push_back(pp);
                 }
         }
@@ -1454,6 +1661,13 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
                                                          env->blocks_d.p, ai);
     note_launch();
     CK(cudaGetLastError());
+    if (ai.ep) {
+        PD_TRY(F.rtd.alloc(env->N));
+        PD_TRY(F.partner.alloc(std::max<int64_t>(env->nnz, 1)));
+        k_partner<R><<<gridn(env->N), kT, 0, env->st>>>(ai, env->fam.p, F.partner.p);
+        note_launch();
+        CK(cudaGetLastError());
+    }
     return PD_OK;
 }
 
@@ -1560,6 +1774,25 @@ bool any_lps(const pd_env *env) {
     return false;
 }
 
+bool any_ep(const pd_env *env) {
+    for (const auto &b : env->hb)
+        if (b.kind == PD_MAT_ELASTO_PLASTIC) return true;
+    return false;
+}
+
+// The dilatation pass runs for state-based and elasto-plastic blocks.
+bool need_theta(const pd_env *env) { return any_lps(env) || any_ep(env); }
+
+// One force evaluation: dilatation, the elasto-plastic td_norm2 pass, and
+// the step kernel; then the plastic strain buffers swap.
+template <class R, int MODE>
+void launch_force(pd_env *env, cudaStream_t st, int cfg, const StepArgs<R> &a, bool theta) {
+    if (theta) launch_theta(st, cfg, a);
+    if (a.ep) launch_td(st, cfg, a);
+    launch_step<R, MODE>(st, cfg, a);
+    if (a.ep) env->ecur = 1 - env->ecur;
+}
+
 // Project autotuner: times the force (and dilatation) kernels for every
 // warps-per-slice split on the environment itself -- force written to a
 // scratch array, no bond breaking, every block treated as deformed -- and
@@ -1572,14 +1805,15 @@ template <class R>
 pd_status autotune(pd_env *env, Fast<R> &F) {
     if (F.wps) return PD_OK;
     // staged shapes: FP32C, 4 or 8 warps per slice, when some slice has a plan
-    const bool can_stage = sizeof(R) == 4 && env->splan_slices > 0;
+    const bool ep = any_ep(env);
+    const bool can_stage = sizeof(R) == 4 && env->splan_slices > 0 && !ep;
     if (can_stage) CK(staged_kernel_attrs());
     auto staged_ok = [&](int w) { return can_stage && (w == 4 || w == 8); };
     if (env->shape) {  // pd_env_set_kernel_shape (+ pd_env_set_record_staging)
         F.wps = env->shape + (env->staging == 1 && staged_ok(env->shape / 10) ? 100 : 0);
         return PD_OK;
     }
-    const bool lps = any_lps(env);
+    const bool lps = need_theta(env);
     const auto key = std::make_tuple(env->N, env->nnz, env->precision * 4 + env->staging + 1, lps);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -1623,6 +1857,14 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     PD_TRY(twords.alloc(nwords));
     CK(cudaMemcpyAsync(twords.p, a.words, nwords * 4, cudaMemcpyDeviceToDevice, env->st));
     a.words = twords.p;
+    DBuf<double> tedp;
+    DBuf<R> trtd;
+    if (a.ep) {  // plastic strain and td_norm2 of the timed steps go to scratch
+        PD_TRY(tedp.alloc(std::max<int64_t>(env->nnz, 1)));
+        PD_TRY(trtd.alloc(N));
+        a.edp_out = tedp.p;
+        a.rtd = trtd.p;
+    }
     int64_t nlast = 0;
     for (int k = 0; k < a.nbc; ++k)
         if (a.bc[k].last) nlast += a.bc[k].n;
@@ -1643,6 +1885,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     std::vector<int> shapes;
     for (int wps : {1, 2, 4, 8})
         for (int u : {Unroll<R>::LO, Unroll<R>::HI}) {
+            if (ep && u != Unroll<R>::LO) continue;  // the elasto-plastic kernels have one unroll
             if (env->staging != 1 || !staged_ok(wps)) shapes.push_back(10 * wps + u);
             if (env->staging >= 1 && staged_ok(wps)) shapes.push_back(100 + 10 * wps + u);
         }
@@ -1663,6 +1906,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
         if (err == cudaSuccess) {
             for (int r = 0; r < kTuneSteps; ++r) {
                 if (lps) launch_theta(env->st, shapes[i], a);
+                if (a.ep) launch_td(env->st, shapes[i], a);
                 launch_step<R, 1>(env->st, shapes[i], a);
             }
             err = cudaStreamEndCapture(env->st, &graph);
@@ -1809,7 +2053,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
             for (auto &g : F.graphs) cudaGraphExecDestroy(g.exec);
             F.graphs.clear();
         }
-        const int cur0 = F.cur;
+        const int cur0 = F.cur, ecur0 = env->ecur;
         const int64_t n0 = launch_count();
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < kGraphSteps; ++k) {
@@ -1817,13 +2061,13 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
             a.dir_vel = a.dir_pos = a0.dir_vel;
             a.ts = 0;
             gate_launch(env, a, F);
-            if (lps) launch_theta(st, F.wps, a);
-            launch_step<R, 1>(st, F.wps, a);
+            launch_force<R, 1>(env, st, F.wps, a, lps);
             F.cur = 1 - F.cur;
         }
         cudaGraph_t graph = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(st, &graph);
-        F.cur = cur0;  // kGraphSteps is even: the parity is unchanged
+        F.cur = cur0;  // kGraphSteps is even: the parities are unchanged
+        env->ecur = ecur0;
         const int64_t kernels = launch_count() - n0;  // captured, not run
         add_launches(-kernels);
         if (ce != cudaSuccess) return cuda_fail(ce, "graph capture", __FILE__, __LINE__);
@@ -1906,7 +2150,7 @@ template <class R>
 pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true) {
     cudaStream_t st = env->st;
     const unsigned grid = gridn(env->N);
-    const bool lps = any_lps(env);
+    const bool lps = need_theta(env);
     const bool contacts = !env->hc.empty();
     PD_TRY(autotune(env, F));
     const int wps = F.wps;
@@ -1928,7 +2172,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
     // against 49.1 us per step; 17.6 k-particle PMB cube: 15.6 against
     // 17.5 us), the grid barriers costing more than graph kernel boundaries.
     const char *pe = std::getenv("PD_PERSIST");
-    const bool persist = graphs && pe && std::strcmp(pe, "1") == 0;
+    const bool persist = graphs && pe && std::strcmp(pe, "1") == 0 && !any_ep(env);
     bool persist_fits = true;
     PD_TRY(gate_prepare(env, F));
     for (int64_t s = 0; s < nsteps;) {
@@ -1963,6 +2207,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         a.ts = env->ts;
         gate_launch(env, a, F);
         if (lps) launch_theta(st, wps, a);
+        if (a.ep) launch_td(st, wps, a);
         prof_begin(env, st);
         if (!contacts) {
             if (stop) launch_step<R, 2>(st, wps, a);
@@ -1976,6 +2221,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
             else k_integrate<R, 3><<<grid, kT, 0, st>>>(a);
             note_launch();
         }
+        if (a.ep) env->ecur = 1 - env->ecur;
         if (check) {
             for (size_t k = 0; k < env->hbc.size(); ++k) {
                 if (!env->hbc[k].scales_at(env->ts - 1)) continue;
@@ -2017,10 +2263,12 @@ pd_status update_acc_fast(pd_env *env, Fast<R> &F) {
     PD_TRY(autotune(env, F));
     StepArgs<R> a = args(env, F);
     PD_TRY(gate_if_needed(env, a, F));
-    if (any_lps(env)) launch_theta(env->st, F.wps, a);
+    if (need_theta(env)) launch_theta(env->st, F.wps, a);
+    if (a.ep) launch_td(env->st, F.wps, a);
     prof_begin(env, env->st);
     launch_step<R, 0>(env->st, F.wps, a);
     prof_end(env, env->st);
+    if (a.ep) env->ecur = 1 - env->ecur;
     PD_TRY(contacts_fast(env, a));
     return PD_OK;
 }
@@ -2036,9 +2284,8 @@ pd_status export_fast(pd_env *env, Fast<R> &F) {
 }
 
 pd_status ensure_fast(pd_env *env) {
-    for (const auto &b : env->hb)
-        if (b.kind == PD_MAT_ELASTO_PLASTIC)
-            return fail(PD_ERR_UNSUPPORTED, "the elasto-plastic solid runs in PD_PREC_FP64_SERIAL only");
+    if (any_ep(env) && env->nnz >= ((int64_t)1 << 31))
+        return fail(PD_ERR_UNSUPPORTED, "elasto-plastic throughput mode: more than 2^31 bond slots");
     if (env->hbc.size() > (size_t)kMaxFastBC)
         return fail(PD_ERR_UNSUPPORTED, "the throughput modes support at most %d boundary conditions", kMaxFastBC);
     if (!env->fast) {

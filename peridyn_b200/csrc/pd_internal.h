@@ -126,6 +126,24 @@ __device__ __forceinline__ int64_t slot_index(const SliceInfo *si, int64_t p, in
     return ((si[p >> 5].word + 32 * (int64_t)(k >> 5) + (p & 31)) << 5) + (k & 31);
 }
 
+// Slot of neighbour p in q's family: slots hold descending neighbour
+// indices (stencil slices: descending offsets), so a binary search.
+__device__ __forceinline__ int32_t slot_of(const SliceInfo *si, const int32_t *nbr, const int32_t *cnt, int64_t q,
+                                           int64_t p) {
+    const SliceInfo s = si[q >> 5];
+    const bool st = s.mode == kStencil;
+    const int32_t *nb = nbr + s.nbr + (st ? 0 : (q & 31));
+    const int32_t target = st ? (int32_t)(p - q) : (int32_t)p;
+    int32_t lo = 0, hi = cnt[q];
+    while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        const int32_t v = st ? nb[mid] : nb[32 * mid];
+        if (v > target) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 struct BCDev {
     int32_t kind;
     int32_t dims;      // bit d set: dimension d constrained

@@ -9,7 +9,7 @@ import pytest
 
 import peridyn_b200 as pb
 from peridyn_b200 import configs, lattice
-from tests.cases import bar_with_bcs, random_cloud, self_contact_block
+from tests.cases import bar_with_bcs, ep_cube, random_cloud, self_contact_block
 
 pytestmark = pytest.mark.gpu
 
@@ -345,3 +345,51 @@ def test_slice_swizzle_is_bit_identical(shape, monkeypatch):
     for a, b in zip(s1, s2):
         assert np.array_equal(a, b)
     assert np.array_equal(i1, i2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+@pytest.mark.parametrize("builder", [lambda: ep_cube(5e6), lambda: ep_cube(2e6, ntypes=2),
+                                     lambda: ep_cube(5e6, peak=300.0, cs=0.003), lambda: configs.ep_bar(nx=40)])
+def test_elasto_plastic_fast(oracle, precision, builder):
+    """Throughput-mode elasto-plastic solid (td_norm2 pass with bond
+    breaking, both visits' terms per bond, per-slot plastic strain) against
+    the serial oracle: displacement, velocity, plastic strain and bonds."""
+    w = builder()
+    bc0 = bool(w["bcs"])
+    nsteps = 40
+    env, ora = _run_pair(oracle, w, precision, nsteps, bc0=bc0)
+    eu, ev, mism = _errors(env, ora)
+    tol = TOL[precision]
+    assert eu <= tol, eu
+    assert ev <= (1e-9 if precision == "fp64" else 1e-3), ev
+    B = ora.blocks[0]
+    edp = env.plastic_strain(0)
+    fam = B.family > 0
+    assert np.abs(B.edp[fam]).max() > 0.0
+    assert rel_l2(edp[fam], B.edp[fam]) <= (1e-8 if precision == "fp64" else 2e-3)
+    if precision == "fp64":
+        assert mism == 0
+    env.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_elasto_plastic_fast_graphs_match_direct(precision, monkeypatch):
+    # graph replays alternate the plastic strain buffers like direct launches
+    w = configs.ep_bar(nx=30)
+
+    def run():
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+        pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=101)
+        out = env.get_state(), env._family(0)[1], env.plastic_strain(0)
+        env.close()
+        return out
+
+    monkeypatch.setenv("PD_NO_GRAPHS", "1")
+    s1, i1, e1 = run()
+    monkeypatch.delenv("PD_NO_GRAPHS")
+    s2, i2, e2 = run()
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    assert np.array_equal(i1, i2)
+    assert np.array_equal(e1, e2)

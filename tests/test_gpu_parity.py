@@ -355,10 +355,11 @@ def test_elasto_plastic_bit_exact(oracle, builder, layout):
     env.close()
 
 
-def test_elasto_plastic_needs_serial_mode():
+def test_elasto_plastic_serial_plastic_strain_export(oracle):
     w = ep_cube(5e6, n=6)
-    env = pb.Env(1, w["materials"], [], [], w["dt"], precision="fp32c")
-    with pytest.raises(pb.PDError) as e:
-        pb.velocity_verlet_step(env, nsteps=2)
-    assert e.value.status == _abi.PD_ERR_UNSUPPORTED
+    env, ora = _pair(oracle, w)
+    for _ in range(10):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=10)
+    assert np.array_equal(env.plastic_strain(0), ora.blocks[0].edp)
     env.close()
