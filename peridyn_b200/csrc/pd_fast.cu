@@ -45,6 +45,7 @@ struct Tr<float> {
     using V4 = float4;
     using V2 = float2;
     static __device__ __forceinline__ float rsq(float a) { return rsqrtf(a); }
+    static __device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
     static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
     // single-instruction approximations (relative error of order 2^-22)
     static __device__ __forceinline__ float sqrt_(float a) {
@@ -72,12 +73,21 @@ struct Tr<float> {
                          : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
                          : "l"(r));
     }
+    // The displacement half of a record alone (u, w): uniform-geometry
+    // slices take the reference bond vector from their slot table.
+    template <bool NC = true>
+    static __device__ __forceinline__ void load_u_rec(const float4 *r, float4 &u) {
+        if (NC) asm("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w) : "l"(r));
+        else
+            asm volatile("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w) : "l"(r));
+    }
 };
 template <>
 struct Tr<double> {
     using V4 = double4;
     using V2 = double2;
     static __device__ __forceinline__ double rsq(double a) { return rsqrt(a); }
+    static __device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
     static __device__ __forceinline__ double sqrt_(double a) { return sqrt(a); }
     static __device__ __forceinline__ double rcp(double a) { return 1.0 / a; }
@@ -92,6 +102,13 @@ struct Tr<double> {
             asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w)
                          : "l"(r + 1));
         }
+    }
+    template <bool NC = true>
+    static __device__ __forceinline__ void load_u_rec(const double4 *r, double4 &u) {
+        if (NC) asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r));
+        else
+            asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w)
+                         : "l"(r));
     }
 };
 
@@ -126,9 +143,10 @@ template <class R>
 struct StepArgs {
     int64_t N;
     // Interleaved particle records, double-buffered by step parity:
-    // xu[2i] = (x, volume) (FP32C: relative to the block centre; identical
-    // in both buffers), xu[2i+1] = (u, -) displacement.  One address per
-    // neighbour fetches both.
+    // xu[2i] = (x, w) (FP32C: relative to the block centre; identical in
+    // both buffers), xu[2i+1] = (u, w) displacement; w = the volume (times
+    // c in bond-based blocks) in both halves.  One address per neighbour
+    // fetches both; uniform-geometry walks read the (u, w) half alone.
     const typename Tr<R>::V4 *xu;
     typename Tr<R>::V4 *xn;  // next-step buffer (only the u records are written)
     double *ax, *ay, *az;    // FP64 displacement accumulator (FP32C)
@@ -137,6 +155,9 @@ struct StepArgs {
     typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
     const int32_t *tinfo, *cnt, *nbr;
     const SliceInfo *si;
+    // uniform-geometry slices: slot table (xi, |xi|) from geo[geo_off[s]]
+    const int32_t *geo_off;
+    const typename Tr<R>::V4 *geo;
     // record staging plans (FP32C staged kernels): see pd_env
     const int32_t *splan_off, *splan, *spos;
     int32_t *serr;        // set when a staging copy did not land in time
@@ -273,11 +294,21 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 template <class R>
 struct Kin {
     R Y0, Y1, Y2, xx2, num;
+    __device__ __forceinline__ Kin(const typename Tr<R>::V4 &g, const typename Tr<R>::V4 &uq,
+                                   const typename Tr<R>::V4 &nu) {
+        const R x0 = g.x, x1 = g.y, x2 = g.z;
+        const R e0 = uq.x + nu.x, e1 = uq.y + nu.y, e2 = uq.z + nu.z;
+        Y0 = x0 + e0;
+        Y1 = x1 + e1;
+        Y2 = x2 + e2;
+        xx2 = g.w * g.w;
+        num = Tr<R>::fma_(e2, x2 + Y2, Tr<R>::fma_(e1, x1 + Y1, e0 * (x0 + Y0)));
+    }
     // f += c Y
     __device__ __forceinline__ void accumulate(R c, R &fx, R &fy, R &fz) const {
-        fx += c * Y0;
-        fy += c * Y1;
-        fz += c * Y2;
+        fx = Tr<R>::fma_(c, Y0, fx);
+        fy = Tr<R>::fma_(c, Y1, fy);
+        fz = Tr<R>::fma_(c, Y2, fz);
     }
     __device__ __forceinline__ Kin(const typename Tr<R>::V4 &xq, const typename Tr<R>::V4 &uq,
                                    const typename Tr<R>::V4 &nx, const typename Tr<R>::V4 &nu) {
@@ -286,18 +317,32 @@ struct Kin {
         Y0 = x0 + e0;
         Y1 = x1 + e1;
         Y2 = x2 + e2;
-        xx2 = x0 * x0 + x1 * x1 + x2 * x2;
-        num = e0 * (x0 + Y0) + e1 * (x1 + Y1) + e2 * (x2 + Y2);
+        xx2 = Tr<R>::fma_(x2, x2, Tr<R>::fma_(x1, x1, x0 * x0));
+        num = Tr<R>::fma_(e2, x2 + Y2, Tr<R>::fma_(e1, x1 + Y1, e0 * (x0 + Y0)));
     }
 };
 // FP32: the (x, y) components as packed f32x2 operations.
 template <>
 struct Kin<float> {
+    // from the slot table: g = (xi, |xi|), so |xi|^2 = |xi| |xi|
+    __device__ __forceinline__ Kin(const float4 &g, const float4 &uq, const float4 &nu) {
+        const float2 d = make_float2(g.x, g.y);
+        const float2 e = __fadd2_rn(make_float2(uq.x, uq.y), make_float2(nu.x, nu.y));
+        const float dz = g.z, ez = uq.z + nu.z;
+        const float2 Y = __fadd2_rn(d, e);
+        const float Yz = dz + ez;
+        const float2 S = __fadd2_rn(d, Y);
+        const float2 es = __fmul2_rn(e, S);
+        xx2 = g.w * g.w;
+        num = fmaf(ez, dz + Yz, es.x + es.y);
+        Yxy = Y;
+        Y2 = Yz;
+    }
     float2 Yxy;
     float Y2, xx2, num;
     __device__ __forceinline__ void accumulate(float c, float2 &fxy, float &fz) const {
         fxy = __ffma2_rn(make_float2(c, c), Yxy, fxy);
-        fz += c * Y2;
+        fz = fmaf(c, Y2, fz);
     }
     __device__ __forceinline__ Kin(const float4 &xq, const float4 &uq, const float4 &nx, const float4 &nu) {
         const float2 d = __fadd2_rn(make_float2(xq.x, xq.y), make_float2(nx.x, nx.y));
@@ -317,12 +362,16 @@ struct Kin<float> {
 
 // STG: the neighbour records come from the block's staged copy in shared
 // memory (stg, lane 0's record of slot k at sp[k]) instead of global memory.
-template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false>
+// UG: a uniform-geometry stencil slice: the reference bond vector and its
+// length come from the slot table (gp[k]) and only the neighbour's (u, w)
+// half-record is loaded.
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false,
+          bool UG = false>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
                                           typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz,
                                           const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
-                                          R rtdp = R(0)) {
+                                          R rtdp = R(0), const typename Tr<R>::V4 *gp = nullptr) {
     using V4 = typename Tr<R>::V4;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -346,6 +395,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
         // stencil slots point at an in-range record and carry a 0 bit.
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         const int32_t *spp = STG ? sp + w0 : nullptr;
+        const V4 *gpp = UG ? gp + w0 : nullptr;
         // elasto-plastic: per-slot state index of the chunk's first slot
         const int64_t ebase = KIND == PD_MAT_ELASTO_PLASTIC ? ((int64_t)(wptr - a.words) << 5) + (w0 & 31) : 0;
         uint32_t okm = 0, bit = 1u;  // okm: slots within the critical stretch
@@ -355,16 +405,20 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
             V4 xq, uq;
             if constexpr (STG) {
                 const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
-                xq = stg[2 * r];
+                xq = UG ? gpp[j] : stg[2 * r];
                 uq = stg[2 * r + 1];
+            } else if constexpr (UG) {
+                xq = gpp[j];  // (xi, |xi|)
+                Tr<R>::template load_u_rec<NC>(a.xu + 2 * (int64_t)q + 1, uq);
             } else {
                 Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             }
-            const Kin<R> k(xq, uq, nx, nu);
+            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
+            const R wq = UG ? uq.w : xq.w;  // V_q (c V_q in bond-based blocks)
             // stretch s = num / dl;  |Y|^2 = |xi|^2 + num
-            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
-            const R dl = ly * lx + xx2;  // (|Y| + |xi|) |xi|
+            const R lx = UG ? xq.w : Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+            const R dl = Tr<R>::fma_(ly, lx, xx2);  // (|Y| + |xi|) |xi|
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             const bool ok = num < pp.cs * dl;
@@ -376,7 +430,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
                 tn = num;
             } else if (KIND == PD_MAT_ORDINARY_STATE_BASED) {
                 typename Tr<R>::V2 mq = a.mab[q];
-                tn = pp.k35 * (Ap + mq.x) * dl + pp.g15 * num * (Bp + mq.y);
+                tn = Tr<R>::fma_(pp.k35 * (Ap + mq.x), dl, pp.g15 * num * (Bp + mq.y));
             } else {
                 // force_density_t_ij (elasto_plastic.jl:215-242) of both
                 // visits: p's (its slot e, its td_norm2) and q's (the
@@ -387,7 +441,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
                 typename Tr<R>::V2 mq = a.mab[q];
                 const R As = Ap + mq.x, Bs = Bp + mq.y;
                 const R ext = num * Tr<R>::rcp(ly + lx);
-                const R ed = ext - As * Tr<R>::rcp(Bs) * lx * R(1.0 / 3.0);
+                const R ed = Tr<R>::fma_(-As * Tr<R>::rcp(Bs), lx * R(1.0 / 3.0), ext);
                 const R gB = pp.g15 * Tr<R>::rcp(lx) * Bs;
                 const int64_t e = ebase + j;
                 const int32_t pe = a.partner[e];
@@ -397,10 +451,10 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
                 const bool pl = Cp <= R(1);  // p's visit yields
                 const R td_p = gB * ede_p * (pl ? Cp : R(1));
                 const R td_q = gB * ede_q * (Cq <= R(1) ? Cq : R(1));
-                tn = (pp.k35 * As + R(0.5) * (td_p + td_q)) * dl;
-                a.edp_out[e] = (live && ok && pl) ? (double)((R)eo + ede_p * (R(1) - Cp)) : eo;
+                tn = Tr<R>::fma_(pp.k35, As, R(0.5) * (td_p + td_q)) * dl;
+                a.edp_out[e] = (live && ok && pl) ? (double)Tr<R>::fma_(ede_p, R(1) - Cp, (R)eo) : eo;
             }
-            const R coef = (live && ok) ? tn * xq.w * Tr<R>::rcp(dl * ly) : R(0);
+            const R coef = (live && ok) ? tn * wq * Tr<R>::rcp(dl * ly) : R(0);
             if constexpr (sizeof(R) == 4) k.accumulate(coef, fxy, fz);
             else k.accumulate(coef, fx, fy, fz);
         }
@@ -430,6 +484,34 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         Bp = m.y;
     }
     if (KIND == PD_MAT_ELASTO_PLASTIC) rtdp = a.rtd[p];
+    const int32_t goff = (a.geo_off && d.mode == kStencil) ? a.geo_off[p >> 5] : -1;
+    if constexpr (STG) {
+        if (stg && goff >= 0) {  // staged records, uniform geometry
+            const int32_t *sp = a.spos + d.nbr;
+            const typename Tr<R>::V4 *gp = a.geo + goff;
+            if (B.nt > 1)
+                bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp,
+                                                                           xp, up, Ap, Bp, fx, fy, fz, stg, sp, rtdp,
+                                                                           gp);
+            else
+                bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp,
+                                                                            xp, up, Ap, Bp, fx, fy, fz, stg, sp, rtdp,
+                                                                            gp);
+            return;
+        }
+    }
+    if (goff >= 0 && !(STG && stg)) {
+        const typename Tr<R>::V4 *gp = a.geo + goff;
+        if (B.nt > 1)
+            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                                                                            up, Ap, Bp, fx, fy, fz, nullptr, nullptr,
+                                                                            rtdp, gp);
+        else
+            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                                                                             up, Ap, Bp, fx, fy, fz, nullptr, nullptr,
+                                                                             rtdp, gp);
+        return;
+    }
     if constexpr (STG) {
         if (stg) {  // a staged slice is a stencil slice
             const int32_t *sp = a.spos + d.nbr;
@@ -549,7 +631,7 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
     o.x = (R)u0;
     o.y = (R)u1;
     o.z = (R)u2;
-    o.w = R(0);
+    o.w = a.xu[2 * p].w;  // the record weight, kept in both halves
     a.xn[2 * p + 1] = o;
 }
 
@@ -566,13 +648,13 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
 // One step of one slice (its WPS warps): bond gather, fixed-order
 // combination, integration.  Shared by k_step and the persistent kernel.
 template <class R, int WPS, int U, int MODE, bool NC, bool STG = false, bool EPK = false>
-__device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], int *arrive,
+__device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (*sh)[3][32], int *arrive,
                                           const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
     constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
+    const int64_t p = (blk * SPB + wid / WPS) * 32 + lane;
     if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     constexpr bool kBreak = MODE != 5;
@@ -606,8 +688,12 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, R (*sh)[3][32], 
     integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
 }
 
+// Elasto-plastic kernels (EPK) keep more state per bond: up to 128 registers.
 template <class R, int WPS, int U, int MODE, bool EPK = false>
-__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? Split<WPS>::MINB_U2 : Split<WPS>::MINB)
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1
+                                                  : EPK     ? Split<WPS>::MINB / 2
+                                                  : U <= 2  ? Split<WPS>::MINB_U2
+                                                            : Split<WPS>::MINB)
     k_step(StepArgs<R> a) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
@@ -616,7 +702,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? 
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    step_body<R, WPS, U, MODE, true, false, EPK>(a, sh, arrive);
+    step_body<R, WPS, U, MODE, true, false, EPK>(a, slice_of_block<SPB>(a), sh, arrive);
 }
 
 // MODE 3/4: integration of forces already in f (after contact forces).
@@ -652,21 +738,21 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
         if (MODE == 2) a.p[p] = V4{m * vp.x, m * vp.y, m * vp.z, R(0)};
     }
     const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
-    R v0 = vp.x + a.c * fx, v1 = vp.y + a.c * fy, v2 = vp.z + a.c * fz;
+    R v0 = Tr<R>::fma_(a.c, fx, vp.x), v1 = Tr<R>::fma_(a.c, fy, vp.y), v2 = Tr<R>::fma_(a.c, fz, vp.z);
     if (bits) bc_velocity(a, p, bits, v0, v1, v2);
     if (MODE == 2 || MODE == 4) {
         a.v[p] = V4{v0, v1, v2, R(0)};
         a.f[p] = V4{fx, fy, fz, R(0)};
         return;
     }
-    v0 += a.c * fx;
-    v1 += a.c * fy;
-    v2 += a.c * fz;
+    v0 = Tr<R>::fma_(a.c, fx, v0);
+    v1 = Tr<R>::fma_(a.c, fy, v1);
+    v2 = Tr<R>::fma_(a.c, fz, v2);
     double u0, u1, u2;
     load_u(a, p, u0, u1, u2);
-    u0 += a.dt * (double)v0;
-    u1 += a.dt * (double)v1;
-    u2 += a.dt * (double)v2;
+    u0 = fma(a.dt, (double)v0, u0);
+    u1 = fma(a.dt, (double)v1, u1);
+    u2 = fma(a.dt, (double)v2, u2);
     if (bits) bc_position(a, p, bits, u0, u1, u2);
     a.v[p] = V4{v0, v1, v2, R(0)};
     store_u(a, p, u0, u1, u2);
@@ -683,22 +769,23 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
         return;
     }
     const V4 ff = a.f[p], vp = a.v[p];
-    const R v0 = vp.x + a.c * ff.x, v1 = vp.y + a.c * ff.y, v2 = vp.z + a.c * ff.z;
+    const R v0 = Tr<R>::fma_(a.c, ff.x, vp.x), v1 = Tr<R>::fma_(a.c, ff.y, vp.y), v2 = Tr<R>::fma_(a.c, ff.z, vp.z);
     double u0, u1, u2;
     load_u(a, p, u0, u1, u2);
-    u0 += a.dt * (double)v0;
-    u1 += a.dt * (double)v1;
-    u2 += a.dt * (double)v2;
+    u0 = fma(a.dt, (double)v0, u0);
+    u1 = fma(a.dt, (double)v1, u1);
+    u2 = fma(a.dt, (double)v2, u2);
     const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
     if (bits) bc_position(a, p, bits, u0, u1, u2);
     a.v[p] = V4{v0, v1, v2, R(0)};
     store_u(a, p, u0, u1, u2);
 }
 
-template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false>
+template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false, bool UG = false>
 __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                         const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up,
-                                        const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr) {
+                                        const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
+                                        const typename Tr<R>::V4 *gp = nullptr) {
     using V4 = typename Tr<R>::V4;
     R acc = 0;
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -709,22 +796,27 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t
         if (!bits) continue;
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         const int32_t *spp = STG ? sp + w0 : nullptr;
+        const V4 *gpp = UG ? gp + w0 : nullptr;
         uint32_t bit = 1u;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             V4 xq, uq;
             if constexpr (STG) {
                 const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
-                xq = stg[2 * r];
+                xq = UG ? gpp[j] : stg[2 * r];
                 uq = stg[2 * r + 1];
+            } else if constexpr (UG) {
+                const int32_t q = slot_neighbour<ST>(np, j, p);
+                xq = gpp[j];
+                Tr<R>::template load_u_rec<NC>(a.xu + 2 * (int64_t)q + 1, uq);
             } else {
                 const int32_t q = slot_neighbour<ST>(np, j, p);
                 Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             }
-            const Kin<R> k(xq, uq, nx, nu);
+            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
             const R num = k.num;
-            const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
-            const R term = num * xq.w * Tr<R>::rcp(ly + lx);
+            const R lx = UG ? xq.w : Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
+            const R term = num * (UG ? uq.w : xq.w) * Tr<R>::rcp(ly + lx);
             acc += (bits & bit) ? term : R(0);
         }
     }
@@ -734,13 +826,13 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
 template <class R, int WPS, int U, bool NC, bool STG = false>
-__device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32], int *arrive,
+__device__ __forceinline__ void theta_body(const StepArgs<R> &a, int64_t blk, R (*sh)[1][32], int *arrive,
                                            const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
     constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
+    const int64_t p = (blk * SPB + wid / WPS) * 32 + lane;
     if (NC && p - lane < a.N) prefetch_slice_indices<WPS>(a.nbr, a.si, p >> 5, w, lane);
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && (a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED ||
@@ -754,9 +846,16 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, R (*sh)[1][32],
         warp_range<WPS>(d.len, w, k0, k1);
         k1 = min(k1, a.cnt[p]);
         const uint32_t *wp = a.words + d.word + (p & 31);
-        if (STG && stg)
+        const int32_t goff = (a.geo_off && d.mode == kStencil) ? a.geo_off[p >> 5] : -1;
+        if (STG && stg && goff >= 0)
+            acc = theta_walk<R, WPS, U, true, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
+                                                              a.spos + d.nbr, a.geo + goff);
+        else if (STG && stg)
             acc = theta_walk<R, WPS, U, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
                                                         a.spos + d.nbr);
+        else if (goff >= 0)
+            acc = theta_walk<R, WPS, U, true, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, nullptr,
+                                                               nullptr, a.geo + goff);
         else if (d.mode == kStencil)
             acc = theta_walk<R, WPS, U, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up);
         else
@@ -778,7 +877,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    theta_body<R, WPS, U, true>(a, sh, arrive);
+    theta_body<R, WPS, U, true>(a, slice_of_block<SPB>(a), sh, arrive);
 }
 
 // ---------------------------------------------------------------------
@@ -790,10 +889,11 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
 // (td_trial^2 exceeds the FP32 range in SI units); stored as
 // 1/sqrt(td_norm2) in the working precision.
 // ---------------------------------------------------------------------
-template <class R, int U, bool ST, bool MULTI>
+template <class R, int U, bool ST, bool MULTI, bool UG = false>
 __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1,
                                           const int32_t *nb, uint32_t *wp, const FBlock<R> &B, int tp,
-                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp) {
+                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp,
+                                          const typename Tr<R>::V4 *gp = nullptr) {
     using V4 = typename Tr<R>::V4;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -805,26 +905,32 @@ __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32
         const uint32_t bits = range_bits(*wptr, w0, kend);
         if (!bits) continue;
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
+        const V4 *gpp = UG ? gp + w0 : nullptr;
         const int64_t ebase = ((int64_t)(wptr - a.words) << 5) + (w0 & 31);
         uint32_t okm = 0, bit = 1u;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            Tr<R>::template load_rec<true>(a.xu + 2 * (int64_t)q, xq, uq);
-            const Kin<R> k(xq, uq, nx, nu);
+            if constexpr (UG) {
+                xq = gpp[j];
+                Tr<R>::template load_u_rec<true>(a.xu + 2 * (int64_t)q + 1, uq);
+            } else {
+                Tr<R>::template load_rec<true>(a.xu + 2 * (int64_t)q, xq, uq);
+            }
+            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
-            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
-            const R dl = ly * lx + xx2;
+            const R lx = UG ? xq.w : Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+            const R dl = Tr<R>::fma_(ly, lx, xx2);
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
             const bool ok = num < pp.cs * dl;
             okm |= ok ? bit : 0u;
             const typename Tr<R>::V2 mq = a.mab[q];
             const R As = Ap + mq.x, Bs = Bp + mq.y;
-            const R ed = num * Tr<R>::rcp(ly + lx) - As * Tr<R>::rcp(Bs) * lx * R(1.0 / 3.0);
+            const R ed = Tr<R>::fma_(-As * Tr<R>::rcp(Bs), lx * R(1.0 / 3.0), num * Tr<R>::rcp(ly + lx));
             const R tdt = pp.g15 * Tr<R>::rcp(lx) * Bs * (ed - (R)a.edp_in[ebase + j]);
-            const double t2 = (double)tdt * (double)tdt * (double)xq.w;
+            const double t2 = (double)tdt * (double)tdt * (double)(UG ? uq.w : xq.w);
             acc += (live && ok) ? t2 : 0.0;
         }
         const uint32_t brk = bits & ~okm;
@@ -834,12 +940,12 @@ __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32
 }
 
 template <class R, int WPS, int U>
-__device__ __forceinline__ void td_body(const StepArgs<R> &a, double (*sh)[1][32], int *arrive) {
+__device__ __forceinline__ void td_body(const StepArgs<R> &a, int64_t blk, double (*sh)[1][32], int *arrive) {
     using V4 = typename Tr<R>::V4;
     constexpr int SPB = Split<WPS>::SPB;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = wid % WPS;
-    const int64_t p = (slice_of_block<SPB>(a) * SPB + wid / WPS) * 32 + lane;
+    const int64_t p = (blk * SPB + wid / WPS) * 32 + lane;
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool ep = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC && a.deformed[ti >> 8];
     double acc = 0.0;
@@ -856,7 +962,12 @@ __device__ __forceinline__ void td_body(const StepArgs<R> &a, double (*sh)[1][32
         const typename Tr<R>::V2 m = a.mab[p];
         const bool st = d.mode == kStencil;
         const int32_t *nb = a.nbr + d.nbr + (st ? 0 : (p & 31));
-        if (B.nt > 1) {
+        const int32_t goff = (a.geo_off && st) ? a.geo_off[p >> 5] : -1;
+        if (goff >= 0) {
+            acc = B.nt > 1 ? td_walk<R, U, true, true, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y, a.geo + goff)
+                           : td_walk<R, U, true, false, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y,
+                                                              a.geo + goff);
+        } else if (B.nt > 1) {
             acc = st ? td_walk<R, U, true, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y)
                      : td_walk<R, U, false, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y);
         } else {
@@ -870,7 +981,7 @@ __device__ __forceinline__ void td_body(const StepArgs<R> &a, double (*sh)[1][32
 }
 
 template <class R, int WPS, int U>
-__global__ void __launch_bounds__(Split<WPS>::BT) k_td(StepArgs<R> a) {
+__global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB / 2) k_td(StepArgs<R> a) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ double sh[WPS > 1 ? NW : 1][1][32];
     __shared__ int arrive[SPB];
@@ -878,7 +989,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT) k_td(StepArgs<R> a) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    td_body<R, WPS, U>(a, sh, arrive);
+    td_body<R, WPS, U>(a, slice_of_block<SPB>(a), sh, arrive);
 }
 
 // Per bond slot e of an elasto-plastic particle, the slot of the reverse
@@ -978,7 +1089,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB) k_step_st(St
     if (threadIdx.x == 0) arrive[0] = 0;
     const float4 *stg = stage_slice(a, blockIdx.x, srec, &bar);
     __syncthreads();
-    step_body<float, WPS, U, MODE, true, true>(a, sh, arrive, stg);
+    step_body<float, WPS, U, MODE, true, true>(a, blockIdx.x, sh, arrive, stg);
 }
 
 template <int WPS, int U>
@@ -991,7 +1102,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB_THETA) k_thet
     if (threadIdx.x == 0) arrive[0] = 0;
     const float4 *stg = stage_slice(a, blockIdx.x, srec, &bar);
     __syncthreads();
-    theta_body<float, WPS, U, true, true>(a, sh, arrive, stg);
+    theta_body<float, WPS, U, true, true>(a, blockIdx.x, sh, arrive, stg);
 }
 
 // ---------------------------------------------------------------------
@@ -1052,10 +1163,10 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         a.xn = (s & 1) ? b0 : b1;
         a.ts = ts0 + s;
         if (LPS) {
-            theta_body<R, WPS, U, false>(a, sh1, arrive);
+            theta_body<R, WPS, U, false>(a, blockIdx.x, sh1, arrive);
             if (!grid_barrier(gb, gridDim.x)) return;
         }
-        step_body<R, WPS, U, 1, false>(a, sh, arrive);
+        step_body<R, WPS, U, 1, false>(a, blockIdx.x, sh, arrive);
         if (s + 1 < nsteps && !grid_barrier(gb, gridDim.x)) return;
     }
 }
@@ -1146,8 +1257,8 @@ __global__ void k_import(int64_t N, const double4 *x4, const double4 *y, const d
     V4 *cur = const_cast<V4 *>(a.xu);
     cur[2 * p] = xs;
     a.xn[2 * p] = xs;
-    cur[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, R(0)};
-    a.xn[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, R(0)};
+    cur[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, xs.w};
+    a.xn[2 * p + 1] = V4{(R)u0, (R)u1, (R)u2, xs.w};
     a.v[p] = V4{(R)vi.x, (R)vi.y, (R)vi.z, R(0)};
     a.f[p] = V4{(R)fi.x, (R)fi.y, (R)fi.z, R(0)};
     a.p[p] = V4{(R)pi.x, (R)pi.y, (R)pi.z, R(0)};
@@ -1326,6 +1437,8 @@ struct Fast {
     DBuf<GridBar> gbar;   // persistent-chunk barrier state
     DBuf<int32_t> serr;   // staged kernels: a staging copy timed out
     DBuf<R> rtd;          // elasto-plastic: 1/sqrt(td_norm2) per particle
+    DBuf<int32_t> geo_off;  // uniform-geometry slices: slot table offsets
+    DBuf<V4> geo;           // (xi, |xi|) per slot of those slices
     DBuf<int32_t> partner;  // elasto-plastic: reverse-bond slot per slot
     bool persisted = false;
     int cur = 0;
@@ -1513,6 +1626,10 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.cnt = env->cnt.p;
     a.nbr = env->nbr.p;
     a.si = env->sinfo.p;
+    if (!std::getenv("PD_NO_UNIFORM_GEOMETRY") && F.geo_off.p) {
+        a.geo_off = F.geo_off.p;
+        a.geo = F.geo.p;
+    }
     a.splan_off = env->splan_off.p;
     a.splan = env->splan.p;
     a.spos = env->spos.p;
@@ -1598,6 +1715,19 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         PD_TRY(F.mab.alloc(N));
         PD_TRY(F.bcbits.alloc(N));
         // parameters in the working precision
+        if (env->uniform_slices > 0) {  // slot tables of the uniform-geometry slices, in R
+            std::vector<typename Tr<R>::V4> g(env->geo_h.size());
+            for (size_t i = 0; i < g.size(); ++i) {
+                const double4 &h = env->geo_h[i];
+                g[i] = typename Tr<R>::V4{(R)h.x, (R)h.y, (R)h.z, (R)h.w};
+            }
+            PD_TRY(F.geo.alloc(g.size()));
+            PD_TRY(F.geo_off.alloc(env->geo_off_h.size()));
+            CK(cudaMemcpyAsync(F.geo.p, g.data(), g.size() * sizeof(g[0]), cudaMemcpyHostToDevice, env->st));
+            CK(cudaMemcpyAsync(F.geo_off.p, env->geo_off_h.data(), env->geo_off_h.size() * 4,
+                               cudaMemcpyHostToDevice, env->st));
+            CK(cudaStreamSynchronize(env->st));
+        }
         std::vector<FBlock<R>> fb;
         std::vector<FPair<R>> fp;
         for (const auto &b : env->hb) {

@@ -246,11 +246,12 @@ class GeneralEnvironment:
         return flags.astype(bool)
 
     def layout(self):
-        """Bond storage: slices, stencil slices, bond slots, index entries."""
-        out = np.zeros(4, dtype=np.int64)
-        _abi.check(_abi.lib().pd_env_layout(self._h, _abi.i64ptr(out)))
+        """Bond storage: slices, stencil slices, bond slots, index entries,
+        uniform-geometry slices, slices with a record staging plan."""
+        out = np.zeros(6, dtype=np.int64)
+        _abi.check(_abi.lib().pd_env_layout_stats(self._h, _abi.i64ptr(out), 6))
         return {"slices": int(out[0]), "stencil_slices": int(out[1]), "slots": int(out[2]),
-                "index_entries": int(out[3])}
+                "index_entries": int(out[3]), "uniform_slices": int(out[4]), "staged_slices": int(out[5])}
 
 
 def Env(id, materials, short_range_contact, boundary_conds, dt, state=2, bskin=0.5, units=False, **kwargs):
