@@ -264,10 +264,7 @@ PD_API pd_status pd_env_check_finite(pd_env *env);
  * environment at finalize disables the stencil form. */
 PD_API pd_status pd_env_layout(const pd_env *env, int64_t *out4);
 /* The same and more (extension): out[0..3] as pd_env_layout, out[4] =
- * stencil slices of uniform geometry (every lane sees the same reference
- * bond vector per slot, as on an exact lattice: the throughput kernels take
- * it from a per-slot table and load only the neighbour's displacement),
- * out[5] = slices with a record staging plan.  Writes min(n, 6) values. */
+ * slices with a record staging plan.  Writes min(n, 5) values. */
 PD_API pd_status pd_env_layout_stats(const pd_env *env, int64_t *out, int64_t n);
 
 /* ---------------------------------------------------------------------- */

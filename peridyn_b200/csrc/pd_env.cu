@@ -485,8 +485,7 @@ extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block
 // others keep the explicit indices.  cnt becomes the number of slots to scan.
 // ---------------------------------------------------------------------
 static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &slice_ptr, std::vector<int32_t> &cnt,
-                                      const std::vector<int32_t> &nbr_b, const std::vector<uint32_t> &w_b,
-                                      const std::vector<double4> &x4) {
+                                      const std::vector<int32_t> &nbr_b, const std::vector<uint32_t> &w_b) {
     const int64_t N = env->N, S = N / kSlice;
     const char *lay = std::getenv("PD_FAMILY_LAYOUT");
     const bool force_explicit = lay && std::strcmp(lay, "explicit") == 0;
@@ -596,61 +595,6 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
             pl.insert(pl.end(), rs.begin(), rs.end());
         }
     });
-    // pass 4 (per stencil slice): uniform geometry.  Slot j is uniform when
-    // every lane holding it as a family member sees the same reference bond
-    // vector x_q - x_p (to 1e-9 relative: an exact lattice, not a jittered
-    // one); a slice is uniform when all its slots are.
-    std::vector<uint8_t> ug(S, 0);
-    parallel_for(S, [&](int64_t s0, int64_t s1) {
-        for (int64_t s = s0; s < s1; ++s) {
-            const SliceInfo &d = si[s];
-            if (d.mode != kStencil || force_explicit) continue;
-            const std::vector<int32_t> &u = uni[s];
-            bool uniform = true;
-            for (size_t j = 0; uniform && j < u.size(); ++j) {
-                bool have = false;
-                double r0 = 0, r1 = 0, r2 = 0;
-                for (int l = 0; l < kSlice; ++l) {
-                    const int64_t p = s * kSlice + l;
-                    if (!((fam[d.word + 32 * (int64_t)(j >> 5) + l] >> (j & 31)) & 1u)) continue;
-                    const int64_t q = p + u[j];
-                    const double e0 = x4[q].x - x4[p].x, e1 = x4[q].y - x4[p].y, e2 = x4[q].z - x4[p].z;
-                    if (!have) {
-                        r0 = e0, r1 = e1, r2 = e2;
-                        have = true;
-                        continue;
-                    }
-                    const double tol = 1e-9 * std::sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-                    if (std::fabs(e0 - r0) > tol || std::fabs(e1 - r1) > tol || std::fabs(e2 - r2) > tol)
-                        uniform = false;
-                }
-            }
-            ug[s] = uniform;
-        }
-    });
-    env->geo_off_h.assign(S + 1, -1);
-    env->geo_h.clear();
-    env->uniform_slices = 0;
-    for (int64_t s = 0; s < S; ++s) {
-        if (!ug[s]) continue;
-        const SliceInfo &d = si[s];
-        const std::vector<int32_t> &u = uni[s];
-        env->geo_off_h[s] = (int32_t)env->geo_h.size();
-        for (int32_t j = 0; j < d.len; ++j) {
-            double4 g = make_double4(1.0, 0.0, 0.0, 1.0);  // slots no lane holds: any finite vector
-            if (j < (int32_t)u.size())
-                for (int l = 0; l < kSlice; ++l) {
-                    const int64_t p = s * kSlice + l;
-                    if (!((fam[d.word + 32 * (int64_t)(j >> 5) + l] >> (j & 31)) & 1u)) continue;
-                    const int64_t q = p + u[j];
-                    const double e0 = x4[q].x - x4[p].x, e1 = x4[q].y - x4[p].y, e2 = x4[q].z - x4[p].z;
-                    g = make_double4(e0, e1, e2, std::sqrt(e0 * e0 + e1 * e1 + e2 * e2));
-                    break;
-                }
-            env->geo_h.push_back(g);
-        }
-        ++env->uniform_slices;
-    }
     std::vector<int32_t> splan_off(S + 1, -1), splan;
     int64_t nplan = 0, pmax = 0;
     for (int64_t s = 0; s < S; ++s) {
@@ -984,7 +928,7 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         }
     }
     // Runtime layout (stencil or explicit per slice), uploaded.
-    PD_TRY(build_runtime_layout(env, slice_ptr, cnt, nbr_b, w_b, x4));
+    PD_TRY(build_runtime_layout(env, slice_ptr, cnt, nbr_b, w_b));
     nbr_b.clear();
     nbr_b.shrink_to_fit();
     w_b.clear();
@@ -1327,9 +1271,8 @@ extern "C" pd_status pd_env_layout(const pd_env *env, int64_t *out4) {
 extern "C" pd_status pd_env_layout_stats(const pd_env *env, int64_t *out, int64_t n) {
     PD_TRY(need_final(env));
     if (!out || n < 0) return fail(PD_ERR_ARG, "out is NULL or n < 0");
-    const int64_t v[6] = {env->N / kSlice, env->stencil_slices, env->nnz, env->nbr_len, env->uniform_slices,
-                          env->splan_slices};
-    for (int64_t i = 0; i < n && i < 6; ++i) out[i] = v[i];
+    const int64_t v[5] = {env->N / kSlice, env->stencil_slices, env->nnz, env->nbr_len, env->splan_slices};
+    for (int64_t i = 0; i < n && i < 5; ++i) out[i] = v[i];
     return PD_OK;
 }
 

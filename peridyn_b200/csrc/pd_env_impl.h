@@ -163,13 +163,6 @@ struct pd_env {
     // (first record, count) per range}.  spos[i] = staged position of lane
     // 0's record of the stencil slot stored at nbr[i].
     int64_t splan_slices = 0, splan_max = 0;
-    // Uniform-geometry stencil slices (exact lattices): every lane that has
-    // slot j in its family sees the same reference bond vector, kept once
-    // per slot as (xi, |xi|) at geo_h[geo_off[s] + j]; geo_off[s] = -1 for
-    // the other slices.
-    std::vector<int32_t> geo_off_h;
-    std::vector<double4> geo_h;
-    int64_t uniform_slices = 0;
 
     pd::DBuf<int64_t> map;
     pd::DBuf<double4> x4, y, v, f, p;

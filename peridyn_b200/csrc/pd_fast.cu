@@ -73,14 +73,6 @@ struct Tr<float> {
                          : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w)
                          : "l"(r));
     }
-    // The displacement half of a record alone (u, w): uniform-geometry
-    // slices take the reference bond vector from their slot table.
-    template <bool NC = true>
-    static __device__ __forceinline__ void load_u_rec(const float4 *r, float4 &u) {
-        if (NC) asm("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w) : "l"(r));
-        else
-            asm volatile("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(u.x), "=f"(u.y), "=f"(u.z), "=f"(u.w) : "l"(r));
-    }
 };
 template <>
 struct Tr<double> {
@@ -102,13 +94,6 @@ struct Tr<double> {
             asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w)
                          : "l"(r + 1));
         }
-    }
-    template <bool NC = true>
-    static __device__ __forceinline__ void load_u_rec(const double4 *r, double4 &u) {
-        if (NC) asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w) : "l"(r));
-        else
-            asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(u.x), "=d"(u.y), "=d"(u.z), "=d"(u.w)
-                         : "l"(r));
     }
 };
 
@@ -146,7 +131,7 @@ struct StepArgs {
     // xu[2i] = (x, w) (FP32C: relative to the block centre; identical in
     // both buffers), xu[2i+1] = (u, w) displacement; w = the volume (times
     // c in bond-based blocks) in both halves.  One address per neighbour
-    // fetches both; uniform-geometry walks read the (u, w) half alone.
+    // fetches both.
     const typename Tr<R>::V4 *xu;
     typename Tr<R>::V4 *xn;  // next-step buffer (only the u records are written)
     double *ax, *ay, *az;    // FP64 displacement accumulator (FP32C)
@@ -155,9 +140,6 @@ struct StepArgs {
     typename Tr<R>::V2 *mab;  // (theta/m, 1/m) of state-based particles
     const int32_t *tinfo, *cnt, *nbr;
     const SliceInfo *si;
-    // uniform-geometry slices: slot table (xi, |xi|) from geo[geo_off[s]]
-    const int32_t *geo_off;
-    const typename Tr<R>::V4 *geo;
     // record staging plans (FP32C staged kernels): see pd_env
     const int32_t *splan_off, *splan, *spos;
     int32_t *serr;        // set when a staging copy did not land in time
@@ -294,16 +276,6 @@ __device__ __forceinline__ bool last_arrival_sum(R (*sh)[NC][32], int *arrive, i
 template <class R>
 struct Kin {
     R Y0, Y1, Y2, xx2, num;
-    __device__ __forceinline__ Kin(const typename Tr<R>::V4 &g, const typename Tr<R>::V4 &uq,
-                                   const typename Tr<R>::V4 &nu) {
-        const R x0 = g.x, x1 = g.y, x2 = g.z;
-        const R e0 = uq.x + nu.x, e1 = uq.y + nu.y, e2 = uq.z + nu.z;
-        Y0 = x0 + e0;
-        Y1 = x1 + e1;
-        Y2 = x2 + e2;
-        xx2 = g.w * g.w;
-        num = Tr<R>::fma_(e2, x2 + Y2, Tr<R>::fma_(e1, x1 + Y1, e0 * (x0 + Y0)));
-    }
     // f += c Y
     __device__ __forceinline__ void accumulate(R c, R &fx, R &fy, R &fz) const {
         fx = Tr<R>::fma_(c, Y0, fx);
@@ -324,20 +296,6 @@ struct Kin {
 // FP32: the (x, y) components as packed f32x2 operations.
 template <>
 struct Kin<float> {
-    // from the slot table: g = (xi, |xi|), so |xi|^2 = |xi| |xi|
-    __device__ __forceinline__ Kin(const float4 &g, const float4 &uq, const float4 &nu) {
-        const float2 d = make_float2(g.x, g.y);
-        const float2 e = __fadd2_rn(make_float2(uq.x, uq.y), make_float2(nu.x, nu.y));
-        const float dz = g.z, ez = uq.z + nu.z;
-        const float2 Y = __fadd2_rn(d, e);
-        const float Yz = dz + ez;
-        const float2 S = __fadd2_rn(d, Y);
-        const float2 es = __fmul2_rn(e, S);
-        xx2 = g.w * g.w;
-        num = fmaf(ez, dz + Yz, es.x + es.y);
-        Yxy = Y;
-        Y2 = Yz;
-    }
     float2 Yxy;
     float Y2, xx2, num;
     __device__ __forceinline__ void accumulate(float c, float2 &fxy, float &fz) const {
@@ -362,16 +320,12 @@ struct Kin<float> {
 
 // STG: the neighbour records come from the block's staged copy in shared
 // memory (stg, lane 0's record of slot k at sp[k]) instead of global memory.
-// UG: a uniform-geometry stencil slice: the reference bond vector and its
-// length come from the slot table (gp[k]) and only the neighbour's (u, w)
-// half-record is loaded.
-template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false,
-          bool UG = false>
+template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                           uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
                                           typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz,
                                           const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
-                                          R rtdp = R(0), const typename Tr<R>::V4 *gp = nullptr) {
+                                          R rtdp = R(0)) {
     using V4 = typename Tr<R>::V4;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -395,7 +349,6 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
         // stencil slots point at an in-range record and carry a 0 bit.
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         const int32_t *spp = STG ? sp + w0 : nullptr;
-        const V4 *gpp = UG ? gp + w0 : nullptr;
         // elasto-plastic: per-slot state index of the chunk's first slot
         const int64_t ebase = KIND == PD_MAT_ELASTO_PLASTIC ? ((int64_t)(wptr - a.words) << 5) + (w0 & 31) : 0;
         uint32_t okm = 0, bit = 1u;  // okm: slots within the critical stretch
@@ -405,19 +358,16 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
             V4 xq, uq;
             if constexpr (STG) {
                 const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
-                xq = UG ? gpp[j] : stg[2 * r];
+                xq = stg[2 * r];
                 uq = stg[2 * r + 1];
-            } else if constexpr (UG) {
-                xq = gpp[j];  // (xi, |xi|)
-                Tr<R>::template load_u_rec<NC>(a.xu + 2 * (int64_t)q + 1, uq);
             } else {
                 Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             }
-            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
+            const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
-            const R wq = UG ? uq.w : xq.w;  // V_q (c V_q in bond-based blocks)
+            const R wq = xq.w;  // V_q (c V_q in bond-based blocks)
             // stretch s = num / dl;  |Y|^2 = |xi|^2 + num
-            const R lx = UG ? xq.w : Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
             const R dl = Tr<R>::fma_(ly, lx, xx2);  // (|Y| + |xi|) |xi|
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
@@ -484,34 +434,6 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         Bp = m.y;
     }
     if (KIND == PD_MAT_ELASTO_PLASTIC) rtdp = a.rtd[p];
-    const int32_t goff = (a.geo_off && d.mode == kStencil) ? a.geo_off[p >> 5] : -1;
-    if constexpr (STG) {
-        if (stg && goff >= 0) {  // staged records, uniform geometry
-            const int32_t *sp = a.spos + d.nbr;
-            const typename Tr<R>::V4 *gp = a.geo + goff;
-            if (B.nt > 1)
-                bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp,
-                                                                           xp, up, Ap, Bp, fx, fy, fz, stg, sp, rtdp,
-                                                                           gp);
-            else
-                bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp,
-                                                                            xp, up, Ap, Bp, fx, fy, fz, stg, sp, rtdp,
-                                                                            gp);
-            return;
-        }
-    }
-    if (goff >= 0 && !(STG && stg)) {
-        const typename Tr<R>::V4 *gp = a.geo + goff;
-        if (B.nt > 1)
-            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
-                                                                            up, Ap, Bp, fx, fy, fz, nullptr, nullptr,
-                                                                            rtdp, gp);
-        else
-            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
-                                                                             up, Ap, Bp, fx, fy, fz, nullptr, nullptr,
-                                                                             rtdp, gp);
-        return;
-    }
     if constexpr (STG) {
         if (stg) {  // a staged slice is a stencil slice
             const int32_t *sp = a.spos + d.nbr;
@@ -781,11 +703,10 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     store_u(a, p, u0, u1, u2);
 }
 
-template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false, bool UG = false>
+template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false>
 __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
                                         const uint32_t *wp, typename Tr<R>::V4 xp, typename Tr<R>::V4 up,
-                                        const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
-                                        const typename Tr<R>::V4 *gp = nullptr) {
+                                        const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr) {
     using V4 = typename Tr<R>::V4;
     R acc = 0;
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -796,27 +717,22 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t
         if (!bits) continue;
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
         const int32_t *spp = STG ? sp + w0 : nullptr;
-        const V4 *gpp = UG ? gp + w0 : nullptr;
         uint32_t bit = 1u;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             V4 xq, uq;
             if constexpr (STG) {
                 const int32_t r = __ldg(spp + j) + (int32_t)(p & 31);
-                xq = UG ? gpp[j] : stg[2 * r];
+                xq = stg[2 * r];
                 uq = stg[2 * r + 1];
-            } else if constexpr (UG) {
-                const int32_t q = slot_neighbour<ST>(np, j, p);
-                xq = gpp[j];
-                Tr<R>::template load_u_rec<NC>(a.xu + 2 * (int64_t)q + 1, uq);
             } else {
                 const int32_t q = slot_neighbour<ST>(np, j, p);
                 Tr<R>::template load_rec<NC>(a.xu + 2 * (int64_t)q, xq, uq);
             }
-            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
+            const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num;
-            const R lx = UG ? xq.w : Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
-            const R term = num * (UG ? uq.w : xq.w) * Tr<R>::rcp(ly + lx);
+            const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
+            const R term = num * xq.w * Tr<R>::rcp(ly + lx);
             acc += (bits & bit) ? term : R(0);
         }
     }
@@ -846,16 +762,9 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, int64_t blk, R 
         warp_range<WPS>(d.len, w, k0, k1);
         k1 = min(k1, a.cnt[p]);
         const uint32_t *wp = a.words + d.word + (p & 31);
-        const int32_t goff = (a.geo_off && d.mode == kStencil) ? a.geo_off[p >> 5] : -1;
-        if (STG && stg && goff >= 0)
-            acc = theta_walk<R, WPS, U, true, NC, true, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
-                                                              a.spos + d.nbr, a.geo + goff);
-        else if (STG && stg)
+        if (STG && stg)
             acc = theta_walk<R, WPS, U, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
                                                         a.spos + d.nbr);
-        else if (goff >= 0)
-            acc = theta_walk<R, WPS, U, true, NC, false, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, nullptr,
-                                                               nullptr, a.geo + goff);
         else if (d.mode == kStencil)
             acc = theta_walk<R, WPS, U, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up);
         else
@@ -889,11 +798,10 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
 // (td_trial^2 exceeds the FP32 range in SI units); stored as
 // 1/sqrt(td_norm2) in the working precision.
 // ---------------------------------------------------------------------
-template <class R, int U, bool ST, bool MULTI, bool UG = false>
+template <class R, int U, bool ST, bool MULTI>
 __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1,
                                           const int32_t *nb, uint32_t *wp, const FBlock<R> &B, int tp,
-                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp,
-                                          const typename Tr<R>::V4 *gp = nullptr) {
+                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp) {
     using V4 = typename Tr<R>::V4;
     FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
@@ -905,22 +813,16 @@ __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32
         const uint32_t bits = range_bits(*wptr, w0, kend);
         if (!bits) continue;
         const int32_t *np = nb + (ST ? 1 : 32) * w0;
-        const V4 *gpp = UG ? gp + w0 : nullptr;
         const int64_t ebase = ((int64_t)(wptr - a.words) << 5) + (w0 & 31);
         uint32_t okm = 0, bit = 1u;
 #pragma unroll U
         for (int32_t j = 0; j < kend; ++j, bit <<= 1) {
             const int32_t q = slot_neighbour<ST>(np, j, p);
             V4 xq, uq;
-            if constexpr (UG) {
-                xq = gpp[j];
-                Tr<R>::template load_u_rec<true>(a.xu + 2 * (int64_t)q + 1, uq);
-            } else {
-                Tr<R>::template load_rec<true>(a.xu + 2 * (int64_t)q, xq, uq);
-            }
-            const Kin<R> k = UG ? Kin<R>(xq, uq, nu) : Kin<R>(xq, uq, nx, nu);
+            Tr<R>::template load_rec<true>(a.xu + 2 * (int64_t)q, xq, uq);
+            const Kin<R> k(xq, uq, nx, nu);
             const R num = k.num, xx2 = k.xx2;
-            const R lx = UG ? xq.w : Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+            const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
             const R dl = Tr<R>::fma_(ly, lx, xx2);
             const bool live = (bits & bit) != 0u;
             if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[q] & 255) * B.nt];
@@ -930,7 +832,7 @@ __device__ __forceinline__ double td_walk(const StepArgs<R> &a, int64_t p, int32
             const R As = Ap + mq.x, Bs = Bp + mq.y;
             const R ed = Tr<R>::fma_(-As * Tr<R>::rcp(Bs), lx * R(1.0 / 3.0), num * Tr<R>::rcp(ly + lx));
             const R tdt = pp.g15 * Tr<R>::rcp(lx) * Bs * (ed - (R)a.edp_in[ebase + j]);
-            const double t2 = (double)tdt * (double)tdt * (double)(UG ? uq.w : xq.w);
+            const double t2 = (double)tdt * (double)tdt * (double)xq.w;
             acc += (live && ok) ? t2 : 0.0;
         }
         const uint32_t brk = bits & ~okm;
@@ -962,12 +864,7 @@ __device__ __forceinline__ void td_body(const StepArgs<R> &a, int64_t blk, doubl
         const typename Tr<R>::V2 m = a.mab[p];
         const bool st = d.mode == kStencil;
         const int32_t *nb = a.nbr + d.nbr + (st ? 0 : (p & 31));
-        const int32_t goff = (a.geo_off && st) ? a.geo_off[p >> 5] : -1;
-        if (goff >= 0) {
-            acc = B.nt > 1 ? td_walk<R, U, true, true, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y, a.geo + goff)
-                           : td_walk<R, U, true, false, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y,
-                                                              a.geo + goff);
-        } else if (B.nt > 1) {
+        if (B.nt > 1) {
             acc = st ? td_walk<R, U, true, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y)
                      : td_walk<R, U, false, true>(a, p, k0, k1, nb, wp, B, tp, xp, up, m.x, m.y);
         } else {
@@ -1437,8 +1334,6 @@ struct Fast {
     DBuf<GridBar> gbar;   // persistent-chunk barrier state
     DBuf<int32_t> serr;   // staged kernels: a staging copy timed out
     DBuf<R> rtd;          // elasto-plastic: 1/sqrt(td_norm2) per particle
-    DBuf<int32_t> geo_off;  // uniform-geometry slices: slot table offsets
-    DBuf<V4> geo;           // (xi, |xi|) per slot of those slices
     DBuf<int32_t> partner;  // elasto-plastic: reverse-bond slot per slot
     bool persisted = false;
     int cur = 0;
@@ -1626,10 +1521,6 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.cnt = env->cnt.p;
     a.nbr = env->nbr.p;
     a.si = env->sinfo.p;
-    if (!std::getenv("PD_NO_UNIFORM_GEOMETRY") && F.geo_off.p) {
-        a.geo_off = F.geo_off.p;
-        a.geo = F.geo.p;
-    }
     a.splan_off = env->splan_off.p;
     a.splan = env->splan.p;
     a.spos = env->spos.p;
@@ -1715,19 +1606,6 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         PD_TRY(F.mab.alloc(N));
         PD_TRY(F.bcbits.alloc(N));
         // parameters in the working precision
-        if (env->uniform_slices > 0) {  // slot tables of the uniform-geometry slices, in R
-            std::vector<typename Tr<R>::V4> g(env->geo_h.size());
-            for (size_t i = 0; i < g.size(); ++i) {
-                const double4 &h = env->geo_h[i];
-                g[i] = typename Tr<R>::V4{(R)h.x, (R)h.y, (R)h.z, (R)h.w};
-            }
-            PD_TRY(F.geo.alloc(g.size()));
-            PD_TRY(F.geo_off.alloc(env->geo_off_h.size()));
-            CK(cudaMemcpyAsync(F.geo.p, g.data(), g.size() * sizeof(g[0]), cudaMemcpyHostToDevice, env->st));
-            CK(cudaMemcpyAsync(F.geo_off.p, env->geo_off_h.data(), env->geo_off_h.size() * 4,
-                               cudaMemcpyHostToDevice, env->st));
-            CK(cudaStreamSynchronize(env->st));
-        }
         std::vector<FBlock<R>> fb;
         std::vector<FPair<R>> fp;
         for (const auto &b : env->hb) {

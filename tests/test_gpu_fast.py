@@ -393,30 +393,3 @@ def test_elasto_plastic_fast_graphs_match_direct(precision, monkeypatch):
         assert np.array_equal(a, b)
     assert np.array_equal(i1, i2)
     assert np.array_equal(e1, e2)
-
-
-@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-def test_uniform_geometry_slices(oracle, precision, monkeypatch):
-    """Exact lattices store one reference bond vector per stencil slot; the
-    walks then load only the neighbour's displacement half-record.  Same
-    tolerance against the oracle as the general walk, and agreement with
-    it; jittered lattices keep the general walk."""
-    w = configs.lps_bar(nx=40, ny=10, nz=10)
-    env, ora = _run_pair(oracle, w, precision, 300)
-    lay = env.layout()
-    assert lay["uniform_slices"] > 0.9 * lay["stencil_slices"]
-    eu, ev, mism = _errors(env, ora)
-    assert eu <= TOL[precision], eu
-    assert mism == 0
-    y1 = env.get_state()[0]
-    env.close()
-    monkeypatch.setenv("PD_NO_UNIFORM_GEOMETRY", "1")
-    env2, _ = _run_pair(oracle, w, precision, 300)
-    y2 = env2.get_state()[0]
-    x = np.hstack([B.x for B in ora.blocks])
-    assert rel_l2(y1 - x, y2 - x) <= TOL[precision]
-    env2.close()
-    jit = configs.pmb_cube(n=10)
-    env3 = pb.Env(1, jit["materials"], [], [], jit["dt"], precision=precision)
-    assert env3.layout()["uniform_slices"] == 0
-    env3.close()
