@@ -1801,13 +1801,15 @@ void launch_force(pd_env *env, cudaStream_t st, int cfg, const StepArgs<R> &a, b
     if (a.ep) env->ecur = 1 - env->ecur;
 }
 
-// Project autotuner: times the force (and dilatation) kernels for every
-// warps-per-slice split on the environment itself -- force written to a
-// scratch array, no bond breaking, every block treated as deformed -- and
-// keeps the fastest.  Results are cached per (particles, bonds, precision,
-// state-based) for the life of the process.
+// Project autotuner: times every kernel shape on the environment itself
+// (captured graphs of full steps on scratch copies of the state they
+// write) and keeps the fastest.  Results are cached for the life of the
+// process per problem class: particle count in steps of 2^(1/2) (~41 %),
+// bond slots per particle in steps of 8, precision and staging mode, and
+// the passes present (dilatation, td_norm2), so a stream of jobs of
+// similar sizes -- the serving loop -- tunes once per class.
 std::mutex g_tune_mutex;
-std::map<std::tuple<int64_t, int64_t, int, bool>, int> g_tune_cache;
+std::map<std::tuple<int64_t, int64_t, int, int>, int> g_tune_cache;
 
 template <class R>
 pd_status autotune(pd_env *env, Fast<R> &F) {
@@ -1822,7 +1824,10 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
         return PD_OK;
     }
     const bool lps = need_theta(env);
-    const auto key = std::make_tuple(env->N, env->nnz, env->precision * 4 + env->staging + 1, lps);
+    const int64_t size_class = (int64_t)std::floor(2.0 * std::log2((double)std::max<int64_t>(env->N, 1)));
+    const int64_t slot_class = env->nnz / std::max<int64_t>(env->N, 1) / 8;
+    const auto key = std::make_tuple(size_class, slot_class, env->precision * 4 + env->staging + 1,
+                                     (int)lps + 2 * (int)ep);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(key);
@@ -1898,9 +1903,10 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
             if (env->staging >= 1 && staged_ok(wps)) shapes.push_back(100 + 10 * wps + u);
         }
     // Each shape runs as the stepping loop does: a captured graph of
-    // kTuneSteps steps, replayed once to warm up and then timed in three
-    // sweeps over the shapes, best of the three per shape.
-    constexpr int kTuneSteps = 12;
+    // kTuneSteps steps (fewer for large problems, whose steps are long
+    // enough to time), replayed once to warm up and then timed in two
+    // sweeps over the shapes, best of the two per shape.
+    const int kTuneSteps = N > 200000 ? 3 : N > 50000 ? 6 : 12;
     std::vector<cudaGraphExec_t> ex(shapes.size(), nullptr);
     auto release = [&] {
         for (auto &g : ex)
@@ -1928,7 +1934,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
         }
     }
     std::vector<float> t(shapes.size(), 1e30f);
-    for (int sweep = 0; sweep < 3; ++sweep)
+    for (int sweep = 0; sweep < 2; ++sweep)
         for (size_t i = 0; i < shapes.size(); ++i) {
             cudaEventRecord(e0, env->st);
             cudaGraphLaunch(ex[i], env->st);
