@@ -267,6 +267,22 @@ PD_API pd_status pd_env_layout(const pd_env *env, int64_t *out4);
  * slices with a record staging plan.  Writes min(n, 5) values. */
 PD_API pd_status pd_env_layout_stats(const pd_env *env, int64_t *out, int64_t n);
 
+/* Halo exchange of a slab decomposition of one specimen (extension: the
+ * multi-GPU plan of a single large body; the reference runs one body on
+ * one device).  idx: n environment-order particle indices, buf: 9 n
+ * doubles, both in device memory of the environment's GPU.  Pack writes,
+ * per particle, q (y in PD_PREC_FP64_SERIAL, the FP64 displacement u in
+ * the throughput modes), v and f; unpack writes them into the listed
+ * particles of another environment of the same precision, between steps.
+ * Both enqueue on the environment's stream and return without waiting. */
+PD_API pd_status pd_env_pack_halo(pd_env *env, const int64_t *idx, int64_t n, double *buf);
+PD_API pd_status pd_env_unpack_halo(pd_env *env, const int64_t *idx, int64_t n, const double *buf);
+/* Sets the per-block deformed flags of the general_material.jl:240-256
+ * gate (extension).  hold != 0: the library no longer evaluates the gate
+ * itself; the flags stay as set (slabs of one body: a gate decided on one
+ * slab's particles would differ from the whole body's). */
+PD_API pd_status pd_env_set_deformed(pd_env *env, const uint8_t *flags, int32_t hold);
+
 /* ---------------------------------------------------------------------- */
 /* Device-pointer entry point for a single block                           */
 /* ---------------------------------------------------------------------- */

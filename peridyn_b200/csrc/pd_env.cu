@@ -1159,6 +1159,20 @@ extern "C" pd_status pd_env_reset_deformed(pd_env *env) {
     return PD_OK;
 }
 
+extern "C" pd_status pd_env_set_deformed(pd_env *env, const uint8_t *flags, int32_t hold) {
+    PD_TRY(need_final(env));
+    if (!flags) return fail(PD_ERR_ARG, "flags is NULL");
+    CK(cudaSetDevice(env->device));
+    PD_TRY(pd::fast_land_flags(env));
+    std::vector<int32_t> h(env->hb.size());
+    for (size_t b = 0; b < h.size(); ++b) h[b] = flags[b] ? 1 : 0;
+    CK(cudaMemcpyAsync(env->deformed.p, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    env->deformed_h.assign(h.begin(), h.end());
+    env->gate_hold = hold != 0;
+    return PD_OK;
+}
+
 extern "C" pd_status pd_env_reset_bonds(pd_env *env) {
     PD_TRY(need_final(env));
     CK(cudaSetDevice(env->device));

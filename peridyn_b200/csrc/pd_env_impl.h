@@ -216,6 +216,7 @@ struct pd_env {
     bool fast_valid = false;
     void *fast = nullptr;
     int shape = 0;  // fixed kernel shape 10 * warps_per_slice + unroll, 0 = autotune
+    bool gate_hold = false;  // pd_env_set_deformed(..., hold): the library does not evaluate the gate
     int staging = 0;  // record staging: 0 = none, 1 = staged shapes, 2 = the autotuner decides
 
     pd::Geo geo() const;

@@ -1682,7 +1682,7 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
 template <class R>
 pd_status gate_prepare(pd_env *env, Fast<R> &F) {
     std::vector<GateItem> items;
-    for (size_t b = 0; b < env->hb.size(); ++b) {
+    for (size_t b = 0; b < env->hb.size() && !env->gate_hold; ++b) {
         const HostBlock &hb = env->hb[b];
         if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
         items.push_back(GateItem{hb.first_int, hb.n, (int32_t)b, 0});
@@ -2479,5 +2479,121 @@ extern "C" pd_status pd_env_record_staging(pd_env *env, int32_t *staged, int64_t
     if (staged) *staged = cfg >= 100;
     if (slices) *slices = env->splan_slices;
     if (max_records) *max_records = env->splan_max;
+    return PD_OK;
+}
+
+// ---------------------------------------------------------------------
+// Halo exchange of a slab decomposition (peridyn_b200/slabs.py): the live
+// state of listed particles packed as 9 doubles each -- q (the position y
+// in the serial mode, the FP64 displacement u in the throughput modes,
+// which the receiving slab holds in the same form), velocity, force --
+// and unpacked into another environment's particles.  Copies of the same
+// numbers, so a ghost continues exactly as its owner.
+// ---------------------------------------------------------------------
+namespace pd {
+namespace {
+
+template <class R>
+__global__ void k_pack_fast(StepArgs<R> a, const int64_t *map, const int64_t *idx, int64_t n, double *buf) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t p = map[idx[i]];
+    double u0, u1, u2;
+    load_u(a, p, u0, u1, u2);
+    const typename Tr<R>::V4 v = a.v[p], f = a.f[p];
+    double *o = buf + 9 * i;
+    o[0] = u0, o[1] = u1, o[2] = u2;
+    o[3] = (double)v.x, o[4] = (double)v.y, o[5] = (double)v.z;
+    o[6] = (double)f.x, o[7] = (double)f.y, o[8] = (double)f.z;
+}
+
+template <class R>
+__global__ void k_unpack_fast(StepArgs<R> a, const int64_t *map, const int64_t *idx, int64_t n, const double *buf) {
+    using V4 = typename Tr<R>::V4;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t p = map[idx[i]];
+    const double *o = buf + 9 * i;
+    if (sizeof(R) == 4) {  // FP32C: the FP64 accumulator is the state; records follow at the next step
+        a.ax[p] = o[0];
+        a.ay[p] = o[1];
+        a.az[p] = o[2];
+    } else {  // FP64: the current record holds u
+        V4 *cur = const_cast<V4 *>(a.xu);
+        cur[2 * p + 1] = V4{(R)o[0], (R)o[1], (R)o[2], cur[2 * p].w};
+    }
+    a.v[p] = V4{(R)o[3], (R)o[4], (R)o[5], R(0)};
+    a.f[p] = V4{(R)o[6], (R)o[7], (R)o[8], R(0)};
+}
+
+__global__ void k_pack_fp64(const double4 *y, const double4 *v, const double4 *f, const int64_t *map,
+                            const int64_t *idx, int64_t n, double *buf) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t p = map[idx[i]];
+    const double4 a = y[p], b = v[p], c = f[p];
+    double *o = buf + 9 * i;
+    o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = b.x, o[4] = b.y, o[5] = b.z, o[6] = c.x, o[7] = c.y, o[8] = c.z;
+}
+
+__global__ void k_unpack_fp64(double4 *y, double4 *v, double4 *f, const int64_t *map, const int64_t *idx, int64_t n,
+                              const double *buf) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t p = map[idx[i]];
+    const double *o = buf + 9 * i;
+    y[p] = make_double4(o[0], o[1], o[2], 0.0);
+    v[p] = make_double4(o[3], o[4], o[5], 0.0);
+    f[p] = make_double4(o[6], o[7], o[8], 0.0);
+}
+
+pd_status halo_check(pd_env *env, const int64_t *idx, int64_t n, const void *buf) {
+    if (!env) return fail(PD_ERR_ARG, "environment handle is NULL");
+    if (!env->finalized) return fail(PD_ERR_STATE, "environment is not finalized (call pd_env_finalize)");
+    if (n < 0) return fail(PD_ERR_ARG, "n < 0");
+    if (n > 0 && (!idx || !buf)) return fail(PD_ERR_ARG, "idx or buf is NULL");
+    CK(cudaSetDevice(env->device));
+    return PD_OK;
+}
+
+}  // namespace
+}  // namespace pd
+
+extern "C" pd_status pd_env_pack_halo(pd_env *env, const int64_t *idx, int64_t n, double *buf) {
+    using namespace pd;
+    PD_TRY(halo_check(env, idx, n, buf));
+    if (n == 0) return PD_OK;
+    FastHolder *h = holder(env);
+    const unsigned g = gridn(n, 256);
+    if (h && env->fast_valid) {
+        if (h->prec == PD_PREC_FP32C)
+            k_pack_fast<float><<<g, 256, 0, env->st>>>(args(env, h->f32), env->map.p, idx, n, buf);
+        else
+            k_pack_fast<double><<<g, 256, 0, env->st>>>(args(env, h->f64), env->map.p, idx, n, buf);
+    } else {
+        k_pack_fp64<<<g, 256, 0, env->st>>>(env->y.p, env->v.p, env->f.p, env->map.p, idx, n, buf);
+    }
+    note_launch();
+    CK(cudaGetLastError());
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_unpack_halo(pd_env *env, const int64_t *idx, int64_t n, const double *buf) {
+    using namespace pd;
+    PD_TRY(halo_check(env, idx, n, buf));
+    if (n == 0) return PD_OK;
+    FastHolder *h = holder(env);
+    const unsigned g = gridn(n, 256);
+    if (h && env->fast_valid) {
+        if (h->prec == PD_PREC_FP32C)
+            k_unpack_fast<float><<<g, 256, 0, env->st>>>(args(env, h->f32), env->map.p, idx, n, buf);
+        else
+            k_unpack_fast<double><<<g, 256, 0, env->st>>>(args(env, h->f64), env->map.p, idx, n, buf);
+        h->dirty = true;  // the throughput state is now newer than the FP64 arrays
+    } else {
+        k_unpack_fp64<<<g, 256, 0, env->st>>>(env->y.p, env->v.p, env->f.p, env->map.p, idx, n, buf);
+    }
+    note_launch();
+    CK(cudaGetLastError());
     return PD_OK;
 }

@@ -185,7 +185,7 @@ pd_status update_acc_serial(pd_env *env) {
     Geo g = env->geo();
     // force_density! gate for blocks still undeformed
     std::vector<GateItem> items;
-    for (size_t b = 0; b < env->hb.size(); ++b) {
+    for (size_t b = 0; b < env->hb.size() && !env->gate_hold; ++b) {
         const HostBlock &hb = env->hb[b];
         if (hb.kind == PD_MAT_SKIP || env->deformed_h[b]) continue;
         items.push_back(GateItem{hb.first_int, hb.n, (int32_t)b, 0});

@@ -245,6 +245,14 @@ class GeneralEnvironment:
         _abi.check(_abi.lib().pd_env_deformed(self._h, _abi.u8ptr(flags)))
         return flags.astype(bool)
 
+    def set_deformed(self, flags, hold=True):
+        """Per-block deformed flags of the rigid-translation gate; with
+        ``hold`` the library stops evaluating the gate itself."""
+        f = np.ascontiguousarray(np.asarray(flags, dtype=np.uint8).reshape(-1))
+        if f.size != len(self.material_blocks):
+            raise ValueError("one flag per material block")
+        _abi.check(_abi.lib().pd_env_set_deformed(self._h, _abi.u8ptr(f), int(bool(hold))))
+
     def layout(self):
         """Bond storage: slices, stencil slices, bond slots, index entries,
         slices with a record staging plan."""

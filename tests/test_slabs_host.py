@@ -1,0 +1,131 @@
+"""Slab decomposition host logic on the CPU: ownership, ghost layers deep
+enough for complete families of owned and first-layer ghost particles,
+the halo schedule, and the point-to-point exchange with two gloo ranks."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import peridyn_b200 as pb
+from peridyn_b200 import configs, lattice
+from peridyn_b200.slabs import SlabPlan, SlabRank
+
+
+def _bar():
+    return configs.lps_bar(nx=40, ny=6, nz=5)
+
+
+def _neighbours(x, h):
+    d2 = ((x[:, :, None] - x[:, None, :]) ** 2).sum(axis=0)
+    nb = (d2 < h * h)
+    np.fill_diagonal(nb, False)
+    return nb
+
+
+@pytest.mark.parametrize("nslabs,axis", [(2, 0), (3, 0), (4, 0), (2, 1)])
+def test_plan_ownership_and_ghost_depth(nslabs, axis):
+    w = _bar()
+    m = w["materials"][0]
+    plan = SlabPlan(w["materials"], nslabs, axis=axis)
+    n = m.general.n
+    owned = np.zeros(n, dtype=np.int64)
+    for s in range(nslabs):
+        assert np.all(np.diff(plan.local[s]) > 0)  # environment order kept
+        owned[plan.local[s][plan.owned[s]]] += 1
+    assert np.all(owned == 1)
+    nb = _neighbours(m.general.x, m.general.horizon)
+    for s in range(nslabs):
+        here = np.zeros(n, dtype=bool)
+        here[plan.local[s]] = True
+        own = plan.local[s][plan.owned[s]]
+        first = np.unique(np.nonzero(nb[own])[1])
+        assert here[first].all()  # owned families complete
+        second = np.unique(np.nonzero(nb[first])[1])
+        assert here[second].all()  # first-layer ghosts' families complete
+
+
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_plan_exchanges_cover_every_ghost_once(nslabs):
+    w = _bar()
+    plan = SlabPlan(w["materials"], nslabs)
+    for s in range(nslabs):
+        ghosts = plan.local[s][~plan.owned[s]]
+        got = np.concatenate([plan.local[r][dst] for (o, r, src, dst) in plan.exchanges if r == s] or [[]])
+        assert np.array_equal(np.sort(got.astype(np.int64)), np.sort(ghosts))
+    for (o, s, src, dst) in plan.exchanges:
+        assert np.array_equal(plan.local[o][src], plan.local[s][dst])
+        assert np.all(plan.owner[plan.local[o][src]] == o)
+
+
+def test_slab_workload_restricts_masks_and_keeps_types():
+    x, vol = lattice.cuboid(20, 4, 4, 1e-3)
+    t = np.where(x[0] < 10e-3, 1, 2).astype(np.int64)
+    gen = pb.GeneralMaterial(x.copy(order="F"), np.zeros_like(x, order="F"), x, vol, t, 3.015e-3, max_neigh=200)
+    mat = pb.PeridynamicsMaterial(gen, pb.BondBasedSpecific([10e9, 11e9, 12e9], [0.01, 0.01, 0.01], [2000.0, 2100.0]))
+    bcs = [pb.FixBC(x[0] < 2e-3)]
+    plan = SlabPlan([mat], 2)
+    for s in range(2):
+        mats, sbcs = plan.slab_workload(s, [mat], bcs)
+        assert mats[0].type == mat.type
+        assert np.array_equal(sbcs[0].bool, bcs[0].bool[plan.local[s]])
+        assert mats[0].general.particle_size == gen.particle_size
+
+
+class _FakeSlab:
+    """State rows (9 values per local particle) standing for a slab's
+    environment: pack/unpack move rows by local index."""
+
+    def __init__(self, rows):
+        self.rows = rows
+
+    def pack(self, idx, buf):
+        buf.view(-1, 9)[:] = self.rows[idx]
+
+    def unpack(self, idx, buf):
+        self.rows[idx] = buf.view(-1, 9)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, nslabs, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w = _bar()
+        plan = SlabPlan(w["materials"], nslabs)
+        loc = plan.local[rank]
+        rows = torch.zeros((loc.size, 9), dtype=torch.float64)
+        own = torch.as_tensor(plan.owned[rank])
+        # owned rows carry their global index; ghost rows start at -1
+        rows[own] = torch.as_tensor(loc[plan.owned[rank]], dtype=torch.float64)[:, None] + torch.arange(9) / 10
+        rows[~own] = -1.0
+        SlabRank(plan, rank, dist, _FakeSlab(rows), device="cpu").exchange()
+        expect = torch.as_tensor(loc, dtype=torch.float64)[:, None] + torch.arange(9) / 10
+        out[rank] = bool(torch.equal(rows, expect))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_halo_exchange_gloo():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, 2, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0] and out[1]
