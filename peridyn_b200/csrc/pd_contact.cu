@@ -578,6 +578,35 @@ pd_status build_reverse(pd_env *env, DevContact &dc, int64_t n_src, int64_t src_
     return PD_OK;
 }
 
+// Lists of the particles with contact work (local indices; order free: each
+// particle's own sum does not depend on it).
+__global__ void k_active(int64_t n_src, const int32_t *__restrict__ nb, int64_t n_tgt,
+                         const int32_t *__restrict__ roff, int self, int32_t *__restrict__ act1,
+                         int32_t *__restrict__ act2, int32_t *__restrict__ counts) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n_src && (nb[i] >= 0 || (self && roff[i + 1] > roff[i]))) act1[atomicAdd(&counts[0], 1)] = (int32_t)i;
+    if (!self && i < n_tgt && roff[i + 1] > roff[i]) act2[atomicAdd(&counts[1], 1)] = (int32_t)i;
+}
+
+pd_status build_active(pd_env *env, DevContact &dc, bool self) {
+    cudaStream_t st = env->st;
+    const int64_t n2 = self ? dc.n1 : dc.n2;
+    if ((int64_t)dc.act1.n < dc.n1) PD_TRY(dc.act1.alloc(std::max<int64_t>(dc.n1, 1)));
+    if (!self && (int64_t)dc.act2.n < n2) PD_TRY(dc.act2.alloc(std::max<int64_t>(n2, 1)));
+    if (!dc.act_n.p) PD_TRY(dc.act_n.alloc(2));
+    CK(cudaMemsetAsync(dc.act_n.p, 0, 2 * sizeof(int32_t), st));
+    const int64_t n = std::max(dc.n1, n2);
+    k_active<<<gridn(n), kT, 0, st>>>(dc.n1, dc.nb.p, n2, dc.rev_off.p, self ? 1 : 0, dc.act1.p,
+                                      self ? nullptr : dc.act2.p, dc.act_n.p);
+    pd::note_launch();
+    int32_t h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, dc.act_n.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    dc.nact1 = h[0];
+    dc.nact2 = self ? 0 : h[1];
+    return PD_OK;
+}
+
 pd_status update12(pd_env *env, const HostContact &hc, DevContact &dc) {
     cudaStream_t st = env->st;
     const int64_t n1 = dc.n1, n2 = dc.n2;
@@ -596,7 +625,7 @@ pd_status update12(pd_env *env, const HostContact &hc, DevContact &dc) {
     dc.has_neighs = true;
     if (bvol < 0.0) {
         PD_TRY(build_reverse(env, dc, n1, dc.first1, n2, dc.first2, dc.nb.p, dc.rows, false));
-        return PD_OK;
+        return build_active(env, dc, false);
     }
     double cell = hc.distance * (1.0 + 1e-9);
     int dims[3];
@@ -645,8 +674,7 @@ pd_status update12(pd_env *env, const HostContact &hc, DevContact &dc) {
     k_c1_select<<<gridn(n1), kT, 0, st>>>(n1, dc.rows, dc.first2, c1off.p, cand.p, dc.nb.p); pd::note_launch();
     CK(cudaGetLastError());
     PD_TRY(build_reverse(env, dc, n1, dc.first1, n2, dc.first2, dc.nb.p, dc.rows, false));
-    CK(cudaStreamSynchronize(st));
-    return PD_OK;
+    return build_active(env, dc, false);
 }
 
 pd_status update11(pd_env *env, const HostContact &hc, DevContact &dc, int64_t max_part) {
@@ -672,8 +700,7 @@ pd_status update11(pd_env *env, const HostContact &hc, DevContact &dc, int64_t m
     dc.has_neighs = true;
     PD_TRY(build_reverse(env, dc, dc.n1, dc.first1, dc.n1, dc.first1, dc.nb.p, dc.nbrows,
                          hc.kind != PD_CONTACT_11_ORDERED));
-    CK(cudaStreamSynchronize(st));
-    return PD_OK;
+    return build_active(env, dc, true);
 }
 
 }  // namespace

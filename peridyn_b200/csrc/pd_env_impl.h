@@ -130,6 +130,11 @@ struct DevContact {
     DBuf<int32_t> rev_cnt;  // n2 scratch
     int64_t rev_cap = 0;
     bool has_neighs = false;
+    // particles with contact work, built with the neighbour lists: set-1
+    // particles with a neighbour (self contact: or a reverse entry), set-2
+    // particles with a reverse entry (two-block contact); -1 = not built
+    DBuf<int32_t> act1, act2, act_n;
+    int64_t nact1 = -1, nact2 = -1;
 };
 
 }  // namespace pd

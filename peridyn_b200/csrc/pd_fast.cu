@@ -151,6 +151,9 @@ struct StepArgs {
     R *rtd;
     const int32_t *partner;
     int32_t ep;  // the environment has elasto-plastic blocks
+    // contact accelerations of this step, added by the fused integration
+    // (MODE 1/2; null without contacts)
+    const typename Tr<R>::V4 *cacc;
     int32_t stage_bytes;  // dynamic shared memory of the staged kernels
     // Slice order of the one-slice-per-block kernels: with swz_g = G > 0,
     // block b = r + G c walks slice r K + c (K = swz_k), so blocks that are
@@ -658,6 +661,12 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
     if (MODE == 2 || MODE == 4) {
         const R m = a.mass[p];
         if (MODE == 2) a.p[p] = V4{m * vp.x, m * vp.y, m * vp.z, R(0)};
+    }
+    if ((MODE == 1 || MODE == 2) && a.cacc) {
+        const typename Tr<R>::V4 c = a.cacc[p];
+        fx += c.x;
+        fy += c.y;
+        fz += c.z;
     }
     const uint8_t bits = a.nbc ? a.bcbits[p] : 0;
     R v0 = Tr<R>::fma_(a.c, fx, vp.x), v1 = Tr<R>::fma_(a.c, fy, vp.y), v2 = Tr<R>::fma_(a.c, fz, vp.z);
@@ -1217,11 +1226,15 @@ __device__ __forceinline__ void ypos(const StepArgs<R> &a, int64_t p, double &y0
     y2 = x.z + u2;
 }
 
+// The contact kernels run over the lists of particles with contact work
+// (act, nact entries; built with the neighbour lists), or over the whole
+// set when act is null.
 template <class R>
 __global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows, const int32_t *nb,
-                         const double *dens, CLawF law) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n1) return;
+                         const double *dens, CLawF law, const int32_t *act, int64_t nact) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nact) return;
+    const int64_t i = act ? act[t] : t;
     const int64_t p = first1 + i;
     double yi0, yi1, yi2, a0 = 0, a1 = 0, a2 = 0;
     ypos(a, p, yi0, yi1, yi2);
@@ -1246,9 +1259,10 @@ __global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows
 
 template <class R>
 __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_t *roff, const int32_t *rev,
-                         const double *dens, CLawF law) {
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= n2) return;
+                         const double *dens, CLawF law, const int32_t *act, int64_t nact) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nact) return;
+    const int64_t j = act ? act[t] : t;
     const int32_t o = roff[j], e = roff[j + 1];
     if (o == e) return;
     const int64_t q = first2 + j;
@@ -1274,9 +1288,11 @@ __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_
 
 template <class R>
 __global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, int64_t nbrows, const int32_t *nb11,
-                       const int32_t *roff, const int32_t *rev, const double *dens, CLawF law) {
-    const int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (li >= n) return;
+                       const int32_t *roff, const int32_t *rev, const double *dens, CLawF law, const int32_t *act,
+                       int64_t nact) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nact) return;
+    const int64_t li = act ? act[t] : t;
     const int64_t p = first + li;
     const int32_t o = roff[li], e = roff[li + 1];
     if (o == e && nb11[li] < 0) return;
@@ -1334,6 +1350,7 @@ struct Fast {
     DBuf<GridBar> gbar;   // persistent-chunk barrier state
     DBuf<int32_t> serr;   // staged kernels: a staging copy timed out
     DBuf<R> rtd;          // elasto-plastic: 1/sqrt(td_norm2) per particle
+    DBuf<V4> cacc;        // contact accelerations of the current step (zero between steps)
     DBuf<int32_t> partner;  // elasto-plastic: reverse-bond slot per slot
     bool persisted = false;
     int cur = 0;
@@ -1605,6 +1622,10 @@ pd_status init_fast(pd_env *env, Fast<R> &F) {
         PD_TRY(F.mass.alloc(N));
         PD_TRY(F.mab.alloc(N));
         PD_TRY(F.bcbits.alloc(N));
+        if (!env->hc.empty()) {
+            PD_TRY(F.cacc.alloc(N));
+            CK(cudaMemsetAsync(F.cacc.p, 0, N * sizeof(typename Tr<R>::V4), env->st));
+        }
         // parameters in the working precision
         std::vector<FBlock<R>> fb;
         std::vector<FPair<R>> fp;
@@ -1760,20 +1781,60 @@ pd_status contacts_fast(pd_env *env, StepArgs<R> &a) {
         DevContact &dc = env->contacts[k];
         if (!dc.has_neighs) continue;
         CLawF law{hc.equi_dist, hc.exponent, hc.stiffness};
+        const bool lists = dc.nact1 >= 0;
+        const int64_t n1 = lists ? dc.nact1 : dc.n1;
+        const int32_t *a1 = lists ? dc.act1.p : nullptr;
         if (hc.kind == PD_CONTACT_12) {
-            k_fc12_1<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.rows, dc.nb.p, env->dens.p, law);
-            k_fc12_2<R><<<gridn(dc.n2, 256), 256, 0, env->st>>>(a, dc.first2, dc.n2, dc.rev_off.p, dc.rev.p,
-                                                                env->dens.p, law);
-            note_launch();
-            note_launch();
-        } else {
-            k_fc11<R><<<gridn(dc.n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nbrows, dc.nb.p, dc.rev_off.p, dc.rev.p,
-                                                             env->dens.p, law);
+            const int64_t n2 = lists ? dc.nact2 : dc.n2;
+            const int32_t *a2 = lists ? dc.act2.p : nullptr;
+            if (n1 > 0) {
+                k_fc12_1<R><<<gridn(n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.rows, dc.nb.p, env->dens.p,
+                                                                 law, a1, n1);
+                note_launch();
+            }
+            if (n2 > 0) {
+                k_fc12_2<R><<<gridn(n2, 256), 256, 0, env->st>>>(a, dc.first2, dc.n2, dc.rev_off.p, dc.rev.p,
+                                                                 env->dens.p, law, a2, n2);
+                note_launch();
+            }
+        } else if (n1 > 0) {
+            k_fc11<R><<<gridn(n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nbrows, dc.nb.p, dc.rev_off.p,
+                                                           dc.rev.p, env->dens.p, law, a1, n1);
             note_launch();
         }
     }
     CK(cudaGetLastError());
     return PD_OK;
+}
+
+template <class V4>
+__global__ void k_czero(V4 *cacc, int64_t first, const int32_t *act, int64_t n) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    cacc[first + (act ? act[t] : t)] = V4{};
+}
+
+// Clears the entries the contact kernels wrote (their particle lists), so
+// the contact acceleration array is zero between steps.
+template <class V4>
+void contacts_clear(pd_env *env, V4 *cacc) {
+    for (size_t k = 0; k < env->hc.size(); ++k) {
+        const DevContact &dc = env->contacts[k];
+        if (!dc.has_neighs) continue;
+        const bool lists = dc.nact1 >= 0;
+        const int64_t n1 = lists ? dc.nact1 : dc.n1;
+        if (n1 > 0) {
+            k_czero<V4><<<gridn(n1, 256), 256, 0, env->st>>>(cacc, dc.first1, lists ? dc.act1.p : nullptr, n1);
+            note_launch();
+        }
+        if (env->hc[k].kind == PD_CONTACT_12) {
+            const int64_t n2 = lists ? dc.nact2 : dc.n2;
+            if (n2 > 0) {
+                k_czero<V4><<<gridn(n2, 256), 256, 0, env->st>>>(cacc, dc.first2, lists ? dc.act2.p : nullptr, n2);
+                note_launch();
+            }
+        }
+    }
 }
 
 bool any_lps(const pd_env *env) {
@@ -2222,18 +2283,23 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         gate_launch(env, a, F);
         if (lps) launch_theta(st, wps, a);
         if (a.ep) launch_td(st, wps, a);
-        prof_begin(env, st);
         if (!contacts) {
+            prof_begin(env, st);
             if (stop) launch_step<R, 2>(st, wps, a);
             else launch_step<R, 1>(st, wps, a);
             prof_end(env, st);
         } else {
-            launch_step<R, 0>(st, wps, a);
+            // contact accelerations at this step's positions into F.cacc,
+            // then the fused step adds them before integrating
+            StepArgs<R> b = a;
+            b.f = F.cacc.p;
+            PD_TRY(contacts_fast(env, b));
+            a.cacc = F.cacc.p;
+            prof_begin(env, st);
+            if (stop) launch_step<R, 2>(st, wps, a);
+            else launch_step<R, 1>(st, wps, a);
             prof_end(env, st);
-            PD_TRY(contacts_fast(env, a));
-            if (stop) k_integrate<R, 4><<<grid, kT, 0, st>>>(a);
-            else k_integrate<R, 3><<<grid, kT, 0, st>>>(a);
-            note_launch();
+            contacts_clear(env, F.cacc.p);
         }
         if (a.ep) env->ecur = 1 - env->ecur;
         if (check) {
