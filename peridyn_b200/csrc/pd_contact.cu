@@ -558,9 +558,8 @@ pd_status build_reverse(pd_env *env, DevContact &dc, int64_t n_src, int64_t src_
     if (c11) k_c11_rev_count<<<gridn(n_src), kT, 0, st>>>(src_first, n_src, nb, dc.rev_cnt.p);
     else k_rev_count<<<gridn(n_src), kT, 0, st>>>(n_src, rows, tgt_first, nb, dc.rev_cnt.p);
     pd::note_launch();
-    DBuf<int32_t> tmp;
-    PD_TRY(tmp.alloc((n_tgt + 1 + kScanTile - 1) / kScanTile + 2));
-    scan_exclusive(st, n_tgt + 1, dc.rev_cnt.p, dc.rev_off.p, tmp.p);
+    PD_TRY(grow(dc.s_rtmp, (n_tgt + 1 + kScanTile - 1) / kScanTile + 2));
+    scan_exclusive(st, n_tgt + 1, dc.rev_cnt.p, dc.rev_off.p, dc.s_rtmp.p);
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, dc.rev_off.p + n_tgt, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -646,21 +645,22 @@ pd_status update12(pd_env *env, const HostContact &hc, DevContact &dc) {
     b.inv_cell = 1.0 / std::max(width * (1.0 + 1e-9), cell);
     b.dims = make_int3(dims[0], dims[1], dims[2]);
     const int64_t ncell = (int64_t)dims[0] * dims[1] * dims[2];
-    DBuf<int32_t> cell_of, ccount, cstart, cursor, clist, tmp, c1cnt, c1off, cand;
-    PD_TRY(cell_of.alloc(n2));
-    PD_TRY(ccount.alloc(ncell + 1));
-    PD_TRY(cstart.alloc(ncell + 1));
-    PD_TRY(cursor.alloc(ncell + 1));
-    PD_TRY(clist.alloc(n2));
-    PD_TRY(tmp.alloc((std::max(ncell, n1) + 1 + kScanTile - 1) / kScanTile + 2));
+    DBuf<int32_t> &cell_of = dc.s_cell_of, &ccount = dc.s_ccount, &cstart = dc.s_cstart, &cursor = dc.s_cursor,
+                  &clist = dc.s_clist, &tmp = dc.s_tmp, &c1cnt = dc.s_c1cnt, &c1off = dc.s_c1off, &cand = dc.s_cand;
+    PD_TRY(grow(cell_of, n2));
+    PD_TRY(grow(ccount, ncell + 1));
+    PD_TRY(grow(cstart, ncell + 1));
+    PD_TRY(grow(cursor, ncell + 1));
+    PD_TRY(grow(clist, n2));
+    PD_TRY(grow(tmp, (std::max(ncell, n1) + 1 + kScanTile - 1) / kScanTile + 2));
     CK(cudaMemsetAsync(ccount.p, 0, (ncell + 1) * 4, st));
     CK(cudaMemsetAsync(cursor.p, 0, (ncell + 1) * 4, st));
     k_c2_count<<<gridn(n2), kT, 0, st>>>(dc.first2, n2, env->y.p, b, cell_of.p, ccount.p); pd::note_launch();
     scan_exclusive(st, ncell + 1, ccount.p, cstart.p, tmp.p);
     k_c2_scatter<<<gridn(n2), kT, 0, st>>>(n2, cell_of.p, cstart.p, cursor.p, clist.p); pd::note_launch();
     const double dist2 = hc.distance * hc.distance;
-    PD_TRY(c1cnt.alloc(n1 + 1));
-    PD_TRY(c1off.alloc(n1 + 1));
+    PD_TRY(grow(c1cnt, n1 + 1));
+    PD_TRY(grow(c1off, n1 + 1));
     CK(cudaMemsetAsync(c1cnt.p, 0, (n1 + 1) * 4, st));
     k_c1_candidates<false><<<gridn(n1), kT, 0, st>>>(dc.first1, n1, dc.first2, env->y.p, b, dist2, cstart.p, clist.p,
                                                      c1cnt.p, nullptr, nullptr); pd::note_launch();
@@ -668,7 +668,7 @@ pd_status update12(pd_env *env, const HostContact &hc, DevContact &dc) {
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, c1off.p + n1, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    PD_TRY(cand.alloc(std::max<int32_t>(total, 1)));
+    PD_TRY(grow(cand, std::max<int32_t>(total, 1)));
     k_c1_candidates<true><<<gridn(n1), kT, 0, st>>>(dc.first1, n1, dc.first2, env->y.p, b, dist2, cstart.p, clist.p,
                                                     nullptr, c1off.p, cand.p); pd::note_launch();
     k_c1_select<<<gridn(n1), kT, 0, st>>>(n1, dc.rows, dc.first2, c1off.p, cand.p, dc.nb.p); pd::note_launch();

@@ -135,7 +135,16 @@ struct DevContact {
     // particles with a reverse entry (two-block contact); -1 = not built
     DBuf<int32_t> act1, act2, act_n;
     int64_t nact1 = -1, nact2 = -1;
+    // neighbour-search scratch, kept between updates (grown, never shrunk)
+    DBuf<int32_t> s_cell_of, s_ccount, s_cstart, s_cursor, s_clist, s_tmp, s_c1cnt, s_c1off, s_cand, s_rtmp;
 };
+
+// Reallocates b only when it holds fewer than n elements.
+template <class T>
+inline pd_status grow(DBuf<T> &b, int64_t n) {
+    if ((int64_t)b.n >= n && b.p) return PD_OK;
+    return b.alloc((size_t)std::max<int64_t>(n, 1));
+}
 
 }  // namespace pd
 
