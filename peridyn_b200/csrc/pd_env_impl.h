@@ -150,6 +150,7 @@ inline pd_status grow(DBuf<T> &b, int64_t n) {
 
 struct pd_env {
     int device = 0, precision = 0;
+    int sm_count = 0;  // multiprocessors of the device (read once)
     double dt = 0;
     int64_t ts = 0;
     cudaStream_t st = nullptr;

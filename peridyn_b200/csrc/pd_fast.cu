@@ -1554,9 +1554,8 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     }
     const char *sw = std::getenv("PD_SWIZZLE");
     if (!(sw && std::strcmp(sw, "0") == 0)) {  // on unless PD_SWIZZLE=0
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (env->sm_count == 0) cudaDeviceGetAttribute(&env->sm_count, cudaDevAttrMultiProcessorCount, env->device);
+        const int sms = env->sm_count;
         const int64_t S = (env->N + 31) / 32;
         if (sms > 0 && S > sms) {
             a.swz_g = sms;
