@@ -1003,11 +1003,10 @@ extern "C" pd_status pd_env_num_bonds(pd_env *env, int64_t *intact_bonds) {
     PD_TRY(need_final(env));
     if (!intact_bonds) return fail(PD_ERR_ARG, "intact_bonds is NULL");
     CK(cudaSetDevice(env->device));
-    DBuf<int32_t> tmp;
-    PD_TRY(tmp.alloc(env->N));
-    launch_popcount(env->st, env->N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, tmp.p);
+    PD_TRY(grow(env->scr_i, env->N));
+    launch_popcount(env->st, env->N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, env->scr_i.p);
     std::vector<int32_t> h(env->N);
-    CK(cudaMemcpyAsync(h.data(), tmp.p, env->N * 4, cudaMemcpyDeviceToHost, env->st));
+    CK(cudaMemcpyAsync(h.data(), env->scr_i.p, env->N * 4, cudaMemcpyDeviceToHost, env->st));
     CK(cudaStreamSynchronize(env->st));
     int64_t s = 0;
     for (int32_t c : h) s += c;
@@ -1190,13 +1189,12 @@ extern "C" pd_status pd_env_reset_bonds(pd_env *env) {
 // diagnostics
 // ---------------------------------------------------------------------
 static pd_status damage_internal(pd_env *env, std::vector<double> &dint) {
-    DBuf<double> d;
-    PD_TRY(d.alloc(env->N));
+    PD_TRY(grow(env->scr_d, env->N));
     launch_damage(env->st, env->N, env->sinfo.p, env->cnt.p, env->words[env->cur].p, env->intact0.p,
-                  env->tinfo.p, d.p);
+                  env->tinfo.p, env->scr_d.p);
     CK(cudaGetLastError());
     dint.resize(env->N);
-    CK(cudaMemcpyAsync(dint.data(), d.p, env->N * sizeof(double), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaMemcpyAsync(dint.data(), env->scr_d.p, env->N * sizeof(double), cudaMemcpyDeviceToHost, env->st));
     CK(cudaStreamSynchronize(env->st));
     return PD_OK;
 }

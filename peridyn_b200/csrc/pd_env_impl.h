@@ -206,6 +206,8 @@ struct pd_env {
 
     // scratch for the device-pointer entry point and solvers
     pd::DBuf<double4> tmp_y, tmp_f, opt;
+    pd::DBuf<double> scr_d;    // per-particle result scratch (damage), kept between calls
+    pd::DBuf<int32_t> scr_i;   // per-particle count scratch (bond counts)
     pd::DBuf<int32_t> free_mask;
     pd::DBuf<double> red;
 

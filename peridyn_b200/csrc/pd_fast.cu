@@ -1712,8 +1712,8 @@ pd_status gate_prepare(pd_env *env, Fast<R> &F) {
         if (!items.empty()) {
             const int ni = (int)items.size();
             const int gx = std::max(1, std::min(kGB, (kGB * 8) / ni));
-            PD_TRY(F.gitems.alloc(items.size()));
-            PD_TRY(F.gpart.alloc(3 * (size_t)ni * gx));
+            PD_TRY(grow(F.gitems, (int64_t)items.size()));
+            PD_TRY(grow(F.gpart, 3 * (int64_t)ni * gx));
             CK(cudaMemcpyAsync(F.gitems.p, items.data(), items.size() * sizeof(GateItem), cudaMemcpyHostToDevice,
                                env->st));
             CK(cudaStreamSynchronize(env->st));

@@ -42,6 +42,11 @@ void pd_env::release_device() {
     bcs.clear();
     contacts.clear();
     tmp_y.reset();
+    scr_d.reset();
+    scr_i.reset();
+    splan_off.reset();
+    splan.reset();
+    spos.reset();
     tmp_f.reset();
     opt.reset();
     free_mask.reset();
@@ -195,8 +200,8 @@ pd_status update_acc_serial(pd_env *env) {
         const int gx = std::max(1, std::min(148, (148 * 8) / ni));
         if (env->gate_items_h.size() != items.size() ||
             std::memcmp(env->gate_items_h.data(), items.data(), items.size() * sizeof(GateItem)) != 0) {
-            PD_TRY(env->gate_items.alloc(items.size()));
-            PD_TRY(env->gate_part.alloc(3 * (size_t)ni * gx));
+            PD_TRY(grow(env->gate_items, (int64_t)items.size()));
+            PD_TRY(grow(env->gate_part, 3 * (int64_t)ni * gx));
             CK(cudaMemcpyAsync(env->gate_items.p, items.data(), items.size() * sizeof(GateItem),
                                cudaMemcpyHostToDevice, st));
             CK(cudaStreamSynchronize(st));
