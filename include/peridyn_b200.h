@@ -247,6 +247,9 @@ PD_API pd_status pd_env_get_contact_neighs(pd_env *env, int64_t contact, int64_t
 /* ---------------------------------------------------------------------- */
 /* Diagnostics                                                             */
 /* ---------------------------------------------------------------------- */
+/* environment.jl:169 intact0: bonds per particle at finalize (environment
+ * order; N_env values). */
+PD_API pd_status pd_env_intact0(pd_env *env, int64_t *intact0);
 /* cal_damage (peri.jl:587-594): N values. */
 PD_API pd_status pd_env_damage(pd_env *env, double *damage);
 /* printdata (environment.jl:308-320): out[0..2] = sum p, out[3..5] =

@@ -142,6 +142,7 @@ _SIGNATURES = {
     "pd_env_layout_stats": (ctypes.c_int32, [c_vp, c_i64p, ctypes.c_int64]),
     "pd_env_pack_halo": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_int64, c_vp]),
     "pd_env_set_deformed": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_int32]),
+    "pd_env_intact0": (ctypes.c_int32, [c_vp, c_i64p]),
     "pd_env_unpack_halo": (ctypes.c_int32, [c_vp, c_vp, ctypes.c_int64, c_vp]),
     "pd_force_density_device": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_vp, c_vp, c_vp]),
     "pd_force_density_device_static": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_vp, c_vp, c_vp]),

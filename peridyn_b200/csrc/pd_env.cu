@@ -1199,6 +1199,17 @@ static pd_status damage_internal(pd_env *env, std::vector<double> &dint) {
     return PD_OK;
 }
 
+extern "C" pd_status pd_env_intact0(pd_env *env, int64_t *intact0) {
+    PD_TRY(need_final(env));
+    if (!intact0) return fail(PD_ERR_ARG, "intact0 is NULL");
+    CK(cudaSetDevice(env->device));
+    std::vector<int32_t> h(env->N);
+    CK(cudaMemcpyAsync(h.data(), env->intact0.p, env->N * sizeof(int32_t), cudaMemcpyDeviceToHost, env->st));
+    CK(cudaStreamSynchronize(env->st));
+    for (int64_t e = 0; e < env->N_env; ++e) intact0[e] = h[env->map_h[e]];
+    return PD_OK;
+}
+
 extern "C" pd_status pd_env_damage(pd_env *env, double *damage) {
     PD_TRY(need_final(env));
     if (!damage) return fail(PD_ERR_ARG, "damage is NULL");

@@ -104,8 +104,8 @@ class GeneralEnvironment:
         self.density = np.zeros(self.N)
         _abi.check(L.pd_env_get_mass(self._h, _abi.dptr(self.mass), _abi.dptr(self.volume),
                                      _abi.dptr(self.density)))
-        self.intact0 = np.concatenate([self._family(b)[1].sum(axis=0).astype(np.int64)
-                                       for b in range(len(self.material_blocks))])
+        self.intact0 = np.zeros(self.N, dtype=np.int64)  # environment.jl:169
+        _abi.check(L.pd_env_intact0(self._h, _abi.i64ptr(self.intact0)))
         y = self.y
         lo, hi = y.min(axis=1), y.max(axis=1)
         cm_, L_ = (lo + hi) / 2, hi - lo
