@@ -1,11 +1,10 @@
 // pd_server.cu -- the serving loop (pd_server_* in include/peridyn_b200.h).
 //
-// One worker thread per server owns every admitted job.  Jobs queue in
-// arrival order; the worker admits the head of the queue while the sum of
-// the resident jobs' HBM footprints stays within the budget (and fewer
-// than max_active run), finalizes the job's environment there, and then
-// advances every resident job in chunks of velocity-Verlet steps on the
-// job's own CUDA stream.  A job gets its next chunk as soon as its previous
+// Jobs queue in arrival order; two admission threads take the head of the
+// queue while the sum of the resident jobs' HBM footprints stays within the
+// budget (and fewer than max_active run) and finalize the job's
+// environment; a stepping thread advances every resident job in chunks of
+// velocity-Verlet steps on the job's own CUDA stream.  A job gets its next chunk as soon as its previous
 // one has finished (an event per job), so short jobs are not held back by
 // long ones and the chunks of different jobs overlap on the device.  A
 // finished job's state is downloaded and its device memory released at
@@ -74,7 +73,11 @@ struct pd_server {
     std::vector<Job *> ready;  // admitted, not yet picked up by the stepper
     int resident = 0;          // admitted and not finished
     bool stop = false;
-    std::thread admitter, stepper;
+    // Admission (family build, layout, initial forces) is mostly host work
+    // of one job at a time; two admission threads finalize two jobs at once
+    // while the stepping thread keeps the device busy.
+    static constexpr int kAdmitters = 2;
+    std::thread admitters[kAdmitters], stepper;
 
     void admit_loop();
     void step_loop();
@@ -137,7 +140,7 @@ void pd_server::admit(Job *j) {
     j->particles = env->N_env;
 }
 
-// Admission thread: takes the head of the queue when its footprint fits
+// Admission threads: each takes the head of the queue when its footprint fits
 // (or nothing else is resident) and a slot is free, finalizes it (family
 // build, BC snapshot, initial forces) and hands it to the stepping thread.
 void pd_server::admit_loop() {
@@ -294,13 +297,15 @@ extern "C" pd_status pd_server_create(pd_server **out, int32_t device, int64_t h
     s->chunk = chunk_steps;
     try {
         s->stepper = std::thread([p = s.get()] { p->step_loop(); });
-        s->admitter = std::thread([p = s.get()] { p->admit_loop(); });
+        for (auto &t : s->admitters) t = std::thread([p = s.get()] { p->admit_loop(); });
     } catch (...) {
         {
             std::lock_guard<std::mutex> lock(s->mu);
             s->stop = true;
             s->wake.notify_all();
         }
+        for (auto &t : s->admitters)
+            if (t.joinable()) t.join();
         if (s->stepper.joinable()) s->stepper.join();
         return fail(PD_ERR_OOM, "cannot start the server threads");
     }
@@ -390,7 +395,8 @@ extern "C" pd_status pd_server_destroy(pd_server *srv) {
         for (Job *j : srv->queue) j->cancel = true;
         srv->wake.notify_all();
     }
-    if (srv->admitter.joinable()) srv->admitter.join();
+    for (auto &t : srv->admitters)
+        if (t.joinable()) t.join();
     if (srv->stepper.joinable()) srv->stepper.join();
     for (auto &kv : srv->jobs)
         if (kv.second->env) pd_env_destroy(kv.second->env);
