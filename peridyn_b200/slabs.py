@@ -211,20 +211,35 @@ class SlabRank:
     the plan's order on every rank.  ``env`` is the rank's slab
     environment (an ``Env`` built from ``plan.slab_workload(rank, ...)`` on
     the rank's device) or any object with ``pack(idx, buf)`` /
-    ``unpack(idx, buf)`` on tensors."""
+    ``unpack(idx, buf)`` on tensors.  ``wire`` is where the send/recv
+    buffers live: ``"device"`` (NCCL moves device memory) or ``"host"``
+    (pinned host copies, for a backend without device tensors such as
+    gloo)."""
 
-    def __init__(self, plan, rank, dist, env, device="cuda"):
+    def __init__(self, plan, rank, dist, env, device="cuda", wire="device"):
+        if wire not in ("device", "host"):
+            raise ValueError("wire must be 'device' or 'host'")
         self.plan, self.rank, self.dist, self.device = plan, int(rank), dist, device
         self.env = env
         torch = _torch()
+        on_dev = str(device).startswith("cuda")
+        self.host_wire = wire == "host" and on_dev
+
+        def wire_buf(n):
+            if self.host_wire:
+                return torch.empty(9 * n, dtype=torch.float64, pin_memory=True)
+            return None
+
         self.sends, self.recvs = [], []
         for (o, s, src, dst) in plan.exchanges:
             if o == self.rank:
                 self.sends.append((s, torch.as_tensor(src, device=device),
-                                   torch.empty(9 * src.size, dtype=torch.float64, device=device)))
+                                   torch.empty(9 * src.size, dtype=torch.float64, device=device),
+                                   wire_buf(src.size)))
             if s == self.rank:
                 self.recvs.append((o, torch.as_tensor(dst, device=device),
-                                   torch.empty(9 * dst.size, dtype=torch.float64, device=device)))
+                                   torch.empty(9 * dst.size, dtype=torch.float64, device=device),
+                                   wire_buf(dst.size)))
 
     def _pack(self, idx, buf):
         if hasattr(self.env, "pack"):
@@ -240,14 +255,35 @@ class SlabRank:
 
     def exchange(self):
         torch = _torch()
-        for _, idx, buf in self.sends:
+        for _, idx, buf, hbuf in self.sends:
             self._pack(idx, buf)
+            if hbuf is not None:
+                hbuf.copy_(buf, non_blocking=True)
         if str(self.device).startswith("cuda"):
             torch.cuda.synchronize(self.device)
-        ops = [self.dist.P2POp(self.dist.isend, buf, peer) for peer, _, buf in self.sends]
-        ops += [self.dist.P2POp(self.dist.irecv, buf, peer) for peer, _, buf in self.recvs]
+        ops = [self.dist.P2POp(self.dist.isend, buf if hbuf is None else hbuf, peer)
+               for peer, _, buf, hbuf in self.sends]
+        ops += [self.dist.P2POp(self.dist.irecv, buf if hbuf is None else hbuf, peer)
+                for peer, _, buf, hbuf in self.recvs]
         if ops:
             for r in self.dist.batch_isend_irecv(ops):
                 r.wait()
-        for _, idx, buf in self.recvs:
+        for _, idx, buf, hbuf in self.recvs:
+            if hbuf is not None:
+                buf.copy_(hbuf, non_blocking=True)
             self._unpack(idx, buf)
+
+    def step(self, nsteps=1):
+        """``nsteps`` velocity-Verlet steps of the rank's slab, a halo
+        exchange after each (every rank calls it with the same count)."""
+        L = _abi.lib()
+        for _ in range(int(nsteps)):
+            _abi.check(L.pd_env_vv_steps(self.env._h, 1))
+            self.exchange()
+
+    def owned_state(self):
+        """(environment-order indices, y, v, f) of the particles this rank
+        owns."""
+        ys, vs, fs, _ = self.env.get_state()
+        own = self.plan.owned[self.rank]
+        return self.plan.local[self.rank][own], ys[:, own], vs[:, own], fs[:, own]

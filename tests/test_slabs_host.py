@@ -129,3 +129,10 @@ def test_two_rank_halo_exchange_gloo():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert out[0] and out[1]
+
+
+def test_rank_wire_must_be_device_or_host():
+    w = _bar()
+    plan = SlabPlan(w["materials"], 2)
+    with pytest.raises(ValueError):
+        SlabRank(plan, 0, dist, _FakeSlab(torch.zeros((plan.local[0].size, 9))), device="cpu", wire="nvlink")
