@@ -1369,6 +1369,7 @@ struct Fast {
     int32_t *flags_h = nullptr;
     cudaEvent_t flags_ev = nullptr;
     bool flags_pending = false;
+    int64_t gate_runs = 0;          // gate steps enqueued since the gate list last changed
     ~Fast() {
         for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
         if (flags_h) cudaFreeHost(flags_h);
@@ -1719,6 +1720,7 @@ pd_status gate_prepare(pd_env *env, Fast<R> &F) {
             CK(cudaStreamSynchronize(env->st));
         }
         F.gitems_h = items;
+        F.gate_runs = 0;
     }
     return PD_OK;
 }
@@ -1740,13 +1742,19 @@ template <class R>
 pd_status gate_if_needed(pd_env *env, StepArgs<R> &a, Fast<R> &F) {
     PD_TRY(gate_prepare(env, F));
     gate_launch(env, a, F);
+    if (!F.gitems_h.empty()) ++F.gate_runs;
     return PD_OK;
 }
 
-// Non-blocking refresh of the host copy of the gate flags: issue an async
-// read-back, and take its result on a later call once it has landed.
+// Refresh of the host copy of the gate flags: issue an async read-back
+// once a gate step has been enqueued, and take its result on a later call.
+// Without wait the result is taken only once it has landed.  With wait
+// (a blocking stepping call) the pending read is waited for: the host otherwise runs so far ahead of the device that a whole
+// call's replays are enqueued before the read lands, each still carrying
+// the gate kernels after the block has deformed.  The wait leaves the
+// replay enqueued after the read in flight, so the device does not idle.
 template <class R>
-pd_status poll_gate_flags(pd_env *env, Fast<R> &F) {
+pd_status poll_gate_flags(pd_env *env, Fast<R> &F, bool wait) {
     if (F.gitems_h.empty()) return PD_OK;
     const size_t nb = env->hb.size();
     if (!F.flags_h) {
@@ -1754,7 +1762,8 @@ pd_status poll_gate_flags(pd_env *env, Fast<R> &F) {
         CK(cudaEventCreateWithFlags(&F.flags_ev, cudaEventDisableTiming));
     }
     if (F.flags_pending) {
-        const cudaError_t q = cudaEventQuery(F.flags_ev);
+        const cudaError_t q =
+            wait ? cudaEventSynchronize(F.flags_ev) : cudaEventQuery(F.flags_ev);
         if (q == cudaErrorNotReady) return PD_OK;
         if (q != cudaSuccess) return cuda_fail(q, "gate flag read-back", __FILE__, __LINE__);
         F.flags_pending = false;
@@ -1767,6 +1776,7 @@ pd_status poll_gate_flags(pd_env *env, Fast<R> &F) {
             if (F.flags_h[b]) env->deformed_h[b] = 1;
         return gate_prepare(env, F);
     }
+    if (F.gate_runs == 0) return PD_OK;  // no gate step since the list was set: nothing new to read
     CK(cudaMemcpyAsync(F.flags_h, env->deformed.p, nb * sizeof(int32_t), cudaMemcpyDeviceToHost, env->st));
     CK(cudaEventRecord(F.flags_ev, env->st));
     F.flags_pending = true;
@@ -2154,6 +2164,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
     }
     CK(cudaGraphLaunch(hit->exec, st));
     add_launches(hit->kernels);
+    if (!hit->gate.empty()) F.gate_runs += kGraphSteps;
     for (int k = 0; k < kGraphSteps; ++k) advance_bc_clock(env);
     return PD_OK;
 }
@@ -2264,7 +2275,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
             }
         }
         if (graphs && nsteps - 1 - s >= kGraphSteps && flip_free_steps(env, kGraphSteps)) {
-            PD_TRY(poll_gate_flags(env, F));
+            PD_TRY(poll_gate_flags(env, F, blocking));
             PD_TRY(replay_graph(env, F, lps));
             s += kGraphSteps;
             continue;
@@ -2280,6 +2291,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         a.dir_pos = dir_bits(env);
         a.ts = env->ts;
         gate_launch(env, a, F);
+        if (!F.gitems_h.empty()) ++F.gate_runs;
         if (lps) launch_theta(st, wps, a);
         if (a.ep) launch_td(st, wps, a);
         if (!contacts) {
