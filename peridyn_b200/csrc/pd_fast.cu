@@ -613,6 +613,19 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (
     integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
 }
 
+// Programmatic dependent launch.  The bond kernels are launched with
+// programmatic stream serialization (launch_dep): a kernel's blocks may be
+// dispatched while the previous kernel on the stream finishes, and wait
+// here, before their first global access, until it has completed and its
+// writes are visible.  Having passed the wait, a block lets the next
+// kernel be dispatched in turn, so at most two grids of the chain are in
+// flight and the older one never waits.  Without the launch attribute
+// both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Elasto-plastic kernels (EPK) keep more state per bond: up to 128 registers.
 template <class R, int WPS, int U, int MODE, bool EPK = false>
 __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1
@@ -623,6 +636,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
     __shared__ int arrive[SPB];
+    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
@@ -791,6 +805,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][1][32];
     __shared__ int arrive[SPB];
+    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
@@ -891,6 +906,7 @@ __global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB / 2) k_td(Ste
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ double sh[WPS > 1 ? NW : 1][1][32];
     __shared__ int arrive[SPB];
+    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
@@ -1387,15 +1403,33 @@ struct Unroll {
     static constexpr int HI = sizeof(R) == 4 ? 4 : 2;
 };
 
+// Launch of a bond kernel with programmatic stream serialization (the
+// kernel enters through pdl_enter); PD_NO_PDL=1 gives ordinary launches.
+template <class... P>
+inline void launch_dep(void (*kern)(P...), unsigned grid, unsigned block, cudaStream_t st, P... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    const char *off = std::getenv("PD_NO_PDL");
+    cfg.attrs = at;
+    cfg.numAttrs = (off && std::strcmp(off, "1") == 0) ? 0 : 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <class R, int MODE, int U, bool EPK = false>
 void launch_step_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
     const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);  // one slice per block
     switch (wps) {
-        case 1: k_step<R, 1, U, MODE, EPK><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_step<R, 2, U, MODE, EPK><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_step<R, 4, U, MODE, EPK><<<g1, 128, 0, st>>>(a); break;
-        default: k_step<R, 8, U, MODE, EPK><<<g1, 256, 0, st>>>(a); break;
+        case 1: launch_dep(k_step<R, 1, U, MODE, EPK>, (unsigned)((slices + 3) / 4), 128, st, a); break;
+        case 2: launch_dep(k_step<R, 2, U, MODE, EPK>, (unsigned)((slices + 1) / 2), 128, st, a); break;
+        case 4: launch_dep(k_step<R, 4, U, MODE, EPK>, g1, 128, st, a); break;
+        default: launch_dep(k_step<R, 8, U, MODE, EPK>, g1, 256, st, a); break;
     }
     note_launch();
 }
@@ -1407,10 +1441,10 @@ void launch_td(cudaStream_t st, int cfg, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
     const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);
     switch (cfg % 100 / 10) {
-        case 1: k_td<R, 1, U><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_td<R, 2, U><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_td<R, 4, U><<<g1, 128, 0, st>>>(a); break;
-        default: k_td<R, 8, U><<<g1, 256, 0, st>>>(a); break;
+        case 1: launch_dep(k_td<R, 1, U>, (unsigned)((slices + 3) / 4), 128, st, a); break;
+        case 2: launch_dep(k_td<R, 2, U>, (unsigned)((slices + 1) / 2), 128, st, a); break;
+        case 4: launch_dep(k_td<R, 4, U>, g1, 128, st, a); break;
+        default: launch_dep(k_td<R, 8, U>, g1, 256, st, a); break;
     }
     note_launch();
 }
@@ -1490,10 +1524,10 @@ void launch_theta_u(cudaStream_t st, int wps, const StepArgs<R> &a) {
     const int64_t slices = (a.N + 31) / 32;
     const unsigned g1 = (unsigned)(a.swz_g ? (int64_t)a.swz_g * a.swz_k : slices);  // one slice per block
     switch (wps) {
-        case 1: k_theta<R, 1, U><<<(unsigned)((slices + 3) / 4), 128, 0, st>>>(a); break;
-        case 2: k_theta<R, 2, U><<<(unsigned)((slices + 1) / 2), 128, 0, st>>>(a); break;
-        case 4: k_theta<R, 4, U><<<g1, 128, 0, st>>>(a); break;
-        default: k_theta<R, 8, U><<<g1, 256, 0, st>>>(a); break;
+        case 1: launch_dep(k_theta<R, 1, U>, (unsigned)((slices + 3) / 4), 128, st, a); break;
+        case 2: launch_dep(k_theta<R, 2, U>, (unsigned)((slices + 1) / 2), 128, st, a); break;
+        case 4: launch_dep(k_theta<R, 4, U>, g1, 128, st, a); break;
+        default: launch_dep(k_theta<R, 8, U>, g1, 256, st, a); break;
     }
     note_launch();
 }
