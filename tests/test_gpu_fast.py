@@ -261,6 +261,34 @@ def test_persistent_chunks_match_graph_replays(precision, monkeypatch):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+@pytest.mark.parametrize("builder", [
+    lambda: configs.lps_bar(nx=30, ny=8, nz=8),
+    lambda: configs.ep_bar(nx=30, ny=8, nz=8, yield_stress=2e5),
+])
+def test_dependent_launch_is_bit_identical(builder, precision, monkeypatch):
+    # the bond kernels launched with programmatic stream serialization
+    # (default) and as ordinary launches (PD_NO_PDL=1): same numbers, in
+    # graph replays and direct launches alike
+    w = builder()
+
+    def run(pdl):
+        if pdl:
+            monkeypatch.delenv("PD_NO_PDL", raising=False)
+        else:
+            monkeypatch.setenv("PD_NO_PDL", "1")
+        env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
+        pb.apply_bc_at0(env, 0)
+        pb.velocity_verlet_step(env, nsteps=5)    # direct launches
+        pb.velocity_verlet_step(env, nsteps=100)  # graph replays
+        out = env.get_state() + (env.num_bonds(),)
+        env.close()
+        return out
+
+    for a, b in zip(run(True), run(False)):
+        assert np.array_equal(a, b)
+
+
 def _two_type_block():
     x, vol = lattice.cuboid(16, 9, 8, 1.0e-3, jitter=2e-5, seed=9)
     t = np.where(x[0] < x[0].mean(), 1, 2).astype(np.int64)
