@@ -423,12 +423,12 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
 
 template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
-                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R &fx, R &fy,
-                                            R &fz, const typename Tr<R>::V4 *stg = nullptr) {
-    const SliceInfo d = a.si[p >> 5];
+                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, const SliceInfo &d,
+                                            int32_t cp, R &fx, R &fy, R &fz,
+                                            const typename Tr<R>::V4 *stg = nullptr) {
     int32_t k0, k1;
     warp_range<WPS>(d.len, w, k0, k1);
-    k1 = min(k1, a.cnt[p]);
+    k1 = min(k1, cp);
     uint32_t *wp = a.words + d.word + (p & 31);
     R Ap = 0, Bp = 0, rtdp = 0;
     if (KIND != PD_MAT_BOND_BASED) {
@@ -570,9 +570,26 @@ __device__ __forceinline__ void store_u(const StepArgs<R> &a, int64_t p, double 
 template <class R, int MODE>
 __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx, R fy, R fz);
 
+// Programmatic dependent launch.  The bond kernels are launched with
+// programmatic stream serialization (launch_dep): a kernel's blocks may be
+// dispatched while the previous kernel on the stream finishes, and wait
+// here, before they read anything a previous kernel writes, until it has
+// completed and its writes are visible.  Having passed the wait, a block lets the next
+// kernel be dispatched in turn, so at most two grids of the chain are in
+// flight and the older one never waits.  Without the launch attribute
+// both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // One step of one slice (its WPS warps): bond gather, fixed-order
 // combination, integration.  Shared by k_step and the persistent kernel.
-template <class R, int WPS, int U, int MODE, bool NC, bool STG = false, bool EPK = false>
+// PDL: the kernel was launched as a programmatic dependent (k_step); the
+// data written only at initialisation (particle types, block parameters,
+// slice descriptors, slot counts, neighbour offsets) is read before
+// pdl_enter, everything a previous kernel writes after it.
+template <class R, int WPS, int U, int MODE, bool NC, bool STG = false, bool EPK = false, bool PDL = false>
 __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (*sh)[3][32], int *arrive,
                                           const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
@@ -584,21 +601,29 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     constexpr bool kBreak = MODE != 5;
     R f[3] = {0, 0, 0};
+    FBlock<R> B{};
+    SliceInfo d{};
+    int32_t cp = 0;
+    if (ti >= 0) {
+        B = a.fb[ti >> 8];
+        d = a.si[p >> 5];
+        cp = a.cnt[p];
+    }
+    if (PDL) pdl_enter();
     if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
-        const FBlock<R> B = a.fb[b];
         if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
             V4 xp, up;
             Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
             if (B.kind == PD_MAT_BOND_BASED) {
-                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0], f[1], f[2],
+                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, d, cp, f[0], f[1], f[2],
                                                                            stg);
             } else if (EPK && B.kind == PD_MAT_ELASTO_PLASTIC) {
                 if constexpr (EPK)
-                    bond_gather<R, PD_MAT_ELASTO_PLASTIC, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, f[0], f[1],
+                    bond_gather<R, PD_MAT_ELASTO_PLASTIC, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, d, cp, f[0], f[1],
                                                                               f[2]);
             } else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, f[0],
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, d, cp, f[0],
                                                                                      f[1], f[2], stg);
         }
     }
@@ -613,19 +638,6 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (
     integrate<R, MODE>(a, p, fx * ir, fy * ir, fz * ir);
 }
 
-// Programmatic dependent launch.  The bond kernels are launched with
-// programmatic stream serialization (launch_dep): a kernel's blocks may be
-// dispatched while the previous kernel on the stream finishes, and wait
-// here, before their first global access, until it has completed and its
-// writes are visible.  Having passed the wait, a block lets the next
-// kernel be dispatched in turn, so at most two grids of the chain are in
-// flight and the older one never waits.  Without the launch attribute
-// both instructions return at once.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // Elasto-plastic kernels (EPK) keep more state per bond: up to 128 registers.
 template <class R, int WPS, int U, int MODE, bool EPK = false>
 __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1
@@ -636,12 +648,11 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
     __shared__ int arrive[SPB];
-    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    step_body<R, WPS, U, MODE, true, false, EPK>(a, slice_of_block<SPB>(a), sh, arrive);
+    step_body<R, WPS, U, MODE, true, false, EPK, true>(a, slice_of_block<SPB>(a), sh, arrive);
 }
 
 // MODE 3/4: integration of forces already in f (after contact forces).
@@ -764,7 +775,7 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t
 
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
-template <class R, int WPS, int U, bool NC, bool STG = false>
+template <class R, int WPS, int U, bool NC, bool STG = false, bool PDL = false>
 __device__ __forceinline__ void theta_body(const StepArgs<R> &a, int64_t blk, R (*sh)[1][32], int *arrive,
                                            const typename Tr<R>::V4 *stg = nullptr) {
     using V4 = typename Tr<R>::V4;
@@ -776,14 +787,20 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, int64_t blk, R 
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
     const bool lps = ti >= 0 && (a.fb[ti >> 8].kind == PD_MAT_ORDINARY_STATE_BASED ||
                                  a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC);
+    SliceInfo d{};
+    int32_t cp = 0;
+    if (lps) {
+        d = a.si[p >> 5];
+        cp = a.cnt[p];
+    }
+    if (PDL) pdl_enter();
     R acc = 0;
     if (lps) {
         V4 xp, up;
         Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
-        const SliceInfo d = a.si[p >> 5];
         int32_t k0, k1;
         warp_range<WPS>(d.len, w, k0, k1);
-        k1 = min(k1, a.cnt[p]);
+        k1 = min(k1, cp);
         const uint32_t *wp = a.words + d.word + (p & 31);
         if (STG && stg)
             acc = theta_walk<R, WPS, U, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
@@ -805,12 +822,11 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][1][32];
     __shared__ int arrive[SPB];
-    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    theta_body<R, WPS, U, true>(a, slice_of_block<SPB>(a), sh, arrive);
+    theta_body<R, WPS, U, true, false, true>(a, slice_of_block<SPB>(a), sh, arrive);
 }
 
 // ---------------------------------------------------------------------
@@ -873,17 +889,25 @@ __device__ __forceinline__ void td_body(const StepArgs<R> &a, int64_t blk, doubl
     const int w = wid % WPS;
     const int64_t p = (blk * SPB + wid / WPS) * 32 + lane;
     const int32_t ti = p < a.N ? a.tinfo[p] : -1;
-    const bool ep = ti >= 0 && a.fb[ti >> 8].kind == PD_MAT_ELASTO_PLASTIC && a.deformed[ti >> 8];
+    // data written only at initialisation before the dependent-launch wait
+    FBlock<R> B{};
+    SliceInfo d{};
+    int32_t cp = 0;
+    if (ti >= 0) {
+        B = a.fb[ti >> 8];
+        d = a.si[p >> 5];
+        cp = a.cnt[p];
+    }
+    pdl_enter();
+    const bool ep = ti >= 0 && B.kind == PD_MAT_ELASTO_PLASTIC && a.deformed[ti >> 8];
     double acc = 0.0;
     if (ep) {
-        const FBlock<R> B = a.fb[ti >> 8];
         const int tp = ti & 255;
         V4 xp, up;
         Tr<R>::template load_rec<true>(a.xu + 2 * p, xp, up);
-        const SliceInfo d = a.si[p >> 5];
         int32_t k0, k1;
         warp_range<WPS>(d.len, w, k0, k1);
-        k1 = min(k1, a.cnt[p]);
+        k1 = min(k1, cp);
         uint32_t *wp = a.words + d.word + (p & 31);
         const typename Tr<R>::V2 m = a.mab[p];
         const bool st = d.mode == kStencil;
@@ -906,7 +930,6 @@ __global__ void __launch_bounds__(Split<WPS>::BT, Split<WPS>::MINB / 2) k_td(Ste
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ double sh[WPS > 1 ? NW : 1][1][32];
     __shared__ int arrive[SPB];
-    pdl_enter();
     if (WPS > 1) {
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
