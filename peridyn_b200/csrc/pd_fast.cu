@@ -165,6 +165,7 @@ struct StepArgs {
     const FBlock<R> *fb;
     const FPair<R> *fp;
     const int32_t *deformed;
+    int32_t all_def;  // every non-skip block has deformed (known on the host): deformed[] is not read
     const double4 *x64;
     const uint8_t *bcbits;
     R c;
@@ -325,12 +326,12 @@ struct Kin<float> {
 // memory (stg, lane 0's record of slot k at sp[k]) instead of global memory.
 template <class R, int KIND, bool kBreak, int WPS, int U, bool ST, bool MULTI, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1, const int32_t *nb,
-                                          uint32_t *wp, const FBlock<R> &B, int tp, typename Tr<R>::V4 xp,
-                                          typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy, R &fz,
-                                          const typename Tr<R>::V4 *stg = nullptr, const int32_t *sp = nullptr,
-                                          R rtdp = R(0)) {
+                                          uint32_t *wp, const FBlock<R> &B, int tp, const FPair<R> &pp0,
+                                          typename Tr<R>::V4 xp, typename Tr<R>::V4 up, R Ap, R Bp, R &fx, R &fy,
+                                          R &fz, const typename Tr<R>::V4 *stg = nullptr,
+                                          const int32_t *sp = nullptr, R rtdp = R(0)) {
     using V4 = typename Tr<R>::V4;
-    FPair<R> pp = a.fp[B.pair_base + tp + tp * B.nt];
+    FPair<R> pp = pp0;  // the pair (type p, type p); MULTI reloads it per slot
     const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
     float2 fxy = make_float2(0.f, 0.f);  // FP32: packed (fx, fy)
     for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
@@ -423,7 +424,7 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
 
 template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
-                                            typename Tr<R>::V4 xp, typename Tr<R>::V4 up, const SliceInfo &d,
+                                            const FPair<R> &pp0, typename Tr<R>::V4 xp, typename Tr<R>::V4 up, const SliceInfo &d,
                                             int32_t cp, R &fx, R &fy, R &fz,
                                             const typename Tr<R>::V4 *stg = nullptr) {
     int32_t k0, k1;
@@ -441,27 +442,27 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
         if (stg) {  // a staged slice is a stencil slice
             const int32_t *sp = a.spos + d.nbr;
             if (B.nt > 1)
-                bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                bond_walk<R, KIND, kBreak, WPS, U, true, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp,
                                                                      up, Ap, Bp, fx, fy, fz, stg, sp);
             else
-                bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp,
+                bond_walk<R, KIND, kBreak, WPS, U, true, false, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp,
                                                                       up, Ap, Bp, fx, fy, fz, stg, sp);
             return;
         }
     }
     if (B.nt > 1) {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
                                                            fy, fz, nullptr, nullptr, rtdp);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp, up,
+            bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, pp0, xp, up,
                                                             Ap, Bp, fx, fy, fz, nullptr, nullptr, rtdp);
     } else {
         if (d.mode == kStencil)
-            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, xp, up, Ap, Bp, fx,
+            bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
                                                             fy, fz, nullptr, nullptr, rtdp);
         else
-            bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, xp,
+            bond_walk<R, KIND, kBreak, WPS, U, false, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, pp0, xp,
                                                              up, Ap, Bp, fx, fy, fz, nullptr, nullptr, rtdp);
     }
 }
@@ -586,9 +587,10 @@ __device__ __forceinline__ void pdl_enter() {
 // One step of one slice (its WPS warps): bond gather, fixed-order
 // combination, integration.  Shared by k_step and the persistent kernel.
 // PDL: the kernel was launched as a programmatic dependent (k_step); the
-// data written only at initialisation (particle types, block parameters,
-// slice descriptors, slot counts, neighbour offsets) is read before
-// pdl_enter, everything a previous kernel writes after it.
+// data written only at initialisation (particle types, block and pair
+// parameters, slice descriptors, slot counts) is read before pdl_enter,
+// everything a previous kernel writes after it.  With all_def the gate
+// flags are not read at all.
 template <class R, int WPS, int U, int MODE, bool NC, bool STG = false, bool EPK = false, bool PDL = false>
 __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (*sh)[3][32], int *arrive,
                                           const typename Tr<R>::V4 *stg = nullptr) {
@@ -602,28 +604,31 @@ __device__ __forceinline__ void step_body(const StepArgs<R> &a, int64_t blk, R (
     constexpr bool kBreak = MODE != 5;
     R f[3] = {0, 0, 0};
     FBlock<R> B{};
+    FPair<R> pp0{};
     SliceInfo d{};
     int32_t cp = 0;
     if (ti >= 0) {
         B = a.fb[ti >> 8];
+        const int tp = ti & 255;
+        if (B.kind != PD_MAT_SKIP) pp0 = a.fp[B.pair_base + tp + tp * B.nt];
         d = a.si[p >> 5];
         cp = a.cnt[p];
     }
     if (PDL) pdl_enter();
     if (ti >= 0) {
         const int b = ti >> 8, tp = ti & 255;
-        if (B.kind != PD_MAT_SKIP && a.deformed[b]) {
+        if (B.kind != PD_MAT_SKIP && (a.all_def || a.deformed[b])) {
             V4 xp, up;
             Tr<R>::template load_rec<NC>(a.xu + 2 * p, xp, up);
             if (B.kind == PD_MAT_BOND_BASED) {
-                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, d, cp, f[0], f[1], f[2],
+                bond_gather<R, PD_MAT_BOND_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, pp0, xp, up, d, cp, f[0], f[1], f[2],
                                                                            stg);
             } else if (EPK && B.kind == PD_MAT_ELASTO_PLASTIC) {
                 if constexpr (EPK)
-                    bond_gather<R, PD_MAT_ELASTO_PLASTIC, kBreak, WPS, U, NC>(a, p, w, B, tp, xp, up, d, cp, f[0], f[1],
+                    bond_gather<R, PD_MAT_ELASTO_PLASTIC, kBreak, WPS, U, NC>(a, p, w, B, tp, pp0, xp, up, d, cp, f[0], f[1],
                                                                               f[2]);
             } else
-                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, xp, up, d, cp, f[0],
+                bond_gather<R, PD_MAT_ORDINARY_STATE_BASED, kBreak, WPS, U, NC, STG>(a, p, w, B, tp, pp0, xp, up, d, cp, f[0],
                                                                                      f[1], f[2], stg);
         }
     }
@@ -899,7 +904,7 @@ __device__ __forceinline__ void td_body(const StepArgs<R> &a, int64_t blk, doubl
         cp = a.cnt[p];
     }
     pdl_enter();
-    const bool ep = ti >= 0 && B.kind == PD_MAT_ELASTO_PLASTIC && a.deformed[ti >> 8];
+    const bool ep = ti >= 0 && B.kind == PD_MAT_ELASTO_PLASTIC && (a.all_def || a.deformed[ti >> 8]);
     double acc = 0.0;
     if (ep) {
         const int tp = ti & 255;
@@ -1624,6 +1629,9 @@ StepArgs<R> args(pd_env *env, Fast<R> &F) {
     a.fb = F.fb.p;
     a.fp = F.fp.p;
     a.deformed = env->deformed.p;
+    a.all_def = 1;
+    for (size_t b = 0; b < env->hb.size(); ++b)
+        if (env->hb[b].kind != PD_MAT_SKIP && !env->deformed_h[b]) a.all_def = 0;
     a.x64 = env->x4.p;
     a.bcbits = F.bcbits.p;
     a.c = (R)(env->dt / 2);
@@ -1992,6 +2000,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     a.ay = F.tune_d.p + N;
     a.az = F.tune_d.p + 2 * N;
     a.deformed = F.ones.p;
+    a.all_def = 1;
     const int64_t nwords = std::max<int64_t>(env->nnz / 32, 1);
     DBuf<uint32_t> twords;
     PD_TRY(twords.alloc(nwords));
