@@ -289,6 +289,26 @@ def test_dependent_launch_is_bit_identical(builder, precision, monkeypatch):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["fp64_serial", "fp64", "fp32c"])
+def test_held_undeformed_block_gets_no_forces(precision):
+    # pd_env_set_deformed(..., hold): a block held undeformed is skipped by
+    # the force kernels (its gate flag is read, since not every block has
+    # deformed), the other block is not: with no force the held block's
+    # velocities stay exactly as they started, in direct launches and in
+    # graph replays alike
+    w = configs.batched_cubes(nspec=2, edge_lo=6, edge_hi=9)
+    n0 = w["materials"][0].general.n
+    env = pb.Env(1, w["materials"], [], [], w["dt"], precision=precision)
+    env.set_deformed(np.array([1, 0], dtype=np.uint8), hold=True)
+    pb.velocity_verlet_step(env, nsteps=5)  # (FP32C keeps v in FP32: compare from here)
+    _, v0, _, _ = env.get_state()
+    pb.velocity_verlet_step(env, nsteps=70)
+    _, v1, _, _ = env.get_state()
+    env.close()
+    assert np.array_equal(v1[:, n0:], v0[:, n0:])
+    assert not np.array_equal(v1[:, :n0], v0[:, :n0])
+
+
 def _two_type_block():
     x, vol = lattice.cuboid(16, 9, 8, 1.0e-3, jitter=2e-5, seed=9)
     t = np.where(x[0] < x[0].mean(), 1, 2).astype(np.int64)
