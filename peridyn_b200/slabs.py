@@ -176,8 +176,12 @@ class SlabRun:
         for (o, s, _, _), (src, _, buf) in zip(self.plan.exchanges, self._idx):
             _abi.check(L.pd_env_pack_halo(self.envs[o]._h, src.data_ptr(), src.numel(), buf.data_ptr()))
         self._sync()
-        for (o, s, _, _), (_, dst, buf) in zip(self.plan.exchanges, self._idx):
-            b = buf if self.devices[o] == self.devices[s] else buf.to(f"cuda:{self.devices[s]}")
+        # copies between devices run on torch's streams: complete them before
+        # the environments' streams unpack
+        bufs = [buf if self.devices[o] == self.devices[s] else buf.to(f"cuda:{self.devices[s]}")
+                for (o, s, _, _), (_, _, buf) in zip(self.plan.exchanges, self._idx)]
+        self._sync()
+        for (o, s, _, _), (_, dst, _), b in zip(self.plan.exchanges, self._idx, bufs):
             _abi.check(L.pd_env_unpack_halo(self.envs[s]._h, dst.data_ptr(), dst.numel(), b.data_ptr()))
         self._sync()
 
@@ -253,14 +257,19 @@ class SlabRank:
         else:
             _abi.check(_abi.lib().pd_env_unpack_halo(self.env._h, idx.data_ptr(), idx.numel(), buf.data_ptr()))
 
-    def exchange(self):
-        torch = _torch()
-        for _, idx, buf, hbuf in self.sends:
-            self._pack(idx, buf)
-            if hbuf is not None:
-                hbuf.copy_(buf, non_blocking=True)
+    def _sync(self):
+        # the environment's stream (pack/unpack) and torch's stream (copies,
+        # NCCL) are not ordered with each other: wait for the whole device
         if str(self.device).startswith("cuda"):
-            torch.cuda.synchronize(self.device)
+            _torch().cuda.synchronize(self.device)
+
+    def exchange(self):
+        for _, idx, buf, _ in self.sends:
+            self._pack(idx, buf)
+        self._sync()
+        if self.host_wire:
+            for _, _, buf, hbuf in self.sends:
+                hbuf.copy_(buf)
         ops = [self.dist.P2POp(self.dist.isend, buf if hbuf is None else hbuf, peer)
                for peer, _, buf, hbuf in self.sends]
         ops += [self.dist.P2POp(self.dist.irecv, buf if hbuf is None else hbuf, peer)
@@ -268,9 +277,11 @@ class SlabRank:
         if ops:
             for r in self.dist.batch_isend_irecv(ops):
                 r.wait()
-        for _, idx, buf, hbuf in self.recvs:
-            if hbuf is not None:
-                buf.copy_(hbuf, non_blocking=True)
+        if self.host_wire:
+            for _, _, buf, hbuf in self.recvs:
+                buf.copy_(hbuf)
+        self._sync()  # received (or copied) halo data complete before the unpack reads it
+        for _, idx, buf, _ in self.recvs:
             self._unpack(idx, buf)
 
     def step(self, nsteps=1):
