@@ -11,15 +11,22 @@ synthetic input.
   e2e       the same run through the public API with host buffers: upload
             of y, v from pinned memory, the run, download of y, v and damage,
             all inside the timed region.
-  roofline  the bond-force kernel's algorithmic bytes per launch over its
-            average launch time: CUDA events around each launch on the
-            library's stream, in one extra run of the same workload right
-            after the timed runs (per-launch events keep the steps out of
-            graph replays, so the timed runs carry none).
+  roofline  algorithmic bytes of one step (per intact directed bond 4.125 B:
+            a 4-byte neighbour index and one intact bit; per particle the
+            state one step must stream: 84 B bond-based FP32C, 168 B FP64;
+            state-based blocks sweep the bonds twice and add 8 B per
+            particle) over the device time of one step, measured in the
+            timed runs themselves: CUDA events on the library's stream
+            around every replay of a captured multi-step graph and around
+            the bond kernels of every directly launched step.
+
+Default workload: 256 independent bond-based cuboids (edges U{12..32} per
+axis, 2.8 M particles, 290 M bonds), 2000 steps in FP32C -- the largest
+single-GPU configuration, larger than L2.
 
 ``--impl reference`` times the CPU restatement of the reference loop
 (oracle/, OpenMP over particles on all host cores) on a bounded sample of
-the same workload.
+the same workload (for the batched workload: its first specimens).
 
 Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
 torch.distributed.run, one rank per GPU, each rank advancing its own
@@ -62,10 +69,23 @@ def build_workload(name, args):
     raise SystemExit(f"unknown workload {name}")
 
 
-# Algorithmic bytes of one bond-force launch: the bond storage the walk must
-# read (one intact bit per bond slot plus the neighbour-index array: one
-# int32 per (slot, particle) in explicit slices, one per slot in stencil
-# slices) and per particle the state the kernel streams (listed per
+def step_bytes(intact_bonds, particles, precision, lps):
+    """Algorithmic bytes of one step: per intact directed bond a 4-byte
+    neighbour index plus its intact bit (4.125 B), counted once per bond
+    sweep (twice for state-based blocks: dilatation and force); per
+    particle the state a step streams -- FP32C bond-based: x, u read, u
+    written (3 x 12 B) plus the FP64 position accumulator read and written
+    (2 x 24 B) = 84 B; FP64: x 24 + y, v, a read and written (6 x 24) =
+    168 B; state-based blocks add the dilatation written and read (8 B)."""
+    sweeps = 2 if lps else 1
+    per_particle = (84 if precision == "fp32c" else 168) + (8 if lps else 0)
+    return sweeps * 4.125 * intact_bonds + per_particle * particles
+
+
+# The layout's own byte count of one bond-force launch: the bond storage the
+# walk must read (one intact bit per bond slot plus the neighbour-index
+# array: one int32 per (slot, particle) in explicit slices, one per slot in
+# stencil slices) and per particle the state the kernel streams (listed per
 # precision below).
 def bond_bytes(layout, ep=False):
     # elasto-plastic: per slot the plastic strain read and written (8 + 8)
@@ -108,11 +128,13 @@ def advance(env, work, nsteps):
 def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
     """Error of a throughput-mode run against the serial-order FP64 path
     (bit-identical to the CPU oracle) over the same run; for the contact
-    workload, whose serial run would take minutes, against the one-pass FP64
-    GPU path."""
+    workload and workloads above 200 k particles, whose serial runs would
+    take minutes, against the one-pass FP64 GPU path (within 1e-10 of the
+    oracle in the tests)."""
     import peridyn_b200 as pb
 
-    ref_prec = "fp64" if work["contacts"] else "fp64_serial"
+    big = sum(m.general.n for m in work["materials"]) > 200000
+    ref_prec = "fp64" if (work["contacts"] or big) else "fp64_serial"
     ref = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision=ref_prec,
                  device=device)
     if work["bcs"]:
@@ -122,6 +144,7 @@ def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
     advance(ref, work, sim_steps)
     yr, vr, _, _ = ref.get_state()
     yf, vf, _, _ = env_fast.get_state()
+    dr, df = pb.cal_damage(ref), pb.cal_damage(env_fast)
     x = np.hstack([m.general.x for m in work["materials"]])
     mism = 0
     broken = 0
@@ -136,7 +159,7 @@ def accuracy_vs_serial(work, precision, sim_steps, env_fast, device):
           "fp64_serial GPU path (bit-identical to the CPU oracle)")
     return {"vs": vs, "vv_steps": int(sim_steps),
             "displacement_rel_l2": l2(yf - x, yr - x), "velocity_rel_l2": l2(vf, vr),
-            "broken_bonds_fp64": broken, "broken_bond_mismatch": mism}
+            "damage_rel_l2": l2(df, dr), "broken_bonds_fp64": broken, "broken_bond_mismatch": mism}
 
 
 class ClockSampler:
@@ -325,10 +348,27 @@ def run_serving(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def cpu_workload(work, max_particles=120000):
+    """The bounded sample of a workload the CPU arms time: the batched
+    workload's first specimens up to about max_particles particles (the
+    specimens are independent, so its per-bond rate is the workload's);
+    other workloads whole."""
+    mats = work["materials"]
+    if not work["workload"].startswith("batched") or len(mats) <= 1:
+        return work, work["workload"]
+    n, k = 0, 0
+    while k < len(mats) and (k == 0 or n + mats[k].general.n <= max_particles):
+        n += mats[k].general.n
+        k += 1
+    sub = dict(work)
+    sub["materials"] = mats[:k]
+    return sub, f"first {k} of {len(mats)} specimens ({n} particles) of {work['workload']}"
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    work = build_workload(args.workload, args)
+    work, sample = cpu_workload(build_workload(args.workload, args))
     nthreads = cpu_threads(work)
     per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
     vals = []
@@ -342,10 +382,10 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": work["workload"], "precision": "fp64", "particles": None},
+            "config": {"workload": build_workload(args.workload, args)["workload"], "precision": "fp64",
+                       "particles": None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
-                             "sample": f"{samples[0][0]} velocity-Verlet steps per bench step of "
-                                       f"{work['workload']} "
+                             "sample": f"{samples[0][0]} velocity-Verlet steps per bench step of {sample} "
                                        + ("(OpenMP, atomic scatter)" if nthreads > 1 else "(single thread)")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -357,7 +397,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lps_bar",
+    ap.add_argument("--workload", default="batched",
                     choices=["lps_bar", "pmb_cube", "batched", "disk_impact", "elasto_plastic", "serving"])
     ap.add_argument("--jobs", type=int, default=48, help="serving: jobs per stream")
     ap.add_argument("--precision", default="fp32c", choices=["fp64_serial", "fp64", "fp32c"])
@@ -368,7 +408,11 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--persist", action="store_true",
+                    help="run flip-free stretches as one persistent cooperative launch (PD_PERSIST=1)")
     args = ap.parse_args()
+    if args.persist:
+        os.environ["PD_PERSIST"] = "1"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -394,8 +438,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     work = build_workload(args.workload, args)
     sim_steps = args.sim_steps or work["steps"]
+    t_setup = time.perf_counter()
     env = pb.Env(1, work["materials"], work["contacts"], work["bcs"], work["dt"], precision=args.precision,
                  device=local)
+    setup_s = time.perf_counter() - t_setup  # assembly + finalize (families, layout, weighted volumes)
     L = _abi.lib()
     stream_ptr = ctypes_void()
     _abi.check(L.pd_env_stream(env._h, ctypes.byref(stream_ptr)))
@@ -429,15 +475,21 @@ def main():
     for _ in range(args.warmup):
         reset()
         one_run()
-    # timed: device-resident
+    # timed: device-resident; CUDA events on the library's stream bracket
+    # every graph replay / direct step inside the run (pd_env_profile), which
+    # times the bond kernels in the launch path the run takes
     times = []
     bonds = []
+    prof_total_ms, prof_steps = 0.0, 0
+    prof_ms = ctypes_double()
+    prof_n = ctypes_i64()
     launches0 = _abi.kernel_launches()
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
             reset()
             b0 = env.num_bonds()
             flush.zero_()
+            _abi.check(L.pd_env_profile(env._h, 1))
             torch.cuda.synchronize()
             if dist is not None:
                 dist.barrier()
@@ -448,20 +500,14 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
+            _abi.check(L.pd_env_profile_read(env._h, ctypes.byref(prof_ms), ctypes.byref(prof_n)))
+            _abi.check(L.pd_env_profile(env._h, 0))
+            prof_total_ms += prof_ms.value
+            prof_steps += prof_n.value
             b1 = env.num_bonds()
             bonds.append(0.5 * (b0 + b1) * sim_steps)
             bonds_start = b0
     launches = _abi.kernel_launches() - launches0
-    # one more, untimed run with CUDA events around every bond-kernel launch
-    # (direct launches: per-launch events keep the steps out of graphs)
-    reset()
-    _abi.check(L.pd_env_profile(env._h, 1))
-    one_run()
-    torch.cuda.synchronize()
-    prof_ms = ctypes_double()
-    prof_n = ctypes_i64()
-    _abi.check(L.pd_env_profile_read(env._h, ctypes.byref(prof_ms), ctypes.byref(prof_n)))
-    _abi.check(L.pd_env_profile(env._h, 0))
     t_total, total_bonds = replicas.reduce_timing(sum(times), sum(bonds), dist, "cuda")
     value = total_bonds / t_total
     # end-to-end through the public API with host buffers
@@ -500,13 +546,16 @@ def main():
     accuracy = None
     if args.precision != "fp64_serial" and rank == 0 and not args.no_accuracy:
         accuracy = accuracy_vs_serial(work, args.precision, sim_steps, env, local)
-    # roofline of the bond-force kernel
+    # roofline of one step (bond-based: the fused k_step launch)
+    n_real = sum(m.general.n for m in work["materials"])
     n_int = sum(((m.general.n + 31) // 32) * 32 for m in work["materials"])
     layout = env.layout()
     shape = env.kernel_shape()
-    bytes_launch = bond_bytes(layout, ep) + n_int * particle_bytes(args.precision, lps)
-    avg_ms = prof_ms.value / max(1, prof_n.value)
-    achieved = bytes_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
+    mean_bonds = sum(bonds) / max(1, len(bonds)) / sim_steps
+    bytes_step = step_bytes(mean_bonds, n_real, args.precision, lps)
+    bytes_layout = bond_bytes(layout, ep) + n_int * particle_bytes(args.precision, lps)
+    avg_ms = prof_total_ms / max(1, prof_steps)
+    achieved = bytes_step / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -533,12 +582,20 @@ def main():
                    "intact_bonds": int(bonds_start), "vv_steps_per_step": int(sim_steps), "dt": work["dt"],
                    "l2": "256 MB buffer written between timed iterations",
                    "parallelism": f"specimen replicas x{world}" if world > 1 else "1 GPU"},
-        "hbm_gbs_algorithmic": bytes_launch * sim_steps * args.steps / t_total / 1e9,
+        "hbm_gbs_algorithmic": bytes_step * sim_steps * args.steps / t_total / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "k_force_serial" if args.precision == "fp64_serial" else "k_step (fused bond force + velocity-Verlet)",
-                     "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms, "launches_timed": int(prof_n.value),
-                     "launch_timing": "CUDA events around each launch, one extra run after the timed runs",
+                     "kernel": ("k_force_serial" if args.precision == "fp64_serial" else
+                                "k_theta + k_step (dilatation, fused bond force + velocity-Verlet)" if lps else
+                                "k_step (fused bond force + velocity-Verlet), one launch per step"),
+                     "bytes_per_launch": bytes_step,
+                     "byte_model": "per step: 4.125 B per intact directed bond per bond sweep + "
+                                   + ("84" if args.precision == "fp32c" else "168")
+                                   + (" + 8" if lps else "") + " B per particle",
+                     "layout_bytes_per_launch": bytes_layout,
+                     "avg_launch_ms": avg_ms, "launches_timed": int(prof_steps),
+                     "launch_timing": "CUDA events on the library's stream around every graph replay and "
+                                      "every directly launched step of the timed runs",
                      "peak_source": f"{peak_src} MEASURED_PEAKS.json hbm_gbs" if peak_src == "measured"
                      else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -547,15 +604,20 @@ def main():
         "accuracy": accuracy,
     }
     line["config"]["bond_layout"] = layout
+    line["config"]["slot_efficiency"] = float(bonds_start) / max(1, layout["slots"])
+    line["config"]["setup_s"] = setup_s
     line["config"]["kernel_shape"] = {"warps_per_slice": shape[0], "unroll": shape[1], "chosen_by":
                                       "PD_KERNEL_SHAPE" if os.environ.get("PD_KERNEL_SHAPE") else "autotuner"}
+    line["config"]["launch_path"] = ("persistent cooperative kernel over flip-free runs" if args.persist else
+                                     "CUDA graphs of 32 steps" if not work["contacts"] else "direct launches")
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:
-        nth = cpu_threads(work)
-        rate, n, dt = cpu_sample(work, args.cpu_sample_s, nth)
+        sub, sample = cpu_workload(work)
+        nth = cpu_threads(sub)
+        rate, n, dt = cpu_sample(sub, args.cpu_sample_s, nth)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": nth, "kind": "port",
-                                "sample": f"{n} velocity-Verlet steps of {work['workload']} in {dt:.1f} s "
+                                "sample": f"{n} velocity-Verlet steps of {sample} in {dt:.1f} s "
                                           + ("(OpenMP over particles, atomic scatter)" if nth > 1 else
                                              "(single thread)")}
     env.close()

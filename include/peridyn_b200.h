@@ -232,6 +232,15 @@ PD_API pd_status pd_env_apply_bc_at0(pd_env *env);
 PD_API pd_status pd_env_update_acc(pd_env *env);
 /* nsteps x velocity_verlet_step! (velocity_verlet.jl:57-89). */
 PD_API pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps);
+/* pd_env_vv_steps without waiting for the steps to finish (extension, no
+ * reference counterpart): enqueues them on the environment's stream and
+ * returns.  An environment whose blocks have all deformed, or whose gate
+ * is held (pd_env_set_deformed), needs no read-back of the gate flags;
+ * otherwise the call waits as pd_env_vv_steps does.  Errors of the
+ * enqueued work surface at the next waiting call.  The slab decomposition
+ * uses it to run slabs on several GPUs at once and to order its halo
+ * exchange with events. */
+PD_API pd_status pd_env_vv_steps_async(pd_env *env, int64_t nsteps);
 /* minimize! (minimize.jl:105-231): one QSDrag solver step.  *iters
  * receives the iteration count (NULL allowed). */
 PD_API pd_status pd_env_qsdrag(pd_env *env, double step_size, double drag, int64_t max_iter,
@@ -307,7 +316,8 @@ PD_API pd_status pd_force_density_device(pd_env *env, int64_t block, double *f_d
  * particles (padded to a multiple of 32), larger blocks get
  * PD_ERR_UNSUPPORTED.  All calls on one GPU share that array, so calls that
  * overlap on the GPU race; the first call on each device looks the array
- * up and should precede any stream capture on that device. */
+ * up and should precede any stream capture on that device.  The address is
+ * kept until exit: do not reset the device while the library is loaded. */
 PD_API pd_status pd_force_density_device_static(pd_env *env, int64_t block, double *f_dev,
                                                 const double *y_dev, void *stream);
 
@@ -318,9 +328,12 @@ PD_API pd_status pd_force_density_device_static(pd_env *env, int64_t block, doub
 PD_API pd_status pd_env_stream(pd_env *env, void **stream);
 /* Total kernel launches issued by the library since it was loaded. */
 PD_API pd_status pd_kernel_launches(int64_t *count);
-/* enable != 0: bracket every bond-force kernel launch with CUDA events;
- * resets the accumulated time.  pd_env_profile_read returns the summed
- * device time (ms) and the number of timed launches since enabling. */
+/* enable != 0: bracket the bond kernels of every step (dilatation,
+ * td_norm2 and force; in the throughput modes each replay of a captured
+ * multi-step graph as a whole) with CUDA events on the environment's
+ * stream, without changing how steps are launched; resets the accumulated
+ * time.  pd_env_profile_read returns the summed device time (ms) and the
+ * number of steps it covers since enabling. */
 PD_API pd_status pd_env_profile(pd_env *env, int32_t enable);
 PD_API pd_status pd_env_profile_read(pd_env *env, double *total_ms, int64_t *launches);
 /* Kernel shape of the throughput modes (extension): warps per 32-particle

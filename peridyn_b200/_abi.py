@@ -148,6 +148,7 @@ _SIGNATURES = {
     "pd_force_density_device_static": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_vp, c_vp, c_vp]),
     "pd_env_stream": (ctypes.c_int32, [c_vp, ctypes.POINTER(c_vp)]),
     "pd_kernel_launches": (ctypes.c_int32, [c_i64p]),
+    "pd_env_vv_steps_async": (ctypes.c_int32, [c_vp, ctypes.c_int64]),
     "pd_env_profile": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
     "pd_env_profile_read": (ctypes.c_int32, [c_vp, c_dp, c_i64p]),
     "pd_env_stage_state": (ctypes.c_int32, [c_vp, ctypes.c_int32]),

@@ -1,8 +1,11 @@
 """Build libperidyn_b200.so in-tree for sm_100a with nvcc.
 
-The exact-arithmetic translation units (the serial-order FP64 path, the
-contact models and the solver pieces) are compiled with -fmad=false so
-that no multiply-add is fused; the throughput path (pd_fast.cu) keeps FMA.
+Every translation unit is compiled with -fmad=false, so the compiler fuses
+no multiply-add on its own: the exact-arithmetic units (the serial-order
+FP64 path, the contact models, the solver pieces) must not fuse any, and
+the throughput path (pd_fast.cu) writes its multiply-adds explicitly
+(fmaf/fma), so that every launch path computes the same numbers whatever
+the compiler's scheduling.
 """
 import os
 import subprocess

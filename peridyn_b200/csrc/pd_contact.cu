@@ -109,6 +109,10 @@ __device__ __forceinline__ double jl_fld(double x, double y) {
 }
 
 // ------------------------------- reductions ------------------------------
+// Fixed partial-reduction width (blocks of the partial kernel, partials
+// combined in block order): a constant rather than the device's SM count,
+// so that the order of the reduction -- and its rounding -- does not depend
+// on the GPU it runs on.
 constexpr int kMMBlocks = 148;
 __global__ void __launch_bounds__(kT)
     k_minmax_partial(int64_t first, int64_t n, const double4 *__restrict__ y, double *__restrict__ part) {

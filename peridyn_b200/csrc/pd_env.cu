@@ -55,9 +55,11 @@ void prof_begin(pd_env *env, cudaStream_t st) {
     cudaEventRecord(env->prof_ev[env->prof_used], st);
 }
 
-void prof_end(pd_env *env, cudaStream_t st) {
+void prof_end(pd_env *env, cudaStream_t st, int32_t steps) {
     if (!env->prof || env->prof_used + 2 > env->prof_ev.size()) return;
     cudaEventRecord(env->prof_ev[env->prof_used + 1], st);
+    if (env->prof_w.size() < env->prof_ev.size() / 2) env->prof_w.resize(env->prof_ev.size() / 2);
+    env->prof_w[env->prof_used / 2] = steps;
     env->prof_used += 2;
 }
 
@@ -614,6 +616,10 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     env->stencil_slices = nst;
     cudaStream_t st = env->st;
     const int64_t nw = std::max<int64_t>(nwords, 1);
+    // zero entries past the end: the stencil walks load the offsets of the
+    // next slots ahead of use and may read up to kNbrPad entries beyond a
+    // slice's own (those values are never used)
+    nbr.resize(nbr.size() + kNbrPad, 0);
     PD_TRY(env->sinfo.alloc(S + 1));
     PD_TRY(env->nbr.alloc((int64_t)nbr.size()));
     PD_TRY(env->words[0].alloc(nw));
@@ -1322,7 +1328,7 @@ static pd_status prof_collect(pd_env *env) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, env->prof_ev[k], env->prof_ev[k + 1]));
         env->prof_ms += ms;
-        env->prof_launches += 1;
+        env->prof_launches += env->prof_w[k / 2];
     }
     env->prof_used = 0;
     return PD_OK;

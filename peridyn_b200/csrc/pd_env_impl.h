@@ -214,6 +214,7 @@ struct pd_env {
     // optional CUDA-event timing of the bond-force kernel launches
     bool prof = false;
     std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+    std::vector<int32_t> prof_w;       // steps covered by each pair
     size_t prof_used = 0;
     double prof_ms = 0.0;
     int64_t prof_launches = 0;
@@ -241,10 +242,11 @@ struct pd_env {
 };
 
 namespace pd {
-// Bracket one launch of the bond-force kernel with timing events (no-op
-// unless profiling is enabled on the environment).
+// Bracket the bond kernels of one step, or one graph replay of `steps`
+// steps, with timing events (no-op unless profiling is enabled on the
+// environment).
 void prof_begin(pd_env *env, cudaStream_t st);
-void prof_end(pd_env *env, cudaStream_t st);
+void prof_end(pd_env *env, cudaStream_t st, int32_t steps = 1);
 pd_status contacts_finalize(pd_env *env);
 pd_status contacts_update_neighs(pd_env *env, int64_t max_part);
 pd_status contacts_force(pd_env *env);
@@ -255,6 +257,11 @@ pd_status sync_state_to_fp64(pd_env *env, bool invalidate = true);
 void fast_release(pd_env *env);
 pd_status fast_vv_steps(pd_env *env, int64_t nsteps);
 pd_status fast_vv_enqueue(pd_env *env, int64_t nsteps);
+// Serving batches: whether an environment may be advanced in shared
+// launches with others, and nsteps of a batch of them (one precision) on
+// stream st.
+bool fast_batchable(pd_env *env);
+pd_status fast_batch_steps(pd_env *const *envs, int n_envs, int64_t nsteps, cudaStream_t st);
 pd_status fast_land_flags(pd_env *env);
 // Device bytes an assembled environment will hold once finalized (upper
 // estimate from particle counts and family rows; for admission control).

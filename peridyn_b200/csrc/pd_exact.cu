@@ -661,6 +661,9 @@ __global__ void k_damage(int64_t N, const SliceInfo *__restrict__ si,
     damage[p] = 1.0 - (double)c / (double)intact0[p];
 }
 
+// Fixed partial-reduction width, independent of the device's SM count so
+// that the summation order (and the rounding of the gate norms) is the same
+// on every GPU.
 constexpr int kSumBlocks = 148;
 __global__ void __launch_bounds__(256)
     k_sum4_partial(int64_t N, const double4 *__restrict__ a, double *__restrict__ partials) {

@@ -422,6 +422,113 @@ __device__ __forceinline__ void bond_walk(const StepArgs<R> &a, int64_t p, int32
     }
 }
 
+// U consecutive stencil offsets in one load.  p is 4 U-byte aligned: a
+// slice's offsets start at a multiple of 32 entries, a warp's slot range at
+// a multiple of 4 (len is a multiple of 32, split over 1, 2, 4 or 8 warps),
+// and the walks step through it U slots at a time.
+template <int U>
+__device__ __forceinline__ void load_offsets(const int32_t *p, int32_t (&o)[U]) {
+    if constexpr (U == 4) {
+        const int4 v = __ldg(reinterpret_cast<const int4 *>(p));
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    } else if constexpr (U == 2) {
+        const int2 v = __ldg(reinterpret_cast<const int2 *>(p));
+        o[0] = v.x;
+        o[1] = v.y;
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) o[u] = __ldg(p + u);
+    }
+}
+
+// The stencil walk of bond_walk (bond-based and state-based blocks, records
+// from global memory) with the slot offsets loaded one group of U slots
+// ahead: the offsets of the next group are in flight while the current
+// group's records are fetched, so a slot waits for one memory access (its
+// record) instead of two in a row (offset, then record).  The neighbour of
+// slot j is p + o_j (o_j shared by the warp), its record xb + 2 o_j.  Same
+// arithmetic in the same slot order as bond_walk.
+template <class R, int KIND, bool kBreak, int U, bool MULTI, bool NC>
+__device__ __forceinline__ void bond_walk_st(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1,
+                                             const int32_t *nb, uint32_t *wp, const FBlock<R> &B, int tp,
+                                             const FPair<R> &pp0, typename Tr<R>::V4 xp, typename Tr<R>::V4 up,
+                                             R Ap, R Bp, R &fx, R &fy, R &fz) {
+    using V4 = typename Tr<R>::V4;
+    FPair<R> pp = pp0;
+    const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
+    const V4 *xb = a.xu + 2 * p;
+    float2 fxy = make_float2(0.f, 0.f);
+    // one slot: kinematics, stretch test, force term into the accumulators;
+    // returns whether the bond stays within the critical stretch
+    auto slot = [&](bool live, const V4 &xq, const V4 &uq, int32_t o) -> bool {
+        const Kin<R> k(xq, uq, nx, nu);
+        const R num = k.num, xx2 = k.xx2;
+        const R wq = xq.w;
+        const R lx = Tr<R>::sqrt_(xx2), ly = Tr<R>::sqrt_(xx2 + num);
+        const R dl = Tr<R>::fma_(ly, lx, xx2);
+        if (MULTI && live) pp = a.fp[B.pair_base + tp + (a.tinfo[p + o] & 255) * B.nt];
+        const bool ok = num < pp.cs * dl;
+        R tn;
+        if (KIND == PD_MAT_BOND_BASED) {
+            tn = num;
+        } else {
+            const typename Tr<R>::V2 mq = a.mab[p + o];
+            tn = Tr<R>::fma_(pp.k35 * (Ap + mq.x), dl, pp.g15 * num * (Bp + mq.y));
+        }
+        const R coef = (live && ok) ? tn * wq * Tr<R>::rcp(dl * ly) : R(0);
+        if constexpr (sizeof(R) == 4) k.accumulate(coef, fxy, fz);
+        else k.accumulate(coef, fx, fy, fz);
+        return ok;
+    };
+    for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
+        wend = min(k1, (w0 | 31) + 1);
+        uint32_t *wptr = wp + 32 * (w0 >> 5);
+        const int32_t kend = wend - w0;
+        const uint32_t bits = range_bits(*wptr, w0, kend);
+        if (!bits) continue;
+        const int32_t *np = nb + w0;
+        uint32_t okm = 0;
+        int32_t o[U];
+        load_offsets<U>(np, o);  // past the chunk: padded array, unused values
+        int32_t j = 0;
+        for (; j + U <= kend; j += U) {
+            V4 xq[U], uq[U];
+            int32_t oc[U];  // this group's offsets (state-based and multi-type terms read p + o)
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                Tr<R>::template load_rec<NC>(xb + 2 * (int64_t)o[u], xq[u], uq[u]);
+                oc[u] = o[u];
+            }
+            // the next group's offsets, in flight while this group computes
+            load_offsets<U>(np + j + U, o);
+            const uint32_t bg = bits >> j;  // bit u <-> slot j + u
+            uint32_t okg = 0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (slot((bg & (1u << u)) != 0u, xq[u], uq[u], oc[u])) okg |= 1u << u;
+            okm |= okg << j;
+        }
+        // remaining kend - j < U slots; o[] holds their offsets
+#pragma unroll
+        for (int u = 0; u < U - 1; ++u) {
+            if (j + u < kend) {
+                V4 xq, uq;
+                Tr<R>::template load_rec<NC>(xb + 2 * (int64_t)o[u], xq, uq);
+                if (slot(((bits >> (j + u)) & 1u) != 0u, xq, uq, o[u])) okm |= 1u << (j + u);
+            }
+        }
+        const uint32_t brk = bits & ~okm;
+        if (kBreak && brk) atomicAnd(wptr, ~(brk << (w0 & 31)));
+    }
+    if constexpr (sizeof(R) == 4) {
+        fx += fxy.x;
+        fy += fxy.y;
+    }
+}
+
 template <class R, int KIND, bool kBreak, int WPS, int U, bool NC = true, bool STG = false>
 __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int w, const FBlock<R> &B, int tp,
                                             const FPair<R> &pp0, typename Tr<R>::V4 xp, typename Tr<R>::V4 up, const SliceInfo &d,
@@ -450,15 +557,22 @@ __device__ __forceinline__ void bond_gather(const StepArgs<R> &a, int64_t p, int
             return;
         }
     }
+    constexpr bool kAhead = KIND != PD_MAT_ELASTO_PLASTIC;  // stencil walks with offsets loaded ahead
     if (B.nt > 1) {
-        if (d.mode == kStencil)
+        if (kAhead && d.mode == kStencil)
+            bond_walk_st<R, KIND, kBreak, U, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
+                                                       fy, fz);
+        else if (d.mode == kStencil)
             bond_walk<R, KIND, kBreak, WPS, U, true, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
                                                            fy, fz, nullptr, nullptr, rtdp);
         else
             bond_walk<R, KIND, kBreak, WPS, U, false, true, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, B, tp, pp0, xp, up,
                                                             Ap, Bp, fx, fy, fz, nullptr, nullptr, rtdp);
     } else {
-        if (d.mode == kStencil)
+        if (kAhead && d.mode == kStencil)
+            bond_walk_st<R, KIND, kBreak, U, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
+                                                        fy, fz);
+        else if (d.mode == kStencil)
             bond_walk<R, KIND, kBreak, WPS, U, true, false, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, B, tp, pp0, xp, up, Ap, Bp, fx,
                                                             fy, fz, nullptr, nullptr, rtdp);
         else
@@ -721,9 +835,8 @@ __device__ __forceinline__ void integrate(const StepArgs<R> &a, int64_t p, R fx,
 
 // First half of a step (velocity_verlet.jl:62-69) from the stored force.
 template <class R>
-__global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
+__device__ __forceinline__ void prologue_body(const StepArgs<R> &a, int64_t p) {
     using V4 = typename Tr<R>::V4;
-    const int64_t p = blockIdx.x * (int64_t)kT + threadIdx.x;
     if (p >= a.N) return;
     if (a.tinfo[p] < 0) {
         a.xn[2 * p + 1] = V4{};
@@ -740,6 +853,11 @@ __global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
     if (bits) bc_position(a, p, bits, u0, u1, u2);
     a.v[p] = V4{v0, v1, v2, R(0)};
     store_u(a, p, u0, u1, u2);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kT) k_prologue(StepArgs<R> a) {
+    prologue_body(a, blockIdx.x * (int64_t)kT + threadIdx.x);
 }
 
 template <class R, int WPS, int U, bool ST, bool NC = true, bool STG = false>
@@ -778,6 +896,53 @@ __device__ __forceinline__ R theta_walk(const StepArgs<R> &a, int64_t p, int32_t
     return acc;
 }
 
+// theta_walk over a stencil slice with the slot offsets loaded one group of
+// U slots ahead (as bond_walk_st); same terms in the same order.
+template <class R, int U, bool NC>
+__device__ __forceinline__ R theta_walk_st(const StepArgs<R> &a, int64_t p, int32_t k0, int32_t k1,
+                                           const int32_t *nb, const uint32_t *wp, typename Tr<R>::V4 xp,
+                                           typename Tr<R>::V4 up) {
+    using V4 = typename Tr<R>::V4;
+    R acc = 0;
+    const V4 nx{-xp.x, -xp.y, -xp.z, R(0)}, nu{-up.x, -up.y, -up.z, R(0)};
+    const V4 *xb = a.xu + 2 * p;
+    auto term = [&](const V4 &xq, const V4 &uq, bool live) {
+        const Kin<R> k(xq, uq, nx, nu);
+        const R num = k.num;
+        const R lx = Tr<R>::sqrt_(k.xx2), ly = Tr<R>::sqrt_(k.xx2 + num);
+        const R t = num * xq.w * Tr<R>::rcp(ly + lx);
+        acc += live ? t : R(0);
+    };
+    for (int32_t w0 = k0, wend; w0 < k1; w0 = wend) {
+        wend = min(k1, (w0 | 31) + 1);
+        const int32_t kend = wend - w0;
+        const uint32_t bits = range_bits(wp[32 * (w0 >> 5)], w0, kend);
+        if (!bits) continue;
+        const int32_t *np = nb + w0;
+        int32_t o[U];
+        load_offsets<U>(np, o);  // past the chunk: padded array, unused values
+        int32_t j = 0;
+        for (; j + U <= kend; j += U) {
+            V4 xq[U], uq[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) Tr<R>::template load_rec<NC>(xb + 2 * (int64_t)o[u], xq[u], uq[u]);
+            load_offsets<U>(np + j + U, o);
+            const uint32_t bg = bits >> j;
+#pragma unroll
+            for (int u = 0; u < U; ++u) term(xq[u], uq[u], (bg & (1u << u)) != 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < U - 1; ++u) {
+            if (j + u < kend) {
+                V4 xq, uq;
+                Tr<R>::template load_rec<NC>(xb + 2 * (int64_t)o[u], xq, uq);
+                term(xq, uq, (bits >> (j + u)) & 1u);
+            }
+        }
+    }
+    return acc;
+}
+
 // Dilatation (peri.jl:155-172): theta_p = 3/m_p sum_q e_pq V_q over intact
 // bonds; stores theta_p/m_p for the force pass.  Same warp split as k_step.
 template <class R, int WPS, int U, bool NC, bool STG = false, bool PDL = false>
@@ -811,7 +976,7 @@ __device__ __forceinline__ void theta_body(const StepArgs<R> &a, int64_t blk, R 
             acc = theta_walk<R, WPS, U, true, NC, true>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up, stg,
                                                         a.spos + d.nbr);
         else if (d.mode == kStencil)
-            acc = theta_walk<R, WPS, U, true, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up);
+            acc = theta_walk_st<R, U, NC>(a, p, k0, k1, a.nbr + d.nbr, wp, xp, up);
         else
             acc = theta_walk<R, WPS, U, false, NC>(a, p, k0, k1, a.nbr + d.nbr + (p & 31), wp, xp, up);
     }
@@ -832,6 +997,71 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         __syncthreads();
     }
     theta_body<R, WPS, U, true, false, true>(a, slice_of_block<SPB>(a), sh, arrive);
+}
+
+// ---------------------------------------------------------------------
+// Job-table kernels of the serving loop: one launch advances up to
+// kJobsPerLaunch resident jobs of a batch (separate environments, each with
+// its own buffers, time step and parameters).  The table is the launch's
+// parameter (t.a[j]: job j's step arguments, t.bstart[j]: its first block,
+// t.bstart[n] the grid size), read in place from the parameter bank
+// (__grid_constant__), so the job's arguments cost no registers, as in the
+// single-environment kernels.  A block finds its job by a binary search
+// over t.bstart and runs the same body as the single-environment kernel
+// over its own slices, so a job computes the same numbers in a batch as
+// alone.
+// ---------------------------------------------------------------------
+constexpr int kJobsPerLaunch = 16;  // 16 x 1856-byte arguments: within the 32 KB parameter limit
+template <class R>
+struct JobTable {
+    StepArgs<R> a[kJobsPerLaunch];
+    int32_t bstart[kJobsPerLaunch + 1];
+    int32_t n;
+};
+
+template <class R>
+__device__ __forceinline__ int job_of_block(const JobTable<R> &t, int32_t b) {
+    int lo = 0, hi = t.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.bstart[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class R, int WPS, int U, int MODE>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) != 4 ? 1 : U <= 2 ? Split<WPS>::MINB_U2 : Split<WPS>::MINB)
+    k_step_jobs(const __grid_constant__ JobTable<R> t) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][3][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    const int j = job_of_block(t, (int32_t)blockIdx.x);
+    step_body<R, WPS, U, MODE, true>(t.a[j], (int32_t)blockIdx.x - t.bstart[j], sh, arrive);
+}
+
+template <class R, int WPS, int U>
+__global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB_THETA : 1)
+    k_theta_jobs(const __grid_constant__ JobTable<R> t) {
+    constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
+    __shared__ R sh[WPS > 1 ? NW : 1][1][32];
+    __shared__ int arrive[SPB];
+    if (WPS > 1) {
+        if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
+        __syncthreads();
+    }
+    const int j = job_of_block(t, (int32_t)blockIdx.x);
+    theta_body<R, WPS, U, true>(t.a[j], (int32_t)blockIdx.x - t.bstart[j], sh, arrive);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kT) k_prologue_jobs(const __grid_constant__ JobTable<R> t) {
+    const int j = job_of_block(t, (int32_t)blockIdx.x);
+    prologue_body(t.a[j], ((int32_t)blockIdx.x - t.bstart[j]) * (int64_t)kT + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------
@@ -1121,7 +1351,10 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
     }
 }
 
-// Deformed gate on y = x + u (general_material.jl:243-255).
+// Deformed gate on y = x + u (general_material.jl:243-255).  kGB: the
+// largest number of CTAs sharing one block's partial norms -- a fixed width
+// rather than the device's SM count, so the norms' summation order does not
+// depend on the GPU.
 constexpr int kGB = 148, kGT = 256;
 // One GateItem per block still undeformed; grid.y walks the list and
 // grid.x = gx CTAs share each block, so any number of blocks is tested in
@@ -1507,9 +1740,17 @@ inline void launch_theta_st(cudaStream_t st, int cfg, StepArgs<float> a) {
 }
 
 // The staged kernels may use up to kStageMaxRecords records of dynamic
-// shared memory; raise their limit once per process.
-inline cudaError_t staged_kernel_attrs() {
-    static cudaError_t status = [] {
+// shared memory; raise their limit once per device (the attribute is a
+// per-device setting), with `device` current.
+constexpr int kAttrDevices = 64;
+std::mutex g_attr_mutex;
+bool g_attr_done[kAttrDevices] = {};
+cudaError_t g_attr_status[kAttrDevices] = {};
+inline cudaError_t staged_kernel_attrs(int device) {
+    if (device < 0 || device >= kAttrDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    if (g_attr_done[device]) return g_attr_status[device];
+    cudaError_t status = [] {
         const int bytes = (int)(kStageMaxRecords * 32);
         cudaError_t e = cudaSuccess;
         auto set = [&](const void *k) {
@@ -1528,6 +1769,8 @@ inline cudaError_t staged_kernel_attrs() {
 #undef PD_STAGED_ATTRS
         return e;
     }();
+    g_attr_done[device] = true;
+    g_attr_status[device] = status;
     return status;
 }
 
@@ -1939,12 +2182,14 @@ void launch_force(pd_env *env, cudaStream_t st, int cfg, const StepArgs<R> &a, b
 // Project autotuner: times every kernel shape on the environment itself
 // (captured graphs of full steps on scratch copies of the state they
 // write) and keeps the fastest.  Results are cached for the life of the
-// process per problem class: particle count in steps of 2^(1/2) (~41 %),
-// bond slots per particle in steps of 8, precision and staging mode, and
-// the passes present (dilatation, td_norm2), so a stream of jobs of
-// similar sizes -- the serving loop -- tunes once per class.
+// process per device and problem class: particle count in steps of
+// 2^(1/2) (~41 %), bond slots per particle in steps of 8, precision and
+// staging mode, and the passes present (dilatation, td_norm2), so
+// environments of similar sizes built one after another on a device tune
+// once per class.  (Served jobs do not come here: the server fixes their
+// shapes from their sizes.)
 std::mutex g_tune_mutex;
-std::map<std::tuple<int64_t, int64_t, int, int>, int> g_tune_cache;
+std::map<std::tuple<int, int64_t, int64_t, int, int>, int> g_tune_cache;
 
 template <class R>
 pd_status autotune(pd_env *env, Fast<R> &F) {
@@ -1952,7 +2197,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     // staged shapes: FP32C, 4 or 8 warps per slice, when some slice has a plan
     const bool ep = any_ep(env);
     const bool can_stage = sizeof(R) == 4 && env->splan_slices > 0 && !ep;
-    if (can_stage) CK(staged_kernel_attrs());
+    if (can_stage) CK(staged_kernel_attrs(env->device));
     auto staged_ok = [&](int w) { return can_stage && (w == 4 || w == 8); };
     if (env->shape) {  // pd_env_set_kernel_shape (+ pd_env_set_record_staging)
         F.wps = env->shape + (env->staging == 1 && staged_ok(env->shape / 10) ? 100 : 0);
@@ -1961,7 +2206,7 @@ pd_status autotune(pd_env *env, Fast<R> &F) {
     const bool lps = need_theta(env);
     const int64_t size_class = (int64_t)std::floor(2.0 * std::log2((double)std::max<int64_t>(env->N, 1)));
     const int64_t slot_class = env->nnz / std::max<int64_t>(env->N, 1) / 8;
-    const auto key = std::make_tuple(size_class, slot_class, env->precision * 4 + env->staging + 1,
+    const auto key = std::make_tuple(env->device, size_class, slot_class, env->precision * 4 + env->staging + 1,
                                      (int)lps + 2 * (int)ep);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -2314,8 +2559,10 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
     }
     // Steps without contacts run as replays of a captured graph of
     // kGraphSteps steps while the BC directions stay constant; the rest
-    // (contacts, direction flips, the last step, profiling) launch directly.
-    const bool graphs = !contacts && !env->prof && !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
+    // (contacts, direction flips, the last step) launch directly.  With
+    // profiling on, timing events bracket each replay (kGraphSteps steps)
+    // and the bond kernels of each direct step.
+    const bool graphs = !contacts && !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
     // With PD_PERSIST=1, once every block has deformed (no gate), flip-free
     // runs go to one persistent cooperative launch when the grid of the
     // chosen shape fits on the device.  Off by default: on B200 the graph
@@ -2342,7 +2589,9 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         }
         if (graphs && nsteps - 1 - s >= kGraphSteps && flip_free_steps(env, kGraphSteps)) {
             PD_TRY(poll_gate_flags(env, F, blocking));
+            prof_begin(env, st);
             PD_TRY(replay_graph(env, F, lps));
+            prof_end(env, st, kGraphSteps);
             s += kGraphSteps;
             continue;
         }
@@ -2358,10 +2607,10 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         a.ts = env->ts;
         gate_launch(env, a, F);
         if (!F.gitems_h.empty()) ++F.gate_runs;
+        if (!contacts) prof_begin(env, st);
         if (lps) launch_theta(st, wps, a);
         if (a.ep) launch_td(st, wps, a);
         if (!contacts) {
-            prof_begin(env, st);
             if (stop) launch_step<R, 2>(st, wps, a);
             else launch_step<R, 1>(st, wps, a);
             prof_end(env, st);
@@ -2420,9 +2669,9 @@ pd_status update_acc_fast(pd_env *env, Fast<R> &F) {
     PD_TRY(autotune(env, F));
     StepArgs<R> a = args(env, F);
     PD_TRY(gate_if_needed(env, a, F));
+    prof_begin(env, env->st);
     if (need_theta(env)) launch_theta(env->st, F.wps, a);
     if (a.ep) launch_td(env->st, F.wps, a);
-    prof_begin(env, env->st);
     launch_step<R, 0>(env->st, F.wps, a);
     prof_end(env, env->st);
     if (a.ep) env->ecur = 1 - env->ecur;
@@ -2497,6 +2746,171 @@ pd_status fast_vv_enqueue(pd_env *env, int64_t nsteps) {
     else PD_TRY(vv_chunk(env, h->f64, nsteps, false));
     h->dirty = true;
     return PD_OK;
+}
+
+namespace {
+
+int64_t step_blocks(int wps, int64_t N) {
+    const int64_t slices = (N + 31) / 32;
+    const int s = wps == 1 ? Split<1>::SPB : wps == 2 ? Split<2>::SPB : 1;
+    return (slices + s - 1) / s;
+}
+
+template <class R, int W>
+void launch_step_jobs(cudaStream_t st, bool last, const JobTable<R> &t) {
+    const unsigned grid = (unsigned)t.bstart[t.n];
+    if (last) k_step_jobs<R, W, Unroll<R>::HI, 2><<<grid, Split<W>::BT, 0, st>>>(t);
+    else k_step_jobs<R, W, Unroll<R>::HI, 1><<<grid, Split<W>::BT, 0, st>>>(t);
+    note_launch();
+}
+
+template <class R, int W>
+void launch_theta_jobs(cudaStream_t st, const JobTable<R> &t) {
+    k_theta_jobs<R, W, Unroll<R>::HI><<<(unsigned)t.bstart[t.n], Split<W>::BT, 0, st>>>(t);
+    note_launch();
+}
+
+template <class R>
+void dispatch_jobs(cudaStream_t st, int wps, bool theta, bool last, const JobTable<R> &t) {
+    switch (wps) {
+        case 1: theta ? launch_theta_jobs<R, 1>(st, t) : launch_step_jobs<R, 1>(st, last, t); break;
+        case 2: theta ? launch_theta_jobs<R, 2>(st, t) : launch_step_jobs<R, 2>(st, last, t); break;
+        case 4: theta ? launch_theta_jobs<R, 4>(st, t) : launch_step_jobs<R, 4>(st, last, t); break;
+        default: theta ? launch_theta_jobs<R, 8>(st, t) : launch_step_jobs<R, 8>(st, last, t); break;
+    }
+}
+
+// nsteps velocity-Verlet steps of every environment in envs (one precision,
+// all batchable) as shared launches on stream st: a prologue over all jobs,
+// then per step the dilatation of the state-based jobs and the fused step of
+// every job, one launch per kernel shape and kJobsPerLaunch jobs.  The steps
+// are those of vv_chunk (prologue, fused steps, a last step that stops
+// after the velocity half kick), so a job's numbers do not depend on its
+// batch.
+template <class R>
+pd_status batch_chunk(pd_env *const *envs, int n_envs, int64_t nsteps, cudaStream_t st,
+                      Fast<R> &(*fast_of)(pd_env *)) {
+    struct Item {
+        pd_env *env;
+        int wps;
+        bool lps;
+        StepArgs<R> a[3];  // prologue, even steps, odd steps
+    };
+    std::vector<Item> items(n_envs);
+    for (int k = 0; k < n_envs; ++k) {
+        pd_env *env = envs[k];
+        Fast<R> &F = fast_of(env);
+        Item &it = items[k];
+        it.env = env;
+        it.wps = F.wps % 100 / 10;
+        it.lps = need_theta(env);
+        const int c0 = F.cur;
+        for (int t = 0; t < 3; ++t) {
+            F.cur = t == 1 ? 1 - c0 : c0;
+            it.a[t] = args(env, F);
+            it.a[t].swz_g = 0;  // block b of a job walks its slice group b
+            it.a[t].dir_vel = it.a[t].dir_pos = dir_bits(env);
+            it.a[t].ts = 0;
+        }
+        F.cur = c0;
+    }
+    // launches: runs of up to kJobsPerLaunch jobs of one kernel shape,
+    // state-based jobs first (the dilatation launches cover them only)
+    std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) {
+        return x.wps != y.wps ? x.wps < y.wps : (x.lps && !y.lps);
+    });
+    struct Run {
+        int first, n, wps;
+        bool lps;
+    };
+    std::vector<Run> runs;
+    for (int k = 0; k < n_envs;) {
+        int e = k;
+        while (e < n_envs && e - k < kJobsPerLaunch && items[e].wps == items[k].wps && items[e].lps == items[k].lps)
+            ++e;
+        runs.push_back(Run{k, e - k, items[k].wps, items[k].lps});
+        k = e;
+    }
+    // one table per (run, argument set); blocks per job: the kernel's grid
+    auto table = [&](const Run &r, int t, bool particles) {
+        JobTable<R> tab;
+        std::memset(&tab, 0, sizeof(tab));
+        int64_t tot = 0;
+        for (int k = 0; k < r.n; ++k) {
+            const Item &it = items[r.first + k];
+            tab.a[k] = it.a[t];
+            tab.bstart[k] = (int32_t)tot;
+            tot += particles ? (int64_t)gridn(it.env->N) : step_blocks(it.wps, it.env->N);
+        }
+        tab.bstart[r.n] = (int32_t)tot;
+        tab.n = r.n;
+        return tab;
+    };
+    std::vector<JobTable<R>> pro, even, odd;
+    for (const Run &r : runs) {
+        pro.push_back(table(r, 0, true));
+        even.push_back(table(r, 1, false));
+        odd.push_back(table(r, 2, false));
+    }
+    for (const auto &t : pro) {
+        k_prologue_jobs<R><<<(unsigned)t.bstart[t.n], kT, 0, st>>>(t);
+        note_launch();
+    }
+    for (int64_t s = 0; s < nsteps; ++s) {
+        const auto &tabs = (s & 1) ? odd : even;
+        const bool last = s == nsteps - 1;
+        for (size_t r = 0; r < runs.size(); ++r)
+            if (runs[r].lps) dispatch_jobs<R>(st, runs[r].wps, true, last, tabs[r]);
+        for (size_t r = 0; r < runs.size(); ++r) dispatch_jobs<R>(st, runs[r].wps, false, last, tabs[r]);
+        if ((s & 63) == 63) CK(cudaGetLastError());
+    }
+    CK(cudaGetLastError());
+    // host bookkeeping, as vv_chunk leaves it: the prologue and every step
+    // but the last flip the record buffers
+    for (Item &it : items) {
+        Fast<R> &F = fast_of(it.env);
+        if (nsteps & 1) F.cur = 1 - F.cur;
+        for (int64_t s = 0; s < nsteps; ++s) advance_bc_clock(it.env);
+        holder(it.env)->dirty = true;
+    }
+    return PD_OK;
+}
+
+Fast<float> &fast32(pd_env *env) { return holder(env)->f32; }
+Fast<double> &fast64(pd_env *env) { return holder(env)->f64; }
+
+}  // namespace
+
+// An environment the serving loop may advance in shared launches: a
+// throughput precision, at most kBatchMaxParticles particles (larger jobs
+// fill the device with launches of their own), every block past the
+// deformed gate (known on the host), no contacts, no boundary conditions,
+// no elasto-plastic blocks, and a kernel shape with the larger unroll and
+// no record staging.
+constexpr int64_t kBatchMaxParticles = 65536;
+bool fast_batchable(pd_env *env) {
+    if (env->precision == PD_PREC_FP64_SERIAL || !env->hc.empty() || !env->hbc.empty() || any_ep(env) ||
+        env->N > kBatchMaxParticles)
+        return false;
+    for (size_t b = 0; b < env->hb.size(); ++b)
+        if (env->hb[b].kind != PD_MAT_SKIP && !env->deformed_h[b]) return false;
+    if (ensure_fast(env) != PD_OK) return false;
+    FastHolder *h = holder(env);
+    const int w = h->prec == PD_PREC_FP32C ? h->f32.wps : h->f64.wps;
+    const int u = h->prec == PD_PREC_FP32C ? Unroll<float>::HI : Unroll<double>::HI;
+    return w > 0 && w < 100 && w % 10 == u;
+}
+
+// Shared-launch chunk of nsteps steps over envs (all batchable, one
+// precision) on stream st.
+pd_status fast_batch_steps(pd_env *const *envs, int n_envs, int64_t nsteps, cudaStream_t st) {
+    if (n_envs <= 0 || nsteps <= 0) return PD_OK;
+    const int prec = envs[0]->precision;
+    for (int k = 0; k < n_envs; ++k)
+        if (envs[k]->precision != prec || !envs[k]->fast_valid)
+            return fail(PD_ERR_ARG, "a batch holds prepared environments of one precision");
+    if (prec == PD_PREC_FP32C) return batch_chunk<float>(envs, n_envs, nsteps, st, fast32);
+    return batch_chunk<double>(envs, n_envs, nsteps, st, fast64);
 }
 
 // Wait for and apply an outstanding gate-flag read-back (before anything

@@ -66,6 +66,9 @@ struct DevBlock {
 // Slots are in descending offset order, so each particle meets its bonds in
 // descending neighbour index -- the reference's family order.
 constexpr int kExplicit = 0, kStencil = 1;
+// Zero entries appended to the neighbour-index array (read-ahead margin of
+// the stencil walks).
+constexpr int64_t kNbrPad = 16;
 struct SliceInfo {
     int64_t nbr;   // offset into nbr[]
     int64_t word;  // offset into the bit arrays

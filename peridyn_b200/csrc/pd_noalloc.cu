@@ -23,7 +23,11 @@
 //    is written by the same call first, so nothing needs clearing;
 //  * the first call on each device looks the array's address up with
 //    cudaGetSymbolAddress (with that device current); make that first call
-//    before any stream capture on the device.
+//    before any stream capture on the device;
+//  * the address is kept for the life of the process, so the device must
+//    not be reset (cudaDeviceReset) while the library is loaded, and calls
+//    must come from the device's primary context (the runtime API's
+//    default, which CUDA.jl also uses).
 #include <mutex>
 
 #include "pd_env_impl.h"
@@ -82,9 +86,10 @@ extern "C" pd_status pd_force_density_device_static(pd_env *env, int64_t block, 
     CK(cudaSetDevice(env->device));
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, f_dev) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
-        cudaPointerGetAttributes(&at, y_dev) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+        at.device != env->device || cudaPointerGetAttributes(&at, y_dev) != cudaSuccess ||
+        at.type != cudaMemoryTypeDevice || at.device != env->device) {
         cudaGetLastError();
-        return fail(PD_ERR_ARG, "f/y must be device pointers");
+        return fail(PD_ERR_ARG, "f/y must be device pointers on the environment's device %d", env->device);
     }
     if (hb.kind == PD_MAT_ELASTO_PLASTIC)
         return fail(PD_ERR_UNSUPPORTED, "the device-pointer entry point does not evaluate elasto-plastic blocks");

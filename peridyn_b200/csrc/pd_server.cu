@@ -3,15 +3,27 @@
 // Jobs queue in arrival order; two admission threads take the head of the
 // queue while the sum of the resident jobs' HBM footprints stays within the
 // budget (and fewer than max_active run) and finalize the job's
-// environment; a stepping thread advances every resident job in chunks of
-// velocity-Verlet steps on the job's own CUDA stream.  A job gets its next chunk as soon as its previous
-// one has finished (an event per job), so short jobs are not held back by
-// long ones and the chunks of different jobs overlap on the device.  A
-// finished job's state is downloaded and its device memory released at
+// environment; a stepping thread advances the resident jobs in chunks of
+// velocity-Verlet steps.
+//
+// Continuous batching: a job's first chunk runs on its own CUDA stream
+// (the deformed gate is decided there).  Once every block of a job has
+// deformed, a job of at most 64 k particles without contacts, boundary
+// conditions or elasto-plastic blocks joins the batch of its precision at
+// the batch's next chunk: the batch's jobs advance together in shared
+// launches (one job-table kernel per step, kernel shape and 16 jobs,
+// pd_fast.cu k_step_jobs), each chunk as long as
+// the shortest remaining run among them; membership changes between
+// chunks, without graph capture.  Other jobs keep running chunk after chunk
+// on their own streams, overlapping with the batch on the device.  A job's
+// numbers are the same alone and in any mix: its kernel shape is fixed
+// from its size, and a run split into chunks computes what one run does.
+// A finished job's state is downloaded and its device memory released at
 // once, which frees its share of the budget for the next admission.
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -41,20 +53,24 @@ struct Job {
     pd_status status = PD_OK;
     std::string err;
     bool cancel = false, inflight = false;
+    bool batched = false;  // advanced by a batch (not on its own stream)
     int64_t footprint = 0, bonds0 = 0, bond_updates = 0;
     Clock::time_point t_submit, t_admit, t_done;
     cudaEvent_t ev = nullptr;
     std::vector<double> y, v, damage;
 };
 
-// Kernel shape of a throughput-mode job from its size alone (never timed,
-// so the result of a job is the same whatever runs beside it): enough
-// warps per slice for about 32 resident warps per SM.
+// Kernel shape of a throughput-mode job from its size and the device's
+// multiprocessor count alone (never timed, so the result of a job is the
+// same whatever runs beside it): enough warps per slice for about 32
+// resident warps per SM.
 void fix_shape(pd_env *env) {
     if (env->precision == PD_PREC_FP64_SERIAL) return;
     const int64_t slices = env->N / kSlice;
+    int sms = env->sm_count;
+    if (sms <= 0 && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, env->device) != cudaSuccess) sms = 148;
     int w = 1;
-    while (w < 8 && slices * w < 148 * 32) w *= 2;
+    while (w < 8 && slices * w < (int64_t)sms * 32) w *= 2;
     pd_env_set_kernel_shape(env, w, env->precision == PD_PREC_FP32C ? 4 : 2);
 }
 
@@ -65,6 +81,9 @@ struct pd_server {
     int64_t budget = 0, used = 0;
     int max_active = 1;
     int64_t chunk = 128;
+    // shared launches for batchable jobs (PD_SERVE_BATCH=0: every job on
+    // its own stream)
+    bool batching = true;
     std::mutex mu;
     std::condition_variable wake, changed;
     std::deque<Job *> queue;
@@ -78,9 +97,20 @@ struct pd_server {
     // while the stepping thread keeps the device busy.
     static constexpr int kAdmitters = 2;
     std::thread admitters[kAdmitters], stepper;
+    // one batch per throughput precision (index 0: FP64, 1: FP32C), owned
+    // by the stepping thread
+    struct Batch {
+        std::vector<Job *> members;
+        std::vector<Job *> pending;  // idle, joining at the next chunk
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        bool inflight = false;
+        int64_t chunk_now = 0;
+    } batch[2];
 
     void admit_loop();
     void step_loop();
+    bool step_batch(Batch &b);
     void admit(Job *j);
     void finish(Job *j, int32_t state);
 };
@@ -179,8 +209,89 @@ void pd_server::admit_loop() {
     }
 }
 
-// Stepping thread: every resident job gets its next chunk as soon as its
-// previous one has finished.
+// One batch: when its chunk has finished, credit the steps and retire the
+// finished and cancelled members; when idle, take in the jobs waiting to
+// join and launch the next chunk.  Returns true when anything changed.
+bool pd_server::step_batch(Batch &b) {
+    bool progressed = false;
+    if (b.inflight) {
+        const cudaError_t q = cudaEventQuery(b.ev);
+        if (q == cudaErrorNotReady) return false;
+        b.inflight = false;
+        progressed = true;
+        for (size_t k = 0; k < b.members.size();) {
+            Job *j = b.members[k];
+            if (q != cudaSuccess) {
+                j->status = fail(PD_ERR_CUDA, "batch stream: %s", cudaGetErrorString(q));
+                j->err = pd_last_error();
+                finish(j, PD_JOB_FAILED);
+                b.members.erase(b.members.begin() + k);
+                continue;
+            }
+            j->done += b.chunk_now;
+            ++k;
+        }
+    }
+    if (!b.pending.empty()) {
+        b.members.insert(b.members.end(), b.pending.begin(), b.pending.end());
+        b.pending.clear();
+        progressed = true;
+    }
+    for (size_t k = 0; k < b.members.size();) {
+        Job *j = b.members[k];
+        bool cancel;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            cancel = j->cancel || stop;
+        }
+        if (cancel || j->done >= j->nsteps) {
+            finish(j, cancel ? PD_JOB_CANCELLED : PD_JOB_DONE);
+            b.members.erase(b.members.begin() + k);
+            progressed = true;
+            continue;
+        }
+        ++k;
+    }
+    if (b.members.empty()) return progressed;
+    if (!b.st) {
+        if (cudaStreamCreateWithFlags(&b.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (Job *j : b.members) {
+                j->status = fail(PD_ERR_CUDA, "batch stream creation failed");
+                j->err = pd_last_error();
+                finish(j, PD_JOB_FAILED);
+            }
+            b.members.clear();
+            return true;
+        }
+    }
+    int64_t n = chunk;
+    for (Job *j : b.members) n = std::min(n, j->nsteps - j->done);
+    std::vector<pd_env *> envs;
+    for (Job *j : b.members) envs.push_back(j->env);
+    pd_status s = fast_batch_steps(envs.data(), (int)envs.size(), n, b.st);
+    if (s == PD_OK && cudaEventRecord(b.ev, b.st) != cudaSuccess) {
+        cudaGetLastError();
+        s = fail(PD_ERR_CUDA, "event record failed");
+    }
+    if (s != PD_OK) {
+        const std::string err = pd_last_error();
+        for (Job *j : b.members) {
+            j->status = s;
+            j->err = err;
+            finish(j, PD_JOB_FAILED);
+        }
+        b.members.clear();
+        return true;
+    }
+    b.chunk_now = n;
+    b.inflight = true;
+    return true;
+}
+
+// Stepping thread: every resident job on its own stream gets its next chunk
+// as soon as its previous one has finished; the batches advance theirs.
 void pd_server::step_loop() {
     cudaSetDevice(device);
     std::vector<Job *> active;
@@ -189,13 +300,22 @@ void pd_server::step_loop() {
             std::unique_lock<std::mutex> lock(mu);
             for (Job *j : ready) active.push_back(j);
             ready.clear();
-            if (active.empty()) {
-                if (stop) return;
+            if (active.empty() && batch[0].members.empty() && batch[1].members.empty() && batch[0].pending.empty() &&
+                batch[1].pending.empty()) {
+                if (stop) {
+                    for (Batch &b : batch) {
+                        if (b.st) cudaStreamDestroy(b.st);
+                        if (b.ev) cudaEventDestroy(b.ev);
+                        b = Batch{};
+                    }
+                    return;
+                }
                 wake.wait(lock);
                 continue;
             }
         }
         bool progressed = false;
+        for (Batch &b : batch) progressed |= step_batch(b);
         for (size_t k = 0; k < active.size();) {
             Job *j = active[k];
             if (j->inflight) {
@@ -222,6 +342,16 @@ void pd_server::step_loop() {
             }
             if (cancel || j->done >= j->nsteps) {
                 finish(j, cancel ? PD_JOB_CANCELLED : PD_JOB_DONE);
+                active.erase(active.begin() + k);
+                progressed = true;
+                continue;
+            }
+            // past its first chunk, a job that may share launches waits for
+            // the next chunk of its precision's batch
+            if (batching && j->done > 0 && j->env->precision != PD_PREC_FP64_SERIAL &&
+                fast_land_flags(j->env) == PD_OK && fast_batchable(j->env)) {
+                j->batched = true;
+                batch[j->env->precision == PD_PREC_FP32C ? 1 : 0].pending.push_back(j);
                 active.erase(active.begin() + k);
                 progressed = true;
                 continue;
@@ -295,6 +425,7 @@ extern "C" pd_status pd_server_create(pd_server **out, int32_t device, int64_t h
     s->budget = hbm_budget_bytes;
     s->max_active = max_active;
     s->chunk = chunk_steps;
+    if (const char *e = std::getenv("PD_SERVE_BATCH")) s->batching = std::strcmp(e, "0") != 0;
     try {
         s->stepper = std::thread([p = s.get()] { p->step_loop(); });
         for (auto &t : s->admitters) t = std::thread([p = s.get()] { p->admit_loop(); });

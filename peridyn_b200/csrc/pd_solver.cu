@@ -116,7 +116,12 @@ __device__ __forceinline__ double nanmax(double a, double b) {
     return a > b ? a : b;
 }
 
+// Fixed partial-reduction width, independent of the device's SM count so
+// that the reduction order is the same on every GPU.
 constexpr int kRedBlocks = 148;
+// Largest number of CTAs sharing one block in the gate's partial norms
+// (fixed for the same reason).
+constexpr int kGateWidth = 148;
 
 // minimize.jl:149-155 apply_! and :202 y[:, mask] .+= dy, fused with the
 // max|f| / max|dy| reductions of :204.
@@ -197,7 +202,7 @@ pd_status update_acc_serial(pd_env *env) {
     }
     if (!items.empty()) {
         const int ni = (int)items.size();
-        const int gx = std::max(1, std::min(148, (148 * 8) / ni));
+        const int gx = std::max(1, std::min(kGateWidth, (kGateWidth * 8) / ni));
         if (env->gate_items_h.size() != items.size() ||
             std::memcmp(env->gate_items_h.data(), items.data(), items.size() * sizeof(GateItem)) != 0) {
             PD_TRY(grow(env->gate_items, (int64_t)items.size()));
@@ -280,12 +285,9 @@ extern "C" pd_status pd_env_apply_bc_at0(pd_env *env) {
     return PD_OK;
 }
 
-// velocity_verlet.jl:57-89, nsteps times.
-extern "C" pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps) {
-    PD_TRY(need_final(env));
-    if (nsteps < 0) return fail(PD_ERR_ARG, "nsteps < 0");
-    CK(cudaSetDevice(env->device));
-    if (env->precision != PD_PREC_FP64_SERIAL) return fast_vv_steps(env, nsteps);
+// velocity_verlet.jl:57-89, nsteps times, in the serial mode, enqueued on
+// the environment's stream.
+static pd_status serial_steps(pd_env *env, int64_t nsteps) {
     const double c = env->dt / 2;
     const double dt = env->dt;
     for (int64_t s = 0; s < nsteps; ++s) {
@@ -301,9 +303,37 @@ extern "C" pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps) {
         if ((s & 63) == 63) CK(cudaGetLastError());
     }
     CK(cudaGetLastError());
+    return PD_OK;
+}
+
+extern "C" pd_status pd_env_vv_steps(pd_env *env, int64_t nsteps) {
+    PD_TRY(need_final(env));
+    if (nsteps < 0) return fail(PD_ERR_ARG, "nsteps < 0");
+    CK(cudaSetDevice(env->device));
+    if (env->precision != PD_PREC_FP64_SERIAL) return fast_vv_steps(env, nsteps);
+    PD_TRY(serial_steps(env, nsteps));
     PD_TRY(refresh_deformed(env));
     CK(cudaStreamSynchronize(env->st));
     return PD_OK;
+}
+
+// pd_env_vv_steps without the final wait: the steps are enqueued on the
+// environment's stream.  Only an environment whose deformed flags the host
+// already knows (every block deformed, or the gate held) can skip the
+// read-back; others wait as pd_env_vv_steps does.
+extern "C" pd_status pd_env_vv_steps_async(pd_env *env, int64_t nsteps) {
+    PD_TRY(need_final(env));
+    if (nsteps < 0) return fail(PD_ERR_ARG, "nsteps < 0");
+    bool known = env->gate_hold;
+    if (!known) {
+        known = true;
+        for (size_t b = 0; b < env->hb.size(); ++b)
+            if (env->hb[b].kind != PD_MAT_SKIP && !env->deformed_h[b]) known = false;
+    }
+    if (!known) return pd_env_vv_steps(env, nsteps);
+    CK(cudaSetDevice(env->device));
+    if (env->precision != PD_PREC_FP64_SERIAL) return fast_vv_enqueue(env, nsteps);
+    return serial_steps(env, nsteps);
 }
 
 // minimize.jl:105-231 (one QSDrag solver step).
@@ -379,9 +409,10 @@ extern "C" pd_status pd_force_density_device(pd_env *env, int64_t block, double 
     CK(cudaSetDevice(env->device));
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, f_dev) != cudaSuccess || at.type != cudaMemoryTypeDevice ||
-        cudaPointerGetAttributes(&at, y_dev) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+        at.device != env->device || cudaPointerGetAttributes(&at, y_dev) != cudaSuccess ||
+        at.type != cudaMemoryTypeDevice || at.device != env->device) {
         cudaGetLastError();
-        return fail(PD_ERR_ARG, "f/y must be device pointers");
+        return fail(PD_ERR_ARG, "f/y must be device pointers on the environment's device %d", env->device);
     }
     cudaStream_t st = stream ? (cudaStream_t)stream : env->st;
     const HostBlock &hb = env->hb[block];

@@ -27,8 +27,18 @@ does; forces skipped by the gate are those of a rigid translation.
 In the serial FP64 mode the slabs reproduce such a whole-body run bit for
 bit (the gather order per particle follows the global indices, which the
 slabs keep); the throughput modes sum each particle's bonds over a
-different slice layout, within their stated tolerances.  Contact models
-are not supported in slab mode.
+different slice layout, within their stated tolerances.
+
+Two-block contact (ContactModel12, contacts.jl:189-247 and 434-476) runs
+in every slab holding particles of both blocks, between the slab's parts
+of them.  The ghost layers are then at least twice the contact search
+distance deep as well: a contact partner of an owned particle lies within
+one search distance, and that partner's own candidates (whose top
+max_neighs by index the search keeps) within two, so both lists come out
+as in the whole body, and the slab's relative order keeps the selection
+and the force gather order.  Each slab rebuilds its contact lists itself
+(``update_neighs``).  Self contact (ContactModel11) reads bond flags of
+ghost particles, which the halo exchange does not carry; it is rejected.
 
 ``SlabRun`` runs all slabs in one process (one device, or one device per
 slab); ``SlabRank`` is one slab per ``torch.distributed`` rank, the halo
@@ -36,10 +46,12 @@ buffers moving by point-to-point send/recv (NCCL between GPUs).  The
 exchange schedule (``SlabPlan.exchanges``) is the same for both.
 """
 import copy
+import ctypes
 
 import numpy as np
 
 from . import _abi
+from .contacts import NonLinearSpringContactModel12
 from .environment import Env
 from .materials import GeneralMaterial, PeridynamicsMaterial
 
@@ -50,12 +62,18 @@ class SlabPlan:
     order).  ``halo`` is the ghost depth in horizons; None: 3 with
     elasto-plastic blocks, else 2."""
 
-    def __init__(self, materials, nslabs, axis=0, halo=None):
+    def __init__(self, materials, nslabs, axis=0, halo=None, contacts=()):
         if nslabs < 1:
             raise ValueError("nslabs must be >= 1")
+        for cm in contacts:
+            if not isinstance(cm, NonLinearSpringContactModel12):
+                raise TypeError("slab mode supports two-block contact models only (self contact reads ghost "
+                                "bond flags, which the halo exchange does not carry)")
         if halo is None:
             halo = 3.0 if any(m.kind == _abi.PD_MAT_ELASTO_PLASTIC for m in materials) else 2.0
         self.halo = float(halo)
+        # contact partners and their candidates: two search distances
+        self.contact_reach = 2.0 * max([cm.distance for cm in contacts], default=0.0)
         self.nslabs = int(nslabs)
         self.axis = int(axis)
         xs, blk, hor = [], [], []
@@ -75,7 +93,7 @@ class SlabPlan:
         for s in range(self.nslabs):
             owner[order[bounds[s]:bounds[s + 1]]] = s
         self.owner = owner
-        reach = halo * np.concatenate(hor) * (1.0 + 1e-9)
+        reach = np.maximum(halo * np.concatenate(hor), self.contact_reach) * (1.0 + 1e-9)
         self.local = []  # per slab: environment-order indices of its particles, ascending
         self.owned = []  # per slab: bool over its local particles
         for s in range(self.nslabs):
@@ -101,11 +119,15 @@ class SlabPlan:
                 dst = np.searchsorted(self.local[s], g)
                 self.exchanges.append((o, s, src.astype(np.int64), dst.astype(np.int64)))
 
-    def slab_workload(self, s, materials, bcs):
-        """Materials and BCs of slab s: per block its particles (owned and
-        ghost) with the block's parameters; BC masks restricted to them."""
+    def slab_workload(self, s, materials, bcs, contacts=()):
+        """Materials, BCs and contact models of slab s: per block its
+        particles (owned and ghost) with the block's parameters; BC masks
+        restricted to them; each two-block contact model between the slab's
+        parts of its blocks (dropped where the slab lacks one of them).
+        With ``contacts`` given, returns (materials, bcs, contacts)."""
         sel = self.local[s]
         mats = []
+        sub_of = {}
         for b, m in enumerate(materials):
             first = int(np.sum(self.block < b))
             pick = sel[self.block[sel] == b] - first
@@ -118,6 +140,7 @@ class SlabPlan:
             pm = PeridynamicsMaterial(sub, copy.copy(m.specific), name=f"{m.name}[slab {s}]")
             pm.type = m.type  # the block's type range, whether or not all types occur here
             mats.append(pm)
+            sub_of[id(m)] = pm
         sub_bcs = []
         for bc in bcs:
             c = copy.copy(bc)
@@ -126,13 +149,32 @@ class SlabPlan:
             if sb is not None:
                 c.scalebool = np.ascontiguousarray(np.asarray(sb, dtype=np.uint8)[sel])
             sub_bcs.append(c)
-        return mats, sub_bcs
+        if not contacts:
+            return mats, sub_bcs
+        sub_contacts = []
+        for cm in contacts:
+            m1, m2 = sub_of.get(id(cm.mat1)), sub_of.get(id(cm.mat2))
+            if m1 is None or m2 is None:
+                continue
+            c = copy.copy(cm)
+            c.mat1, c.mat2 = m1, m2
+            c.max_neighs = min(cm.max_neighs, m2.general.n)
+            sub_contacts.append(c)
+        return mats, sub_bcs, sub_contacts
 
 
 def _torch():
     import torch
 
     return torch
+
+
+def env_stream(env, device):
+    """The environment's CUDA stream as a torch stream (for event ordering)."""
+    torch = _torch()
+    sp = ctypes.c_void_p()
+    _abi.check(_abi.lib().pd_env_stream(env._h, ctypes.byref(sp)))
+    return torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", device))
 
 
 class SlabRun:
@@ -142,27 +184,52 @@ class SlabRun:
     ``state()`` gathers y, v, f of the owned particles in environment
     order."""
 
-    def __init__(self, materials, bcs, dt, nslabs, axis=0, precision="fp64_serial", devices=None, halo=None):
+    def __init__(self, materials, bcs, dt, nslabs, axis=0, precision="fp64_serial", devices=None, halo=None,
+                 contacts=()):
         if any(getattr(m, "kind", None) is None for m in materials):
             raise TypeError("materials must be PeridynamicsMaterial blocks")
-        self.plan = SlabPlan(materials, nslabs, axis=axis, halo=halo)
+        self.plan = SlabPlan(materials, nslabs, axis=axis, halo=halo, contacts=contacts)
         self.devices = list(devices) if devices is not None else [0] * nslabs
         self.envs = []
         for s in range(nslabs):
-            mats, sbcs = self.plan.slab_workload(s, materials, bcs)
-            env = Env(1, mats, [], sbcs, dt, precision=precision, device=self.devices[s])
+            if contacts:
+                mats, sbcs, scs = self.plan.slab_workload(s, materials, bcs, contacts)
+            else:
+                (mats, sbcs), scs = self.plan.slab_workload(s, materials, bcs), []
+            env = Env(1, mats, scs, sbcs, dt, precision=precision, device=self.devices[s])
             env.set_deformed(np.ones(len(mats), dtype=np.uint8), hold=True)
             self.envs.append(env)
         torch = _torch()
         self._idx = []
         for (o, s, src, dst) in self.plan.exchanges:
+            cross = self.devices[o] != self.devices[s]
             self._idx.append((torch.as_tensor(src, device=f"cuda:{self.devices[o]}"),
                               torch.as_tensor(dst, device=f"cuda:{self.devices[s]}"),
-                              torch.empty(9 * src.size, dtype=torch.float64, device=f"cuda:{self.devices[o]}")))
+                              torch.empty(9 * src.size, dtype=torch.float64, device=f"cuda:{self.devices[o]}"),
+                              torch.empty(9 * src.size, dtype=torch.float64, device=f"cuda:{self.devices[s]}")
+                              if cross else None))
+        self._streams = [env_stream(e, d) for e, d in zip(self.envs, self.devices)]
+        self._copy = {d: torch.cuda.Stream(device=d) for d in set(self.devices)}
+        # per exchange: the event after which its send buffer / receive
+        # buffer may be overwritten (the last reader has finished)
+        self._free_send = [None] * len(self.plan.exchanges)
+        self._free_recv = [None] * len(self.plan.exchanges)
 
     def apply_bc_at0(self):
         for e in self.envs:
             _abi.check(_abi.lib().pd_env_apply_bc_at0(e._h))
+
+    def update_neighs(self, max_part=30):
+        """update_neighs! (solvers.jl:351-361) in every slab."""
+        for e in self.envs:
+            _abi.check(_abi.lib().pd_env_update_neighs(e._h, int(max_part)))
+
+    def update_acc(self):
+        """update_acc! in every slab (forces at the current positions, e.g.
+        save_state! at t0); ghosts receive their owners' values."""
+        for e in self.envs:
+            _abi.check(_abi.lib().pd_env_update_acc(e._h))
+        self.exchange()
 
     def _sync(self):
         torch = _torch()
@@ -170,27 +237,54 @@ class SlabRun:
             torch.cuda.synchronize(d)
 
     def exchange(self):
-        """Owners' (q, v, f) into the ghosts standing for them."""
+        """Owners' (q, v, f) into the ghosts standing for them, ordered on
+        the device by CUDA events, without host waits: pack on the owner's
+        stream, the copy between GPUs on a copy stream of the receiving GPU,
+        unpack on the receiver's stream, and the next pack into a buffer
+        only after its last reader."""
+        torch = _torch()
         L = _abi.lib()
-        self._sync()
-        for (o, s, _, _), (src, _, buf) in zip(self.plan.exchanges, self._idx):
+        for k, ((o, s, _, _), (src, dst, buf, rbuf)) in enumerate(zip(self.plan.exchanges, self._idx)):
+            so, ss = self._streams[o], self._streams[s]
+            if self._free_send[k] is not None:
+                so.wait_event(self._free_send[k])
             _abi.check(L.pd_env_pack_halo(self.envs[o]._h, src.data_ptr(), src.numel(), buf.data_ptr()))
-        self._sync()
-        # copies between devices run on torch's streams: complete them before
-        # the environments' streams unpack
-        bufs = [buf if self.devices[o] == self.devices[s] else buf.to(f"cuda:{self.devices[s]}")
-                for (o, s, _, _), (_, _, buf) in zip(self.plan.exchanges, self._idx)]
-        self._sync()
-        for (o, s, _, _), (_, dst, _), b in zip(self.plan.exchanges, self._idx, bufs):
-            _abi.check(L.pd_env_unpack_halo(self.envs[s]._h, dst.data_ptr(), dst.numel(), b.data_ptr()))
-        self._sync()
+            packed = torch.cuda.Event()
+            packed.record(so)
+            if rbuf is None:
+                ss.wait_event(packed)
+                src_buf = buf
+            else:
+                cs = self._copy[self.devices[s]]
+                cs.wait_event(packed)
+                if self._free_recv[k] is not None:
+                    cs.wait_event(self._free_recv[k])
+                with torch.cuda.stream(cs):
+                    rbuf.copy_(buf, non_blocking=True)
+                moved = torch.cuda.Event()
+                moved.record(cs)
+                self._free_send[k] = moved
+                ss.wait_event(moved)
+                src_buf = rbuf
+            _abi.check(L.pd_env_unpack_halo(self.envs[s]._h, dst.data_ptr(), dst.numel(), src_buf.data_ptr()))
+            unpacked = torch.cuda.Event()
+            unpacked.record(ss)
+            if rbuf is None:
+                self._free_send[k] = unpacked
+            else:
+                self._free_recv[k] = unpacked
 
     def step(self, nsteps=1):
+        """nsteps velocity-Verlet steps of every slab, a halo exchange
+        after each; the slabs' steps are enqueued without host waits
+        (pd_env_vv_steps_async: their gates are held), so slabs on
+        different GPUs run at once.  Returns when all have finished."""
         L = _abi.lib()
         for _ in range(int(nsteps)):
             for e in self.envs:
-                _abi.check(L.pd_env_vv_steps(e._h, 1))
+                _abi.check(L.pd_env_vv_steps_async(e._h, 1))
             self.exchange()
+        self._sync()
 
     def state(self):
         n = self.plan.n
@@ -234,6 +328,9 @@ class SlabRank:
                 return torch.empty(9 * n, dtype=torch.float64, pin_memory=True)
             return None
 
+        # the slab environment's stream, for event ordering on the device wire
+        self._env_stream = env_stream(env, torch.device(device).index or 0) \
+            if (on_dev and hasattr(env, "_h")) else None
         self.sends, self.recvs = [], []
         for (o, s, src, dst) in plan.exchanges:
             if o == self.rank:
@@ -264,8 +361,26 @@ class SlabRank:
             _torch().cuda.synchronize(self.device)
 
     def exchange(self):
+        torch = _torch()
         for _, idx, buf, _ in self.sends:
             self._pack(idx, buf)
+        if not self.host_wire and self._env_stream is not None:
+            # device wire: NCCL runs on torch's current stream; order it after
+            # the packs, and the unpacks after it, with events (no host wait)
+            packed = torch.cuda.Event()
+            packed.record(self._env_stream)
+            torch.cuda.current_stream(self.device).wait_event(packed)
+            ops = [self.dist.P2POp(self.dist.isend, buf, peer) for peer, _, buf, _ in self.sends]
+            ops += [self.dist.P2POp(self.dist.irecv, buf, peer) for peer, _, buf, _ in self.recvs]
+            if ops:
+                for r in self.dist.batch_isend_irecv(ops):
+                    r.wait()
+            done = torch.cuda.Event()
+            done.record(torch.cuda.current_stream(self.device))
+            self._env_stream.wait_event(done)
+            for _, idx, buf, _ in self.recvs:
+                self._unpack(idx, buf)
+            return
         self._sync()
         if self.host_wire:
             for _, _, buf, hbuf in self.sends:
@@ -288,9 +403,12 @@ class SlabRank:
         """``nsteps`` velocity-Verlet steps of the rank's slab, a halo
         exchange after each (every rank calls it with the same count)."""
         L = _abi.lib()
+        run = L.pd_env_vv_steps_async if self._env_stream is not None and not self.host_wire else L.pd_env_vv_steps
         for _ in range(int(nsteps)):
-            _abi.check(L.pd_env_vv_steps(self.env._h, 1))
+            _abi.check(run(self.env._h, 1))
             self.exchange()
+        if self._env_stream is not None:
+            self._env_stream.synchronize()
 
     def owned_state(self):
         """(environment-order indices, y, v, f) of the particles this rank

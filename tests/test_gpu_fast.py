@@ -126,7 +126,8 @@ def test_contact_impact_fast(oracle, precision):
         ora.vv_step()
         pb.velocity_verlet_step(env)
     eu, ev, mism = _errors(env, ora)
-    assert eu <= (1e-9 if precision == "fp64" else 2e-4), eu
+    print(f"\ncontact impact {precision}: displacement {eu:.3e}, velocity {ev:.3e}, mismatched {mism}")
+    assert eu <= (1e-9 if precision == "fp64" else TOL["fp32c"]), eu
     assert mism == 0
     env.close()
 

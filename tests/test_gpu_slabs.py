@@ -66,3 +66,58 @@ def test_slabs_throughput_modes(name, precision, tol):
     y1, v1, _ = _slabs(w, precision, 80, 3)
     du = np.linalg.norm((y1 - x) - (y0 - x)) / np.linalg.norm(y0 - x)
     assert du <= tol, du
+
+
+def _disk(speed=300.0):
+    return configs.disk_impact(radius=3.0e-3, thickness=1.0e-3, spacing=2.5e-4, sphere_radius=1.0e-3, speed=speed)
+
+
+def _whole_contact(w, precision, nsteps, every):
+    env = pb.Env(1, w["materials"], w["contacts"], [], w["dt"], precision=precision)
+    env.set_deformed(np.ones(len(w["materials"]), dtype=np.uint8), hold=True)
+    pb.update_neighs(env)
+    pb.update_acc(env)
+    for s in range(nsteps):
+        if s and s % every == 0:
+            pb.update_neighs(env)
+        pb.velocity_verlet_step(env)
+    y, v, f, _ = env.get_state()
+    broken = sum(int((env._family(b)[0] > 0).sum() - env._family(b)[1].sum()) for b in range(2))
+    env.close()
+    return y, v, f, broken
+
+
+def _slabs_contact(w, precision, nsteps, every, nslabs, axis):
+    run = SlabRun(w["materials"], [], w["dt"], nslabs, axis=axis, precision=precision, contacts=w["contacts"])
+    run.update_neighs()
+    run.update_acc()
+    for s in range(nsteps):
+        if s and s % every == 0:
+            run.update_neighs()
+        run.step(1)
+    y, v, f = run.state()
+    run.close()
+    return y, v, f
+
+
+@pytest.mark.parametrize("nslabs,axis", [(2, 0), (3, 1)])
+def test_slabs_with_contact_serial_bit_identical(nslabs, axis):
+    """Disk struck by a stiff sphere (nonlinear contact), cut into slabs
+    across the contact zone: the serial FP64 slabs equal the whole body bit
+    for bit, contact neighbour lists rebuilt every 10 steps; by step 100
+    ~2,000 bonds under the sphere have broken."""
+    w = _disk()
+    y0, v0, f0, broken = _whole_contact(w, "fp64_serial", 100, 10)
+    assert broken > 0  # the impact breaks bonds under the sphere
+    y1, v1, f1 = _slabs_contact(w, "fp64_serial", 100, 10, nslabs, axis)
+    assert np.array_equal(y0, y1) and np.array_equal(v0, v1) and np.array_equal(f0, f1)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32c", 1e-4)])
+def test_slabs_with_contact_throughput_modes(precision, tol):
+    w = _disk()
+    x = np.hstack([m.general.x for m in w["materials"]])
+    y0, v0, _, _ = _whole_contact(w, precision, 100, 10)
+    y1, v1, _ = _slabs_contact(w, precision, 100, 10, 2, 0)
+    du = np.linalg.norm((y1 - x) - (y0 - x)) / np.linalg.norm(y0 - x)
+    assert du <= tol, du

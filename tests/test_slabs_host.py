@@ -136,3 +136,44 @@ def test_rank_wire_must_be_device_or_host():
     plan = SlabPlan(w["materials"], 2)
     with pytest.raises(ValueError):
         SlabRank(plan, 0, dist, _FakeSlab(torch.zeros((plan.local[0].size, 9))), device="cpu", wire="nvlink")
+
+
+def _disk_with_contact():
+    return configs.disk_impact(radius=3.0e-3, thickness=1.0e-3, spacing=2.5e-4, sphere_radius=1.0e-3, speed=100.0)
+
+
+@pytest.mark.parametrize("nslabs,axis", [(2, 0), (3, 0), (2, 1)])
+def test_plan_contact_partners_and_their_candidates_are_local(nslabs, axis):
+    """Two-block contact in slabs: for every owned particle of either block,
+    its contact partners (other block, within the search distance) and
+    their own candidates are in the slab, so the slab's contact lists and
+    reactions are the whole body's."""
+    w = _disk_with_contact()
+    cm = w["contacts"][0]
+    m1, m2 = w["materials"]
+    plan = SlabPlan(w["materials"], nslabs, axis=axis, contacts=w["contacts"])
+    x = np.hstack([m1.general.x, m2.general.x])
+    n1 = m1.general.n
+    d2 = ((x[:, :n1, None] - x[:, None, n1:]) ** 2).sum(axis=0)
+    near = d2 < cm.distance ** 2  # n1 x n2 candidate pairs
+    for s in range(nslabs):
+        here = np.zeros(x.shape[1], dtype=bool)
+        here[plan.local[s]] = True
+        own = plan.local[s][plan.owned[s]]
+        own1, own2 = own[own < n1], own[own >= n1] - n1
+        p2 = np.unique(np.nonzero(near[own1])[1])  # partners of owned block-1 particles
+        p1 = np.unique(np.nonzero(near[:, own2])[0])  # partners of owned block-2 particles
+        assert here[n1 + p2].all() and here[p1].all()
+        assert here[np.unique(np.nonzero(near[:, p2])[0])].all()  # candidates of those partners
+        assert here[n1 + np.unique(np.nonzero(near[p1])[1])].all()
+    mats, _, scs = plan.slab_workload(0, w["materials"], [], w["contacts"])
+    assert len(scs) == 1 and scs[0].mat1 is mats[0] and scs[0].mat2 is mats[1]
+
+
+def test_plan_rejects_self_contact():
+    x, vol = lattice.cuboid(8, 4, 4, 1e-3)
+    gen = pb.GeneralMaterial(x.copy(order="F"), np.zeros_like(x, order="F"), x, vol, np.ones(x.shape[1], np.int64),
+                             3.015e-3, max_neigh=200)
+    mat = pb.PeridynamicsMaterial(gen, pb.BondBasedSpecific([10e9], [0.01], [2000.0]))
+    with pytest.raises(TypeError):
+        SlabPlan([mat], 2, contacts=[pb.LinearSpringContactModel(1e18, mat)])

@@ -73,3 +73,36 @@ def test_static_scratch_rejects_large_blocks():
     assert b"static scratch holds at most 65536" in L.pd_last_error()
     assert torch.count_nonzero(fd).item() == 0
     env.close()
+
+
+def test_static_entry_point_allocates_no_device_memory():
+    """The property the entry point exists for: with its code loaded (a
+    first call on the device does the one-time set-up), a call on a fresh
+    environment leaves the device's free memory unchanged, while the
+    allocating entry point's first call on the same size of block visibly
+    takes its two staging buffers -- so the measurement would see an
+    allocation if the static path made one."""
+    pytest.importorskip("torch")
+    import torch
+
+    L = _abi.lib()
+    warm = _env(configs.pmb_cube(n=8))
+    yw, _, _, _ = warm.get_state()
+    _call(L.pd_force_density_device_static, warm, np.zeros_like(yw), yw)
+    dims = (40, 40, 37)  # 59200 particles: two 32-byte staging arrays are 3.8 MB
+    free = []
+    for fn in (L.pd_force_density_device_static, L.pd_force_density_device):
+        env = _env(configs.pmb_cube(dims=dims))
+        y, _, _, _ = env.get_state()
+        yd = torch.from_numpy(np.ascontiguousarray(y.T)).cuda()
+        fd = torch.zeros_like(yd)
+        torch.cuda.synchronize()
+        before = torch.cuda.mem_get_info()[0]
+        _abi.check(fn(env._h, 0, ctypes.c_void_p(fd.data_ptr()), ctypes.c_void_p(yd.data_ptr()), None))
+        torch.cuda.synchronize()
+        free.append(before - torch.cuda.mem_get_info()[0])
+        env.close()
+    warm.close()
+    n = dims[0] * dims[1] * dims[2]
+    assert free[1] >= 2 * n * 32, f"the allocating entry point's staging buffers were not seen ({free[1]} B)"
+    assert free[0] == 0, f"the static entry point changed free device memory by {free[0]} B"
