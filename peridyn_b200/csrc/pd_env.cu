@@ -2,6 +2,7 @@
 // device memory ownership, family construction and the solver sequencing of
 // src/solvers/*.jl on one CUDA stream.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <functional>
@@ -135,57 +136,38 @@ pd_status need_final(const pd_env *env) {
     return PD_OK;
 }
 
-// Binning for the family search: cubic cells one horizon (times 1+1e-9)
-// wide, stable counting sort by cell.  Any binning whose cells are at
+// Cell grid of a block for the family search: cubic cells one horizon
+// (times 1+1e-9) wide over the block's bounding box, at most 1024 per axis
+// (wider domains fold into the edge cells).  Any binning whose cells are at
 // least a horizon wide yields the same family sets; the order is fixed
-// afterwards by sorting.
-struct Cells {
+// afterwards by sorting.  The particles are binned on the device
+// (k_cell_ids / k_cell_scatter).
+struct CellGrid {
+    double3 lo;
+    double cell;
     int3 dims;
-    std::vector<int32_t> cell_of, start, list;
 };
 
-Cells bin_block(const HostBlock &b, int64_t first_int) {
-    Cells c;
+CellGrid block_grid(const HostBlock &b) {
+    CellGrid g;
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int64_t i = 0; i < b.n; ++i)
         for (int d = 0; d < 3; ++d) {
             mn[d] = std::min(mn[d], b.x[3 * i + d]);
             mx[d] = std::max(mx[d], b.x[3 * i + d]);
         }
-    double cell = b.horizon * (1.0 + 1e-9);
+    g.cell = b.horizon * (1.0 + 1e-9);
     int dims[3];
     for (int d = 0; d < 3; ++d) {
-        double span = b.n > 0 ? (mx[d] - mn[d]) / cell : 0.0;
+        double span = b.n > 0 ? (mx[d] - mn[d]) / g.cell : 0.0;
         double nd = std::floor(span) + 1.0;
         if (!(nd >= 1.0)) nd = 1.0;
-        if (nd > 1024.0) nd = 1024.0;  // wider domains fold into the edge cells
+        if (nd > 1024.0) nd = 1024.0;
         dims[d] = (int)nd;
     }
-    c.dims = make_int3(dims[0], dims[1], dims[2]);
-    int64_t ncell = (int64_t)dims[0] * dims[1] * dims[2];
-    c.cell_of.resize(b.n);
-    std::vector<int32_t> count(ncell + 1, 0);
-    for (int64_t i = 0; i < b.n; ++i) {
-        int ijk[3];
-        for (int d = 0; d < 3; ++d) {
-            double q = std::floor((b.x[3 * i + d] - mn[d]) / cell);
-            if (!(q >= 0.0)) q = 0.0;
-            if (q > dims[d] - 1) q = dims[d] - 1;
-            ijk[d] = (int)q;
-        }
-        int32_t cid = ijk[0] + dims[0] * (ijk[1] + dims[1] * ijk[2]);
-        c.cell_of[i] = cid;
-        count[cid + 1]++;
-    }
-    for (int64_t k = 0; k < ncell; ++k) count[k + 1] += count[k];
-    c.start = count;
-    c.list.resize(b.n);
-    std::vector<int32_t> fill(ncell, 0);
-    for (int64_t i = 0; i < b.n; ++i) {
-        int32_t cid = c.cell_of[i];
-        c.list[c.start[cid] + fill[cid]++] = (int32_t)(first_int + i);
-    }
-    return c;
+    g.lo = make_double3(b.n > 0 ? mn[0] : 0.0, b.n > 0 ? mn[1] : 0.0, b.n > 0 ? mn[2] : 0.0);
+    g.dims = make_int3(dims[0], dims[1], dims[2]);
+    return g;
 }
 
 }  // namespace
@@ -477,6 +459,78 @@ extern "C" pd_status pd_env_add_contact(pd_env *env, int32_t kind, int64_t block
     return PD_OK;
 }
 
+namespace {
+// Wall-clock phases of pd_env_finalize (and of the device layout
+// conversion), printed to stderr when the process environment has
+// PD_SETUP_TIMES=1 (a diagnostic for setup cost).
+struct SetupClock {
+    bool on = false;
+    std::chrono::steady_clock::time_point t0, t;
+    SetupClock() {
+        const char *e = std::getenv("PD_SETUP_TIMES");
+        on = e && std::strcmp(e, "1") == 0;
+        t0 = t = std::chrono::steady_clock::now();
+    }
+    void mark(const char *phase, cudaStream_t st) {
+        if (!on) return;
+        cudaStreamSynchronize(st);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "pd_env_finalize %-32s %8.1f ms (total %8.1f ms)\n", phase,
+                     std::chrono::duration<double, std::milli>(now - t).count(),
+                     std::chrono::duration<double, std::milli>(now - t0).count());
+        t = now;
+    }
+};
+}  // namespace
+
+// Record staging plans of the stencil slices (opt-in staged kernels), from
+// each slice's union of offsets, built on the host and uploaded: per plan
+// {ranges, records, (first record, count) per range}, and per stencil slot
+// the staged position of lane 0's record.  nbr_size: entries of the
+// runtime neighbour array (spos has one per entry).
+static pd_status upload_stage_plans(pd_env *env, const std::vector<SliceInfo> &si,
+                                    const std::vector<std::vector<int32_t>> &uni, size_t nbr_size) {
+    const int64_t N = env->N, S = N / kSlice;
+    std::vector<std::vector<int32_t>> plans(S);
+    std::vector<int32_t> spos(nbr_size, 0);
+    parallel_for(S, [&](int64_t s0, int64_t s1) {
+        std::vector<int32_t> rs, pos;
+        for (int64_t s = s0; s < s1; ++s) {
+            const SliceInfo &d = si[s];
+            if (d.mode != kStencil) continue;
+            const int64_t T = stage_plan(s * kSlice, N, uni[s], rs, pos);
+            if (T == 0 || T > kStageMaxRecords) continue;
+            std::copy(pos.begin(), pos.end(), spos.begin() + d.nbr);
+            std::vector<int32_t> &pl = plans[s];
+            pl.reserve(2 + rs.size());
+            pl.push_back((int32_t)(rs.size() / 2));
+            pl.push_back((int32_t)T);
+            pl.insert(pl.end(), rs.begin(), rs.end());
+        }
+    });
+    std::vector<int32_t> splan_off(S + 1, -1), splan;
+    int64_t nplan = 0, pmax = 0;
+    for (int64_t s = 0; s < S; ++s) {
+        if (plans[s].empty()) continue;
+        splan_off[s] = (int32_t)splan.size();
+        splan.insert(splan.end(), plans[s].begin(), plans[s].end());
+        pmax = std::max<int64_t>(pmax, plans[s][1]);
+        ++nplan;
+    }
+    if (splan.empty()) splan.push_back(0);
+    env->splan_slices = nplan;
+    env->splan_max = pmax;
+    cudaStream_t st = env->st;
+    PD_TRY(env->splan_off.alloc(S + 1));
+    PD_TRY(env->splan.alloc((int64_t)splan.size()));
+    PD_TRY(env->spos.alloc((int64_t)spos.size()));
+    CK(cudaMemcpyAsync(env->splan_off.p, splan_off.data(), (S + 1) * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->splan.p, splan.data(), splan.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(env->spos.p, spos.data(), spos.size() * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return PD_OK;
+}
+
 // ---------------------------------------------------------------------
 // Runtime bond layout.  Input: the build layout (SELL-32, bond k of lane l
 // of slice s at nbr_b[slice_ptr[s] + 32k + l], intact bit k%32 of word
@@ -580,35 +634,7 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     });
     cnt.swap(cnt_rt);
     // pass 3 (per stencil slice): record staging plans
-    std::vector<std::vector<int32_t>> plans(S);
-    std::vector<int32_t> spos(nbr.size(), 0);
-    parallel_for(S, [&](int64_t s0, int64_t s1) {
-        std::vector<int32_t> rs, pos;
-        for (int64_t s = s0; s < s1; ++s) {
-            const SliceInfo &d = si[s];
-            if (d.mode != kStencil) continue;
-            const int64_t T = stage_plan(s * kSlice, N, uni[s], rs, pos);
-            if (T == 0 || T > kStageMaxRecords) continue;
-            std::copy(pos.begin(), pos.end(), spos.begin() + d.nbr);
-            std::vector<int32_t> &pl = plans[s];
-            pl.reserve(2 + rs.size());
-            pl.push_back((int32_t)(rs.size() / 2));
-            pl.push_back((int32_t)T);
-            pl.insert(pl.end(), rs.begin(), rs.end());
-        }
-    });
-    std::vector<int32_t> splan_off(S + 1, -1), splan;
-    int64_t nplan = 0, pmax = 0;
-    for (int64_t s = 0; s < S; ++s) {
-        if (plans[s].empty()) continue;
-        splan_off[s] = (int32_t)splan.size();
-        splan.insert(splan.end(), plans[s].begin(), plans[s].end());
-        pmax = std::max<int64_t>(pmax, plans[s][1]);
-        ++nplan;
-    }
-    if (splan.empty()) splan.push_back(0);
-    env->splan_slices = nplan;
-    env->splan_max = pmax;
+    PD_TRY(upload_stage_plans(env, si, uni, nbr.size()));
     env->sinfo_h = si;
     env->cnt_h = cnt;
     env->nnz = (int64_t)kSlice * nwords;
@@ -633,25 +659,108 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     CK(cudaMemcpyAsync(env->words0.p, words.data(), nw * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(env->fam.p, fam.data(), nw * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    PD_TRY(env->splan_off.alloc(S + 1));
-    PD_TRY(env->splan.alloc((int64_t)splan.size()));
-    PD_TRY(env->spos.alloc((int64_t)spos.size()));
-    CK(cudaMemcpyAsync(env->splan_off.p, splan_off.data(), (S + 1) * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(env->splan.p, splan.data(), splan.size() * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(env->spos.p, spos.data(), spos.size() * 4, cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
+    return PD_OK;
+}
+
+// The runtime layout of build_runtime_layout, converted on the device from
+// the build layout already there (d_nbr, d_words; cnt_b = the build family
+// sizes, also in env->cnt): the per-slice unions and stencil decisions
+// (k_layout_union), the slice offsets on the host from the slices' modes
+// and lengths, then the runtime arrays (k_layout_fill).  Only per-slice
+// values, the slot counts and the runtime neighbour array (one entry per
+// stencil slot) come back to the host, instead of the whole build layout.
+static pd_status build_runtime_layout_device(pd_env *env, const std::vector<int64_t> &slice_ptr,
+                                             std::vector<int32_t> &cnt_b, const int64_t *d_slice_ptr,
+                                             const int32_t *d_nbr, const uint32_t *d_words) {
+    const int64_t N = env->N, S = N / kSlice;
+    cudaStream_t st = env->st;
+    SetupClock clk;
+    const char *lay = std::getenv("PD_FAMILY_LAYOUT");
+    const bool force_explicit = lay && std::strcmp(lay, "explicit") == 0;
+    int32_t maxc_all = 0;
+    for (int64_t p = 0; p < N; ++p) maxc_all = std::max(maxc_all, cnt_b[p]);
+    const int64_t ustride = round_up((int64_t)maxc_all + maxc_all / 4 + 33, 32);
+    DBuf<int32_t> d_mode, d_len, d_uni, d_cnt_rt;
+    PD_TRY(d_mode.alloc(std::max<int64_t>(S, 1)));
+    PD_TRY(d_len.alloc(std::max<int64_t>(S, 1)));
+    PD_TRY(d_uni.alloc(std::max<int64_t>(S * ustride, 1)));
+    PD_TRY(d_cnt_rt.alloc(std::max<int64_t>(N, 1)));
+    launch_layout_union(st, S, N, d_slice_ptr, env->cnt.p, d_nbr, force_explicit ? 1 : 0, ustride, d_mode.p,
+                        d_len.p, d_uni.p);
+    CK(cudaGetLastError());
+    std::vector<int32_t> mode(S), ulen(S);
+    if (S > 0) {
+        CK(cudaMemcpyAsync(mode.data(), d_mode.p, S * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ulen.data(), d_len.p, S * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    clk.mark("  layout: unions", st);
+    std::vector<SliceInfo> si(S + 1);
+    int64_t nbr_len = 0, nwords = 0, nst = 0;
+    for (int64_t s = 0; s < S; ++s) {
+        SliceInfo &d = si[s];
+        d.mode = mode[s];
+        d.len = (int32_t)round_up((int64_t)ulen[s], 32);
+        d.nbr = nbr_len;
+        d.word = nwords;
+        nbr_len += d.mode == kStencil ? d.len : (int64_t)kSlice * d.len;
+        nwords += d.len;
+        nst += d.mode == kStencil;
+    }
+    si[S].nbr = nbr_len;
+    si[S].word = nwords;
+    si[S].len = 0;
+    si[S].mode = kExplicit;
+    const int64_t nw = std::max<int64_t>(nwords, 1);
+    const int64_t nb = std::max<int64_t>(nbr_len, 32) + kNbrPad;  // zero read-ahead margin past the end
+    PD_TRY(env->sinfo.alloc(S + 1));
+    PD_TRY(env->nbr.alloc(nb));
+    PD_TRY(env->words[0].alloc(nw));
+    PD_TRY(env->words[1].alloc(nw));
+    PD_TRY(env->words0.alloc(nw));
+    PD_TRY(env->fam.alloc(nw));
+    CK(cudaMemcpyAsync(env->sinfo.p, si.data(), (S + 1) * sizeof(SliceInfo), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(env->nbr.p, 0, nb * 4, st));
+    CK(cudaMemsetAsync(env->words[0].p, 0, nw * 4, st));
+    CK(cudaMemsetAsync(env->fam.p, 0, nw * 4, st));
+    launch_layout_fill(st, N, d_slice_ptr, env->cnt.p, d_nbr, d_words, env->sinfo.p, d_len.p, ustride, d_uni.p,
+                       env->nbr.p, env->words[0].p, env->fam.p, d_cnt_rt.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(env->words[1].p, env->words[0].p, nw * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(env->words0.p, env->words[0].p, nw * 4, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(env->cnt.p, d_cnt_rt.p, N * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    std::vector<int32_t> cnt_rt(N), nbr(std::max<int64_t>(nbr_len, 32));
+    CK(cudaMemcpyAsync(cnt_rt.data(), d_cnt_rt.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nbr.data(), env->nbr.p, nbr.size() * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    clk.mark("  layout: fill, slot counts back", st);
+    // staging plans from the stencil slices' unions
+    std::vector<std::vector<int32_t>> uni(S);
+    for (int64_t s = 0; s < S; ++s)
+        if (si[s].mode == kStencil) uni[s].assign(nbr.begin() + si[s].nbr, nbr.begin() + si[s].nbr + ulen[s]);
+    PD_TRY(upload_stage_plans(env, si, uni, nbr.size()));
+    clk.mark("  layout: staging plans", st);
+    cnt_b.swap(cnt_rt);
+    env->sinfo_h = si;
+    env->cnt_h = cnt_b;
+    env->nnz = (int64_t)kSlice * nwords;
+    env->nbr_len = nbr_len;
+    env->stencil_slices = nst;
     return PD_OK;
 }
 
 // ---------------------------------------------------------------------
 // finalize: layout, upload, families, weighted volume, intact0
 // ---------------------------------------------------------------------
+
 extern "C" pd_status pd_env_finalize(pd_env *env) {
     PD_TRY(check_env(env));
     if (env->finalized) return fail(PD_ERR_STATE, "environment already finalized");
     if (env->hb.empty()) return fail(PD_ERR_STATE, "environment has no material blocks");
     CK(cudaSetDevice(env->device));
     cudaStream_t st = env->st;
+    SetupClock clk;
 
     // --- internal layout ---
     int64_t N = 0;
@@ -763,42 +872,63 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         CK(cudaStreamSynchronize(st));
     }
 
+    clk.mark("assembly and upload", st);
     // --- family sizes: GPU neighbour count per GPU-built block ---
     std::vector<int32_t> cnt(N, 0);
-    std::vector<Cells> cells(env->hb.size());
+    std::vector<CellGrid> cells(env->hb.size());
     std::vector<int64_t> cell_base(env->hb.size(), 0);
     DBuf<int32_t> d_cell_of, d_cell_start, d_cell_list;
     {
         int64_t tot_cells = 0, tot_part = 0;
+        std::vector<int64_t> part_off(env->hb.size(), 0);
         for (size_t bi = 0; bi < env->hb.size(); ++bi) {
             HostBlock &b = env->hb[bi];
             if (b.kind == PD_MAT_SKIP || b.host_family) continue;
-            cells[bi] = bin_block(b, b.first_int);
+            cells[bi] = block_grid(b);
             cell_base[bi] = tot_cells;
+            part_off[bi] = tot_part;
+            b.cell_part_off = tot_part;
             tot_cells += (int64_t)cells[bi].dims.x * cells[bi].dims.y * cells[bi].dims.z;
             tot_part += b.n;
         }
+        if (tot_cells >= ((int64_t)1 << 31) || tot_part >= ((int64_t)1 << 31))
+            return fail(PD_ERR_UNSUPPORTED, "family search grid too large (%lld cells)", (long long)tot_cells);
         if (tot_part > 0) {
-            std::vector<int32_t> cell_of_all, start_all, list_all;
-            std::vector<int64_t> part_off(env->hb.size(), 0);
-            start_all.reserve(tot_cells + 1);
+            // counting sort by cell on the device: ids and counts, starts
+            // (scanned on the host: one entry per cell), lists
+            PD_TRY(d_cell_of.alloc(tot_part));
+            PD_TRY(d_cell_start.alloc(tot_cells + 1));
+            PD_TRY(d_cell_list.alloc(tot_part));
+            DBuf<int32_t> d_count;
+            PD_TRY(d_count.alloc(tot_cells + 1));
+            CK(cudaMemsetAsync(d_count.p, 0, (tot_cells + 1) * sizeof(int32_t), st));
             for (size_t bi = 0; bi < env->hb.size(); ++bi) {
                 HostBlock &b = env->hb[bi];
                 if (b.kind == PD_MAT_SKIP || b.host_family) continue;
-                part_off[bi] = (int64_t)cell_of_all.size();
-                int32_t list_off = (int32_t)list_all.size();
-                for (int32_t c : cells[bi].cell_of) cell_of_all.push_back(c + (int32_t)cell_base[bi]);
-                int64_t nc = (int64_t)cells[bi].start.size() - 1;
-                for (int64_t k = 0; k < nc; ++k) start_all.push_back(cells[bi].start[k] + list_off);
-                for (int32_t v : cells[bi].list) list_all.push_back(v);
+                launch_cell_ids(st, b.n, b.first_int, env->x4.p, cells[bi].lo, cells[bi].cell, cells[bi].dims,
+                                cell_base[bi], d_cell_of.p + part_off[bi], d_count.p);
             }
-            start_all.push_back((int32_t)list_all.size());
-            PD_TRY(d_cell_of.alloc(cell_of_all.size()));
-            PD_TRY(d_cell_start.alloc(start_all.size()));
-            PD_TRY(d_cell_list.alloc(list_all.size()));
-            CK(cudaMemcpyAsync(d_cell_of.p, cell_of_all.data(), cell_of_all.size() * 4, cudaMemcpyHostToDevice, st));
-            CK(cudaMemcpyAsync(d_cell_start.p, start_all.data(), start_all.size() * 4, cudaMemcpyHostToDevice, st));
-            CK(cudaMemcpyAsync(d_cell_list.p, list_all.data(), list_all.size() * 4, cudaMemcpyHostToDevice, st));
+            CK(cudaGetLastError());
+            std::vector<int32_t> start(tot_cells + 1, 0);
+            CK(cudaMemcpyAsync(start.data(), d_count.p, tot_cells * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            int32_t run = 0;
+            for (int64_t c = 0; c < tot_cells; ++c) {
+                const int32_t k = start[c];
+                start[c] = run;
+                run += k;
+            }
+            start[tot_cells] = run;
+            CK(cudaMemcpyAsync(d_cell_start.p, start.data(), (tot_cells + 1) * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_count.p, start.data(), (tot_cells + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               st));  // scatter cursors
+            for (size_t bi = 0; bi < env->hb.size(); ++bi) {
+                HostBlock &b = env->hb[bi];
+                if (b.kind == PD_MAT_SKIP || b.host_family) continue;
+                launch_cell_scatter(st, b.n, b.first_int, d_cell_of.p + part_off[bi], d_count.p, d_cell_list.p);
+            }
+            CK(cudaGetLastError());
             CK(cudaMemsetAsync(env->cnt.p, 0, N * sizeof(int32_t), st));
             for (size_t bi = 0; bi < env->hb.size(); ++bi) {
                 HostBlock &b = env->hb[bi];
@@ -806,12 +936,6 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
                 launch_count_neighbors(st, b.n, b.first_int, env->x4.p, d_cell_of.p + part_off[bi],
                                        d_cell_start.p, d_cell_list.p, cell_base[bi], cells[bi].dims,
                                        b.horizon, env->cnt.p);
-                cells[bi].cell_of.clear();
-                cells[bi].cell_of.shrink_to_fit();
-                cells[bi].list.clear();
-                cells[bi].start.clear();
-                cells[bi].dims = cells[bi].dims;
-                b.cell_part_off = part_off[bi];
             }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(cnt.data(), env->cnt.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -844,6 +968,7 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
             b.rows = maxc + 1;
         }
     }
+    clk.mark("binning and family counts", st);
     // Build layout: SELL-32 with one explicit index per (slot, lane), filled
     // and sorted on the device.
     const int64_t S = N / kSlice;
@@ -856,10 +981,17 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
     const int64_t bnnz = slice_ptr[S];
     std::vector<int32_t> nbr_b;
     std::vector<uint32_t> w_b;
+    bool any_host = false;
+    for (auto &b : env->hb) any_host |= b.host_family;
+    // The runtime layout is converted on the device unless a block's family
+    // came from the host (then the build layout is patched on the host) or
+    // PD_LAYOUT_HOST=1 asks for the host conversion.
+    const char *lh = std::getenv("PD_LAYOUT_HOST");
+    const bool layout_on_device = !any_host && !(lh && std::strcmp(lh, "1") == 0);
+    DBuf<int64_t> d_slice_ptr;
+    DBuf<int32_t> d_nbr;
+    DBuf<uint32_t> d_words;
     {
-        DBuf<int64_t> d_slice_ptr;
-        DBuf<int32_t> d_nbr;
-        DBuf<uint32_t> d_words;
         PD_TRY(d_slice_ptr.alloc(S + 1));
         PD_TRY(d_nbr.alloc(std::max<int64_t>(bnnz, 32)));
         PD_TRY(d_words.alloc(std::max<int64_t>(bnnz / 32, 1)));
@@ -876,17 +1008,17 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         launch_sort_neighbors(st, N, d_slice_ptr.p, env->cnt.p, d_nbr.p);
         launch_init_intact(st, N, d_slice_ptr.p, env->cnt.p, d_words.p);
         CK(cudaGetLastError());
-        nbr_b.assign(bnnz, 0);
-        w_b.assign(bnnz / 32, 0);
-        if (bnnz > 0) {
-            CK(cudaMemcpyAsync(nbr_b.data(), d_nbr.p, bnnz * 4, cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(w_b.data(), d_words.p, (bnnz / 32) * 4, cudaMemcpyDeviceToHost, st));
+        if (!layout_on_device) {
+            nbr_b.assign(bnnz, 0);
+            w_b.assign(bnnz / 32, 0);
+            if (bnnz > 0) {
+                CK(cudaMemcpyAsync(nbr_b.data(), d_nbr.p, bnnz * 4, cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(w_b.data(), d_words.p, (bnnz / 32) * 4, cudaMemcpyDeviceToHost, st));
+            }
         }
         CK(cudaStreamSynchronize(st));
     }
     // host-provided families (already descending): write entries and bits
-    bool any_host = false;
-    for (auto &b : env->hb) any_host |= b.host_family;
     if (any_host) {
         for (auto &b : env->hb) {
             if (!b.host_family) continue;
@@ -933,8 +1065,16 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
             }
         }
     }
-    // Runtime layout (stencil or explicit per slice), uploaded.
-    PD_TRY(build_runtime_layout(env, slice_ptr, cnt, nbr_b, w_b));
+    clk.mark("family fill, sort, download", st);
+    // Runtime layout (stencil or explicit per slice).
+    if (layout_on_device) {
+        PD_TRY(build_runtime_layout_device(env, slice_ptr, cnt, d_slice_ptr.p, d_nbr.p, d_words.p));
+    } else {
+        PD_TRY(build_runtime_layout(env, slice_ptr, cnt, nbr_b, w_b));
+    }
+    d_nbr.reset();
+    d_words.reset();
+    d_slice_ptr.reset();
     nbr_b.clear();
     nbr_b.shrink_to_fit();
     w_b.clear();
@@ -951,12 +1091,14 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
             CK(cudaMemsetAsync(e.p, 0, std::max<int64_t>(env->nnz, 32) * sizeof(double), st));
         }
     }
+    clk.mark("runtime layout", st);
     // weighted volume (peri.jl:342-354) and intact0 (environment.jl:169)
     launch_weighted_volume(st, env->geo(), env->mth.p);
     launch_popcount(st, N, env->sinfo.p, env->cnt.p, env->words[0].p, env->intact0.p);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
 
+    clk.mark("weighted volume, intact0", st);
     // --- boundary conditions ---
     for (auto &hb : env->hbc) {
         DevBC d;
@@ -980,6 +1122,7 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
     }
     PD_TRY(pd::contacts_finalize(env));
     CK(cudaStreamSynchronize(st));
+    clk.mark("boundary conditions, contacts", st);
     env->finalized = true;
     // release host copies of the big per-particle inputs
     for (auto &b : env->hb) {

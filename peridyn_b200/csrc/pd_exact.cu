@@ -9,6 +9,7 @@
 //   get_ij         x[:, j] - x[:, i]                   const_macros.jl:153-155
 //   stretch        (|Y| - |X|) / |X|                   general_material.jl:338-341
 //   force          ((0.5*t/|Y|) * Y_d * V_j) / rho_i   general_material.jl:351-362
+#include <climits>
 #include <cstdio>
 
 #include "pd_internal.h"
@@ -84,6 +85,40 @@ __global__ void k_neighbors(int64_t n, int64_t first, const double4 *__restrict_
     if (!kFill) cnt[i] = k;
 }
 
+// Cell binning of one block for the family search (a counting sort by cell
+// id on the device): the cell of particle i is floor((x - lo) / cell) per
+// axis, clamped to the grid (wider domains fold into the edge cells), as
+// an index into the environment's concatenated cell grids; k_cell_ids
+// counts the particles of each cell, the host turns the counts into cell
+// starts, k_cell_scatter fills each cell's list.  The order within a cell
+// is whatever the atomics give: the search finds the same members in any
+// order and sorts each list afterwards.
+__global__ void k_cell_ids(int64_t n, int64_t first, const double4 *__restrict__ x4, double3 lo, double cell,
+                           int3 dims, int64_t cell_base, int32_t *__restrict__ cell_of, int32_t *__restrict__ count) {
+    const int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (li >= n) return;
+    const double4 x = x4[first + li];
+    const double xs[3] = {x.x, x.y, x.z}, los[3] = {lo.x, lo.y, lo.z};
+    const int dm[3] = {dims.x, dims.y, dims.z};
+    int ijk[3];
+    for (int d = 0; d < 3; ++d) {
+        double q = floor((xs[d] - los[d]) / cell);
+        if (!(q >= 0.0)) q = 0.0;
+        if (q > dm[d] - 1) q = dm[d] - 1;
+        ijk[d] = (int)q;
+    }
+    const int64_t c = cell_base + ijk[0] + (int64_t)dm[0] * (ijk[1] + (int64_t)dm[1] * ijk[2]);
+    cell_of[li] = (int32_t)c;
+    atomicAdd(count + c, 1);
+}
+
+__global__ void k_cell_scatter(int64_t n, int64_t first, const int32_t *__restrict__ cell_of,
+                               int32_t *__restrict__ cursor, int32_t *__restrict__ cell_list) {
+    const int64_t li = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (li >= n) return;
+    cell_list[atomicAdd(cursor + cell_of[li], 1)] = (int32_t)(first + li);
+}
+
 // Insertion sort of one particle's strided list into descending order.
 __global__ void k_sort_neighbors(int64_t N, const int64_t *__restrict__ slice_ptr,
                                  const int32_t *__restrict__ cnt, int32_t *__restrict__ nbr) {
@@ -112,6 +147,118 @@ __global__ void k_init_intact(int64_t N, const int64_t *__restrict__ slice_ptr,
         int32_t rem = n - w * 32;
         words[wb + 32 * (int64_t)w] = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
     }
+}
+
+// ---------------------------------------------------------------------
+// Runtime layout on the device (the conversion build_runtime_layout in
+// pd_env.cu performs on the host; both give the same arrays).  Pass 1, one
+// warp per slice: the union of the lanes' neighbour offsets q - p, merged
+// from the lanes' descending lists one element at a time (the warp's
+// maximum of the lanes' heads is the union's next element; lanes holding it
+// advance).  A slice takes the stencil form when the union has at most
+// maxc + maxc/4 + 32 entries (maxc: the slice's largest family) and every
+// union offset of every lane with bonds names an in-range record.
+// Outputs per slice: mode, union length (stencil) and the union itself in
+// uni[s * ustride ...]; the first merge only counts, so a slice found too
+// large writes nothing.
+// ---------------------------------------------------------------------
+__global__ void k_layout_union(int64_t S, int64_t N, const int64_t *__restrict__ slice_ptr,
+                               const int32_t *__restrict__ cnt, const int32_t *__restrict__ nbr_b,
+                               int32_t force_explicit, int64_t ustride, int32_t *__restrict__ mode,
+                               int32_t *__restrict__ len, int32_t *__restrict__ uni) {
+    const int64_t s = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (s >= S) return;  // whole warps: blockDim is a multiple of 32
+    const int64_t p = s * 32 + lane;
+    const int32_t c = cnt[p];
+    int32_t maxc = c;
+    for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+    const int32_t *lst = nbr_b + slice_ptr[s] + lane;  // lane's k-th neighbour at lst[32 k]
+    const int64_t limit = (int64_t)maxc + maxc / 4 + 32;
+    bool stencil = !force_explicit && maxc > 0;
+    int64_t ulen = 0;
+    int32_t umax = 0, umin = 0;
+    if (stencil) {
+        for (int pass = 0; pass < 2 && stencil; ++pass) {
+            int32_t k = 0;
+            int32_t head = k < c ? lst[0] - (int32_t)p : INT_MIN;
+            int64_t pos = 0;
+            for (;;) {
+                const int32_t m = __reduce_max_sync(0xffffffffu, head);
+                if (m == INT_MIN) break;
+                if (pass == 0) {
+                    if (pos == 0) umax = m;
+                    umin = m;
+                    if (pos + 1 > limit) {
+                        stencil = false;
+                        break;
+                    }
+                } else if (lane == 0) {
+                    uni[s * ustride + pos] = m;
+                }
+                if (head == m) {
+                    ++k;
+                    head = k < c ? lst[32 * (int64_t)k] - (int32_t)p : INT_MIN;
+                }
+                ++pos;
+            }
+            ulen = pos;
+            if (pass == 0 && stencil) {
+                // every slot a lane scans must name an in-range record
+                const bool ok = c == 0 || (p + umax < N && p + umin >= 0);
+                stencil = __all_sync(0xffffffffu, ok);
+            }
+        }
+    }
+    if (lane == 0) {
+        mode[s] = stencil ? kStencil : kExplicit;
+        len[s] = stencil ? (int32_t)ulen : maxc;
+    }
+}
+
+// Pass 2, one thread per particle (a warp per slice): the runtime arrays.
+// Stencil slices: the union offsets into nbr, and each bond's slot found by
+// a binary search of its offset in the (descending) union; explicit slices:
+// the build layout's indices copied.  Intact and family-member bits go to
+// the lane's own words; cnt_rt = last occupied slot + 1.
+__global__ void k_layout_fill(int64_t N, const int64_t *__restrict__ slice_ptr, const int32_t *__restrict__ cnt,
+                              const int32_t *__restrict__ nbr_b, const uint32_t *__restrict__ w_b,
+                              const SliceInfo *__restrict__ si, const int32_t *__restrict__ ulen, int64_t ustride,
+                              const int32_t *__restrict__ uni, int32_t *__restrict__ nbr, uint32_t *__restrict__ words,
+                              uint32_t *__restrict__ fam, int32_t *__restrict__ cnt_rt) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const int64_t s = p >> 5;
+    const int lane = (int)(p & 31);
+    const SliceInfo d = si[s];
+    const int32_t c = cnt[p];
+    const int64_t base = slice_ptr[s] + lane, wb = slice_ptr[s] / 32 + lane, ow = d.word + lane;
+    const int32_t *u = uni + s * ustride;
+    const int32_t ul = d.mode == kStencil ? ulen[s] : 0;
+    if (d.mode == kStencil) {
+        for (int32_t j = lane; j < ul; j += 32) nbr[d.nbr + j] = u[j];
+    } else {
+        for (int32_t k = 0; k < d.len; ++k) nbr[d.nbr + 32 * (int64_t)k + lane] = nbr_b[base + 32 * (int64_t)k];
+    }
+    int32_t last = -1;
+    for (int32_t k = 0; k < c; ++k) {
+        int32_t slot = k;
+        if (d.mode == kStencil) {
+            const int32_t o = nbr_b[base + 32 * (int64_t)k] - (int32_t)p;
+            int32_t lo = 0, hi = ul - 1;  // u descends: find u[slot] == o
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (u[mid] > o) lo = mid + 1;
+                else hi = mid;
+            }
+            slot = lo;
+        }
+        const uint32_t bit = 1u << (slot & 31);
+        fam[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+        if ((w_b[wb + 32 * (int64_t)(k >> 5)] >> (k & 31)) & 1u) words[ow + 32 * (int64_t)(slot >> 5)] |= bit;
+        last = slot;
+    }
+    cnt_rt[p] = last + 1;
 }
 
 __global__ void k_popcount(int64_t N, const SliceInfo *__restrict__ si,
@@ -749,6 +896,20 @@ void launch_fill_neighbors(cudaStream_t st, int64_t n, int64_t first, const doub
                                                         nullptr, slice_ptr, nbr); pd::note_launch();
 }
 
+void launch_cell_ids(cudaStream_t st, int64_t n, int64_t first, const double4 *x4, double3 lo, double cell,
+                     int3 dims, int64_t cell_base, int32_t *cell_of, int32_t *count) {
+    if (n <= 0) return;
+    k_cell_ids<<<grid_for(n), kThreads, 0, st>>>(n, first, x4, lo, cell, dims, cell_base, cell_of, count);
+    pd::note_launch();
+}
+
+void launch_cell_scatter(cudaStream_t st, int64_t n, int64_t first, const int32_t *cell_of, int32_t *cursor,
+                         int32_t *cell_list) {
+    if (n <= 0) return;
+    k_cell_scatter<<<grid_for(n), kThreads, 0, st>>>(n, first, cell_of, cursor, cell_list);
+    pd::note_launch();
+}
+
 void launch_sort_neighbors(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                            const int32_t *cnt, int32_t *nbr) {
     k_sort_neighbors<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, nbr); pd::note_launch();
@@ -757,6 +918,26 @@ void launch_sort_neighbors(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
 void launch_init_intact(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                         const int32_t *cnt, uint32_t *words) {
     k_init_intact<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, words); pd::note_launch();
+}
+
+void launch_layout_union(cudaStream_t st, int64_t S, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                         const int32_t *nbr_b, int32_t force_explicit, int64_t ustride, int32_t *mode, int32_t *len,
+                         int32_t *uni) {
+    if (S <= 0) return;
+    const int64_t threads = S * 32;
+    k_layout_union<<<(unsigned)((threads + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        S, N, slice_ptr, cnt, nbr_b, force_explicit, ustride, mode, len, uni);
+    pd::note_launch();
+}
+
+void launch_layout_fill(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                        const int32_t *nbr_b, const uint32_t *w_b, const SliceInfo *si, const int32_t *ulen,
+                        int64_t ustride, const int32_t *uni, int32_t *nbr, uint32_t *words, uint32_t *fam,
+                        int32_t *cnt_rt) {
+    if (N <= 0) return;
+    k_layout_fill<<<grid_for(N), kThreads, 0, st>>>(N, slice_ptr, cnt, nbr_b, w_b, si, ulen, ustride, uni, nbr,
+                                                      words, fam, cnt_rt);
+    pd::note_launch();
 }
 
 void launch_popcount(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,

@@ -165,11 +165,12 @@ struct BCDev {
 // Launchers (pd_exact.cu, compiled with -fmad=false)
 // ---------------------------------------------------------------------
 // Family build.
-void launch_cell_ids(cudaStream_t st, int64_t n, const double4 *x4, int64_t first,
-                     double3 origin, double inv_cell, int3 dims, int64_t cell_base,
-                     int32_t *cell_of);
-void launch_cell_scatter(cudaStream_t st, int64_t n, int64_t first, const int32_t *cell_of,
-                         int32_t *cursor, int32_t *cell_list);
+// Cell binning of one block: cell ids (into the concatenated grids) and
+// per-cell counts, then, from the cell starts, the cell lists.
+void launch_cell_ids(cudaStream_t st, int64_t n, int64_t first, const double4 *x4, double3 lo, double cell,
+                     int3 dims, int64_t cell_base, int32_t *cell_of, int32_t *count);
+void launch_cell_scatter(cudaStream_t st, int64_t n, int64_t first, const int32_t *cell_of, int32_t *cursor,
+                         int32_t *cell_list);
 void launch_count_neighbors(cudaStream_t st, int64_t n, int64_t first, const double4 *x4,
                             const int32_t *cell_of, const int32_t *cell_start,
                             const int32_t *cell_list, int64_t cell_base, int3 dims,
@@ -182,6 +183,16 @@ void launch_sort_neighbors(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                            const int32_t *cnt, int32_t *nbr);
 void launch_init_intact(cudaStream_t st, int64_t N, const int64_t *slice_ptr,
                         const int32_t *cnt, uint32_t *words);
+// Runtime layout built on the device from the build layout: per-slice
+// unions and stencil decision (mode, len, union offsets at s * ustride),
+// then the runtime arrays (nbr, words, fam zeroed beforehand; cnt_rt).
+void launch_layout_union(cudaStream_t st, int64_t S, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                         const int32_t *nbr_b, int32_t force_explicit, int64_t ustride, int32_t *mode, int32_t *len,
+                         int32_t *uni);
+void launch_layout_fill(cudaStream_t st, int64_t N, const int64_t *slice_ptr, const int32_t *cnt,
+                        const int32_t *nbr_b, const uint32_t *w_b, const SliceInfo *si, const int32_t *ulen,
+                        int64_t ustride, const int32_t *uni, int32_t *nbr, uint32_t *words, uint32_t *fam,
+                        int32_t *cnt_rt);
 // Runtime layout (SliceInfo) from here on.
 void launch_popcount(cudaStream_t st, int64_t N, const SliceInfo *si, const int32_t *cnt,
                      const uint32_t *words, int32_t *out);
