@@ -609,7 +609,8 @@ def main():
     line["config"]["kernel_shape"] = {"warps_per_slice": shape[0], "unroll": shape[1], "chosen_by":
                                       "PD_KERNEL_SHAPE" if os.environ.get("PD_KERNEL_SHAPE") else "autotuner"}
     line["config"]["launch_path"] = ("persistent cooperative kernel over flip-free runs" if args.persist else
-                                     "CUDA graphs of 32 steps" if not work["contacts"] else "direct launches")
+                                     "CUDA graphs of 32 steps" if not work["contacts"] else
+                                     "CUDA graphs of 32 steps between contact neighbour updates")
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:

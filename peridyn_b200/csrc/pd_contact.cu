@@ -761,6 +761,7 @@ pd_status contacts_finalize(pd_env *env) {
 }
 
 pd_status contacts_update_neighs(pd_env *env, int64_t max_part) {
+    ++env->contact_epoch;  // captured contact steps of older lists are stale
     for (size_t k = 0; k < env->hc.size(); ++k) {
         if (env->hc[k].kind == PD_CONTACT_12) PD_TRY(update12(env, env->hc[k], env->contacts[k]));
         else PD_TRY(update11(env, env->hc[k], env->contacts[k], max_part));

@@ -203,6 +203,7 @@ struct pd_env {
     pd::DBuf<int32_t> flag;
     std::vector<pd::DevBC> bcs;
     std::vector<pd::DevContact> contacts;
+    int64_t contact_epoch = 0;  // incremented whenever the contact lists change
 
     // scratch for the device-pointer entry point and solvers
     pd::DBuf<double4> tmp_y, tmp_f, opt;

@@ -1637,6 +1637,7 @@ struct Fast {
     struct Graph {
         StepArgs<R> a0;
         std::vector<GateItem> gate;
+        int64_t cepoch;  // contact-list generation the captured contact kernels use
         int wps;
         int64_t kernels;  // kernel nodes per replay
         cudaGraphExec_t exec;
@@ -2437,7 +2438,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
     a0.ts = 0;  // graphs run only without time-dependent BCs
     typename Fast<R>::Graph *hit = nullptr;
     for (auto &g : F.graphs)
-        if (g.wps == F.wps && g.gate.size() == F.gitems_h.size() &&
+        if (g.wps == F.wps && g.cepoch == env->contact_epoch && g.gate.size() == F.gitems_h.size() &&
             std::memcmp(&g.a0, &a0, sizeof(a0)) == 0 &&
             std::memcmp(g.gate.data(), F.gitems_h.data(), g.gate.size() * sizeof(GateItem)) == 0) {
             hit = &g;
@@ -2456,7 +2457,31 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
             a.dir_vel = a.dir_pos = a0.dir_vel;
             a.ts = 0;
             gate_launch(env, a, F);
-            launch_force<R, 1>(env, st, F.wps, a, lps);
+            if (env->hc.empty()) {
+                launch_force<R, 1>(env, st, F.wps, a, lps);
+            } else {
+                // as a direct contact step: contact accelerations at this
+                // step's positions into F.cacc, the fused step adds them,
+                // the touched entries are cleared
+                if (lps) launch_theta(st, F.wps, a);
+                if (a.ep) launch_td(st, F.wps, a);
+                StepArgs<R> b = a;
+                b.f = F.cacc.p;
+                const pd_status cs = contacts_fast(env, b);
+                if (cs != PD_OK) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(st, &g);
+                    if (g) cudaGraphDestroy(g);
+                    F.cur = cur0;
+                    env->ecur = ecur0;
+                    add_launches(-(launch_count() - n0));
+                    return cs;
+                }
+                a.cacc = F.cacc.p;
+                launch_step<R, 1>(st, F.wps, a);
+                if (a.ep) env->ecur = 1 - env->ecur;
+                contacts_clear(env, F.cacc.p);
+            }
             F.cur = 1 - F.cur;
         }
         cudaGraph_t graph = nullptr;
@@ -2470,7 +2495,7 @@ pd_status replay_graph(pd_env *env, Fast<R> &F, bool lps) {
         const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         if (ie != cudaSuccess) return cuda_fail(ie, "graph instantiate", __FILE__, __LINE__);
-        F.graphs.push_back(typename Fast<R>::Graph{a0, F.gitems_h, F.wps, kernels, exec});
+        F.graphs.push_back(typename Fast<R>::Graph{a0, F.gitems_h, env->contact_epoch, F.wps, kernels, exec});
         hit = &F.graphs.back();
     }
     CK(cudaGraphLaunch(hit->exec, st));
@@ -2557,12 +2582,13 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
         note_launch();
         F.cur = 1 - F.cur;
     }
-    // Steps without contacts run as replays of a captured graph of
-    // kGraphSteps steps while the BC directions stay constant; the rest
-    // (contacts, direction flips, the last step) launch directly.  With
-    // profiling on, timing events bracket each replay (kGraphSteps steps)
-    // and the bond kernels of each direct step.
-    const bool graphs = !contacts && !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
+    // Steps run as replays of a captured graph of kGraphSteps steps while
+    // the BC directions stay constant (with contacts: between neighbour
+    // updates, which change the contact lists; a graph is keyed by their
+    // generation); the rest (direction flips, time-dependent BCs, the last
+    // step) launch directly.  With profiling on, timing events bracket each
+    // replay (kGraphSteps steps) and the bond kernels of each direct step.
+    const bool graphs = !time_dependent_bcs(env) && !std::getenv("PD_NO_GRAPHS");
     // With PD_PERSIST=1, once every block has deformed (no gate), flip-free
     // runs go to one persistent cooperative launch when the grid of the
     // chosen shape fits on the device.  Off by default: on B200 the graph
@@ -2570,7 +2596,7 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
     // against 49.1 us per step; 17.6 k-particle PMB cube: 15.6 against
     // 17.5 us), the grid barriers costing more than graph kernel boundaries.
     const char *pe = std::getenv("PD_PERSIST");
-    const bool persist = graphs && pe && std::strcmp(pe, "1") == 0 && !any_ep(env);
+    const bool persist = graphs && !contacts && pe && std::strcmp(pe, "1") == 0 && !any_ep(env);
     bool persist_fits = true;
     PD_TRY(gate_prepare(env, F));
     for (int64_t s = 0; s < nsteps;) {

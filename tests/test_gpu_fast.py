@@ -186,18 +186,30 @@ def _tofro_bar():
     return {"materials": [mat], "contacts": [], "bcs": bcs, "dt": 2e-8}
 
 
+def _small_impact():
+    return configs.disk_impact(radius=3.0e-3, thickness=1.0e-3, spacing=2.5e-4, sphere_radius=1.0e-3, speed=300.0)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-@pytest.mark.parametrize("builder", [_tofro_bar, lambda: configs.batched_cubes(nspec=6, edge_lo=5, edge_hi=9)])
+@pytest.mark.parametrize("builder", [_tofro_bar, lambda: configs.batched_cubes(nspec=6, edge_lo=5, edge_hi=9),
+                                     _small_impact])
 def test_graph_replay_matches_direct_launches(precision, builder, monkeypatch):
     # graph replays of 32 steps (between BC direction flips, gate kernels
-    # included while a block is undeformed) against one launch per kernel
+    # included while a block is undeformed; with contact, between neighbour
+    # updates, the contact kernels captured with the step) against one
+    # launch per kernel
     w = builder()
 
     def run():
         env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
         if w["bcs"]:
             pb.apply_bc_at0(env, 0)
+        if w["contacts"]:
+            pb.update_neighs(env)
+            pb.update_acc(env)
         pb.velocity_verlet_step(env, nsteps=150)
+        if w["contacts"]:
+            pb.update_neighs(env)  # new lists: the captured contact steps are re-captured
         pb.velocity_verlet_step(env, nsteps=75)
         out = env.get_state(), [env._family(b)[1] for b in range(len(w["materials"]))], env.deformed()
         env.close()
