@@ -681,11 +681,11 @@ static pd_status build_runtime_layout_device(pd_env *env, const std::vector<int6
     int32_t maxc_all = 0;
     for (int64_t p = 0; p < N; ++p) maxc_all = std::max(maxc_all, cnt_b[p]);
     const int64_t ustride = round_up((int64_t)maxc_all + maxc_all / 4 + 33, 32);
-    DBuf<int32_t> d_mode, d_len, d_uni, d_cnt_rt;
-    PD_TRY(d_mode.alloc(std::max<int64_t>(S, 1)));
-    PD_TRY(d_len.alloc(std::max<int64_t>(S, 1)));
-    PD_TRY(d_uni.alloc(std::max<int64_t>(S * ustride, 1)));
-    PD_TRY(d_cnt_rt.alloc(std::max<int64_t>(N, 1)));
+    SBuf<int32_t> d_mode, d_len, d_uni, d_cnt_rt;
+    PD_TRY(d_mode.alloc(std::max<int64_t>(S, 1), st));
+    PD_TRY(d_len.alloc(std::max<int64_t>(S, 1), st));
+    PD_TRY(d_uni.alloc(std::max<int64_t>(S * ustride, 1), st));
+    PD_TRY(d_cnt_rt.alloc(std::max<int64_t>(N, 1), st));
     launch_layout_union(st, S, N, d_slice_ptr, env->cnt.p, d_nbr, force_explicit ? 1 : 0, ustride, d_mode.p,
                         d_len.p, d_uni.p);
     CK(cudaGetLastError());
@@ -877,7 +877,7 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
     std::vector<int32_t> cnt(N, 0);
     std::vector<CellGrid> cells(env->hb.size());
     std::vector<int64_t> cell_base(env->hb.size(), 0);
-    DBuf<int32_t> d_cell_of, d_cell_start, d_cell_list;
+    SBuf<int32_t> d_cell_of, d_cell_start, d_cell_list;
     {
         int64_t tot_cells = 0, tot_part = 0;
         std::vector<int64_t> part_off(env->hb.size(), 0);
@@ -896,11 +896,11 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
         if (tot_part > 0) {
             // counting sort by cell on the device: ids and counts, starts
             // (scanned on the host: one entry per cell), lists
-            PD_TRY(d_cell_of.alloc(tot_part));
-            PD_TRY(d_cell_start.alloc(tot_cells + 1));
-            PD_TRY(d_cell_list.alloc(tot_part));
-            DBuf<int32_t> d_count;
-            PD_TRY(d_count.alloc(tot_cells + 1));
+            PD_TRY(d_cell_of.alloc(tot_part, st));
+            PD_TRY(d_cell_start.alloc(tot_cells + 1, st));
+            PD_TRY(d_cell_list.alloc(tot_part, st));
+            SBuf<int32_t> d_count;
+            PD_TRY(d_count.alloc(tot_cells + 1, st));
             CK(cudaMemsetAsync(d_count.p, 0, (tot_cells + 1) * sizeof(int32_t), st));
             for (size_t bi = 0; bi < env->hb.size(); ++bi) {
                 HostBlock &b = env->hb[bi];
@@ -988,13 +988,13 @@ extern "C" pd_status pd_env_finalize(pd_env *env) {
     // PD_LAYOUT_HOST=1 asks for the host conversion.
     const char *lh = std::getenv("PD_LAYOUT_HOST");
     const bool layout_on_device = !any_host && !(lh && std::strcmp(lh, "1") == 0);
-    DBuf<int64_t> d_slice_ptr;
-    DBuf<int32_t> d_nbr;
-    DBuf<uint32_t> d_words;
+    SBuf<int64_t> d_slice_ptr;
+    SBuf<int32_t> d_nbr;
+    SBuf<uint32_t> d_words;
     {
-        PD_TRY(d_slice_ptr.alloc(S + 1));
-        PD_TRY(d_nbr.alloc(std::max<int64_t>(bnnz, 32)));
-        PD_TRY(d_words.alloc(std::max<int64_t>(bnnz / 32, 1)));
+        PD_TRY(d_slice_ptr.alloc(S + 1, st));
+        PD_TRY(d_nbr.alloc(std::max<int64_t>(bnnz, 32), st));
+        PD_TRY(d_words.alloc(std::max<int64_t>(bnnz / 32, 1), st));
         CK(cudaMemcpyAsync(d_slice_ptr.p, slice_ptr.data(), (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(env->cnt.p, cnt.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d_nbr.p, 0, std::max<int64_t>(bnnz, 32) * sizeof(int32_t), st));

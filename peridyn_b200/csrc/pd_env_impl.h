@@ -69,6 +69,37 @@ struct DBuf {
     }
 };
 
+// Device buffer allocated and freed in stream order (cudaMallocAsync /
+// cudaFreeAsync on one stream): for temporaries of a call that may run
+// while other streams of the device are busy (a server admitting a job),
+// since cudaMalloc / cudaFree wait for the whole device.
+template <class T>
+struct SBuf {
+    T *p = nullptr;
+    cudaStream_t st = nullptr;
+    SBuf() = default;
+    SBuf(const SBuf &) = delete;
+    SBuf &operator=(const SBuf &) = delete;
+    ~SBuf() { reset(); }
+    void reset() {
+        if (p) cudaFreeAsync(p, st);
+        p = nullptr;
+    }
+    pd_status alloc(size_t count, cudaStream_t stream) {
+        reset();
+        st = stream;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMallocAsync((void **)&p, count * sizeof(T), stream);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return fail(PD_ERR_OOM, "cudaMallocAsync of %zu bytes failed: %s", count * sizeof(T),
+                        cudaGetErrorString(e));
+        }
+        return PD_OK;
+    }
+};
+
 struct HostBlock {
     int64_t n = 0;
     int32_t kind = 0, nt = 1;

@@ -1018,6 +1018,8 @@ struct JobTable {
     int32_t bstart[kJobsPerLaunch + 1];
     int32_t n;
 };
+static_assert(sizeof(JobTable<float>) <= 32764 && sizeof(JobTable<double>) <= 32764,
+              "a job table must fit the kernel parameter space");
 
 template <class R>
 __device__ __forceinline__ int job_of_block(const JobTable<R> &t, int32_t b) {

@@ -410,6 +410,29 @@ class SlabRank:
         if self._env_stream is not None:
             self._env_stream.synchronize()
 
+    def diagnostics(self):
+        """printdata's sums (environment.jl:308-320) over the whole body:
+        momentum and force sums, mean damage and intact bonds of the
+        particles each rank owns (ghosts excluded), summed over the ranks
+        by one all-reduce (NCCL on the device wire, else on the host).
+        Returns {"p": (3,), "f": (3,), "damage": mean, "bonds": count}."""
+        torch = _torch()
+        own = np.asarray(self.plan.owned[self.rank])
+        if hasattr(self.env, "owned_sums"):
+            local = np.asarray(self.env.owned_sums(own), dtype=np.float64)
+        else:
+            _, _, f, p = self.env.get_state()
+            d = np.zeros(own.size)
+            _abi.check(_abi.lib().pd_env_damage(self.env._h, _abi.dptr(d)))
+            i0 = np.asarray(self.env.intact0, dtype=np.float64)
+            local = np.concatenate([p[:, own].sum(axis=1), f[:, own].sum(axis=1),
+                                    [d[own].sum(), float(own.sum()), ((1.0 - d[own]) * i0[own]).sum()]])
+        dev = self.device if (str(self.device).startswith("cuda") and not self.host_wire) else "cpu"
+        t = torch.as_tensor(local, dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t)
+        g = t.cpu().numpy()
+        return {"p": g[0:3], "f": g[3:6], "damage": g[6] / max(g[7], 1.0), "bonds": int(round(g[8]))}
+
     def owned_state(self):
         """(environment-order indices, y, v, f) of the particles this rank
         owns."""

@@ -50,6 +50,7 @@ def _rank_main(rank, world, port, precision, nsteps, out):
         r = SlabRank(plan, rank, dist, env, device="cuda:0", wire="host")
         r.step(nsteps)
         out[rank] = r.owned_state()
+        out[f"diag{rank}"] = r.diagnostics()
         env.close()
     finally:
         dist.destroy_process_group()
@@ -63,8 +64,12 @@ def _whole(w, precision, nsteps):
     pb.apply_bc_at0(env, 0)
     pb.velocity_verlet_step(env, nsteps=nsteps)
     y, v, f, _ = env.get_state()
+    diag = np.zeros(8)
+    from peridyn_b200 import _abi
+
+    _abi.check(_abi.lib().pd_env_diagnostics(env._h, _abi.dptr(diag)))
     env.close()
-    return y, v, f
+    return y, v, f, diag
 
 
 @pytest.mark.parametrize("precision", ["fp64_serial", "fp32c"])
@@ -85,13 +90,21 @@ def test_two_slab_ranks_match_whole_body(precision):
         assert p.exitcode == 0
 
     w = _workload()
-    y0, v0, f0 = _whole(w, precision, nsteps)
+    y0, v0, f0, diag = _whole(w, precision, nsteps)
     n = y0.shape[1]
     y1, v1, f1 = np.full((3, n), np.nan), np.full((3, n), np.nan), np.full((3, n), np.nan)
     for rank in range(2):
         idx, ys, vs, fs = out[rank]
         y1[:, idx], v1[:, idx], f1[:, idx] = ys, vs, fs
     assert not np.isnan(y1).any()  # every particle owned by exactly one rank
+    # the ranks' all-reduced diagnostics: the whole body's, counted once
+    d0, d1 = out["diag0"], out["diag1"]
+    assert np.array_equal(d0["p"], d1["p"]) and d0["bonds"] == d1["bonds"]
+    assert d0["bonds"] == int(diag[7])
+    for got, ref in ((d0["p"], diag[0:3]), (d0["f"], diag[3:6])):
+        scale = np.abs(ref).max() + 1e-300
+        assert np.abs(np.asarray(got) - ref).max() <= 1e-9 * scale
+    assert abs(d0["damage"] - diag[6]) <= 1e-12
     if precision == "fp64_serial":
         assert np.array_equal(y0, y1)
         assert np.array_equal(v0, v1)

@@ -117,6 +117,54 @@ def _rank_main(rank, world, port, nslabs, out):
         dist.destroy_process_group()
 
 
+class _FakeDiag:
+    """Per-particle values standing for a slab's state: owned_sums returns
+    the local sums SlabRank.diagnostics reduces."""
+
+    def __init__(self, vals):
+        self.vals = vals  # (n, 9): p (3), f (3), damage, 1, intact bonds
+
+    def owned_sums(self, own):
+        return self.vals[own].sum(axis=0)
+
+
+def _diag_main(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w = _bar()
+        plan = SlabPlan(w["materials"], world)
+        loc = plan.local[rank]
+        g = loc.astype(np.float64)  # values keyed by the global index: ghosts repeat owners' rows
+        vals = np.stack([g, 2 * g, -g, g, 0 * g, 1 + 0 * g, 0.5 + 0 * g, 1 + 0 * g, 10 + 0 * g], axis=1)
+        d = SlabRank(plan, rank, dist, _FakeDiag(vals), device="cpu").diagnostics()
+        out[rank] = (list(d["p"]), list(d["f"]), d["damage"], d["bonds"])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_diagnostics_allreduce_gloo():
+    """The body's sums counted once: owned particles only, summed over the
+    ranks; every rank gets the same totals."""
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_diag_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    n = _bar()["materials"][0].general.n
+    s = n * (n - 1) / 2
+    assert out[0] == out[1]
+    p, f, dmg, bonds = out[0]
+    assert p == [s, 2 * s, -s] and f == [s, 0.0, float(n)]
+    assert dmg == 0.5 and bonds == 10 * n
+
+
 def test_two_rank_halo_exchange_gloo():
     ctx = mp.get_context("spawn")
     mgr = ctx.Manager()
