@@ -320,7 +320,7 @@ def run_serving(args, rank, world, local):
         jobs, arrivals = [jobs[i] for i in mine], [arrivals[i] for i in mine]
         warm, warm_arr = configs.serving_jobs(4, seed=99, n_lo=5e3, n_hi=2e4, steps_lo=100, steps_hi=200,
                                               precision=precision)
-        with pb.Server(device=local) as srv:
+        with pb.Server(device=local, max_active=args.max_active) as srv:
             pb.serve_stream(srv, warm, [0.0] * len(warm))
             runs = []
             for _ in range(args.steps):
@@ -337,7 +337,7 @@ def run_serving(args, rank, world, local):
         line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": 1, "ms_per_step": 1e3 * main["wall_s"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 (f64 position accumulator)", "data": "synthetic",
-                "config": {"workload": f"serving_{args.jobs}_jobs_poisson50",
+                "config": {"workload": f"serving_{args.jobs}_jobs_poisson50", "max_active": args.max_active,
                            "sizes": "log-uniform 5e3..5e5 particles", "steps": "U{500..5000}",
                            "parallelism": f"one server per GPU x{world}" if world > 1 else "1 GPU"},
                 "latency_ms": main["latency_ms"], "fp64_compare": out["fp64"],
@@ -400,6 +400,9 @@ def main():
     ap.add_argument("--workload", default="batched",
                     choices=["lps_bar", "pmb_cube", "batched", "disk_impact", "elasto_plastic", "serving"])
     ap.add_argument("--jobs", type=int, default=48, help="serving: jobs per stream")
+    ap.add_argument("--max-active", type=int, default=16, help="serving: most jobs resident at once")
+    ap.add_argument("--no-pipe-peaks", action="store_true",
+                    help="skip measuring the FP32 and MUFU pipe rates for the compute roofline")
     ap.add_argument("--precision", default="fp32c", choices=["fp64_serial", "fp64", "fp32c"])
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip timing the plain FP64 GPU path beside an FP32C run")
@@ -611,6 +614,8 @@ def main():
     line["config"]["launch_path"] = ("persistent cooperative kernel over flip-free runs" if args.persist else
                                      "CUDA graphs of 32 steps" if not work["contacts"] else
                                      "CUDA graphs of 32 steps between contact neighbour updates")
+    if args.precision == "fp32c" and not lps and not args.no_pipe_peaks:
+        line["compute"] = compute_roofline(layout["slots"], avg_ms, local)
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:
@@ -625,6 +630,40 @@ def main():
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# Per slot of the FP32C bond-based stencil walk (one lane, one bond slot),
+# counted from the walk's source: FP32-pipe lane operations, a multiply-add
+# counting once -- bond vector 3, displacement difference 3, deformed bond 3,
+# 2 xi + eta 3, |xi|^2 4, numerator e.(2 xi + e) 4, |Y|^2 1, (|Y|+|xi|)|xi| 1,
+# critical-stretch test 1, 1/(dl |Y|) operand 1, c V num 1, coefficient 1,
+# force accumulation 3 -- and MUFU operations: sqrt.approx twice,
+# rcp.approx once.
+FP32_OPS_PER_SLOT = 29
+MUFU_OPS_PER_SLOT = 3
+
+
+def compute_roofline(slots, avg_ms, device):
+    """The bond walk's compute side against the GPU's measured pipe rates
+    (pd_pipe_peaks): lane operations of one step's slots divided by the
+    measured step time, as fractions of the FP32 FMA pipe and of the MUFU
+    pipe."""
+    from peridyn_b200 import _abi
+
+    peaks = _abi.pipe_peaks(device)
+    if not avg_ms or avg_ms <= 0:
+        return {"pipe_peaks": peaks}
+    t = avg_ms * 1e-3
+    fp32 = FP32_OPS_PER_SLOT * slots / t
+    mufu = MUFU_OPS_PER_SLOT * slots / t
+    mufu_peak = min(peaks["sqrt_approx_lane_ops_per_s"], peaks["rcp_approx_lane_ops_per_s"])
+    return {"slots_per_launch": int(slots), "fp32_ops_per_slot": FP32_OPS_PER_SLOT,
+            "mufu_ops_per_slot": MUFU_OPS_PER_SLOT,
+            "fp32_achieved": fp32, "fp32_peak": peaks["ffma_lane_ops_per_s"],
+            "fp32_frac": fp32 / peaks["ffma_lane_ops_per_s"],
+            "mufu_achieved": mufu, "mufu_peak": mufu_peak, "mufu_frac": mufu / mufu_peak,
+            "unit": "lane ops/s", "pipe_peaks": peaks,
+            "peak_source": "measured in this run (pd_pipe_peaks)"}
 
 
 def ctypes_void():

@@ -355,6 +355,13 @@ PD_API pd_status pd_env_set_record_staging(pd_env *env, int32_t mode);
 /* staged = 1 when the running FP32C shape stages; slices with a staging
  * plan and the largest plan in records (any pointer may be NULL). */
 PD_API pd_status pd_env_record_staging(pd_env *env, int32_t *staged, int64_t *slices, int64_t *max_records);
+/* Measured pipe rates of GPU `device` (extension; the compute-side
+ * denominators of the bond walk's roofline), each the best of three ~10 ms
+ * launches over every SM: out[0] FP32 FMA and out[1] packed f32x2 FMA lane
+ * operations per second, out[2] MUFU sqrt.approx and out[3] MUFU
+ * rcp.approx lane operations per second, out[4] warp instructions issued
+ * per second by a mix of FP32 FMA and integer logic (both pipes busy). */
+PD_API pd_status pd_pipe_peaks(int32_t device, double *out5);
 
 /* ---------------------------------------------------------------------- */
 /* Serving (extension): a request loop that admits simulation jobs by HBM  */

@@ -148,6 +148,7 @@ _SIGNATURES = {
     "pd_force_density_device_static": (ctypes.c_int32, [c_vp, ctypes.c_int64, c_vp, c_vp, c_vp]),
     "pd_env_stream": (ctypes.c_int32, [c_vp, ctypes.POINTER(c_vp)]),
     "pd_kernel_launches": (ctypes.c_int32, [c_i64p]),
+    "pd_pipe_peaks": (ctypes.c_int32, [ctypes.c_int32, c_dp]),
     "pd_env_vv_steps_async": (ctypes.c_int32, [c_vp, ctypes.c_int64]),
     "pd_env_profile": (ctypes.c_int32, [c_vp, ctypes.c_int32]),
     "pd_env_profile_read": (ctypes.c_int32, [c_vp, c_dp, c_i64p]),
@@ -228,3 +229,15 @@ def kernel_launches():
     n = ctypes.c_int64(0)
     check(lib().pd_kernel_launches(ctypes.byref(n)))
     return int(n.value)
+
+
+PIPE_KEYS = ("ffma_lane_ops_per_s", "ffma2_lane_fmas_per_s", "sqrt_approx_lane_ops_per_s",
+             "rcp_approx_lane_ops_per_s", "ffma_lop3_warp_instr_per_s")
+
+
+def pipe_peaks(device=0):
+    """Measured pipe rates of a GPU (pd_pipe_peaks) as a dict keyed by
+    PIPE_KEYS."""
+    out = np.zeros(5)
+    check(lib().pd_pipe_peaks(int(device), dptr(out)))
+    return dict(zip(PIPE_KEYS, (float(x) for x in out)))

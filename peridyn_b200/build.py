@@ -35,6 +35,7 @@ UNITS = [
     ("pd_fast.cu", ["-fmad=false", "-ftz=true"]),
     ("pd_noalloc.cu", ["-fmad=false"]),
     ("pd_server.cu", ["-fmad=false"]),
+    ("pd_peaks.cu", ["-fmad=false", "-ftz=true"]),
 ]
 
 

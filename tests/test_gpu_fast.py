@@ -454,3 +454,24 @@ def test_elasto_plastic_fast_graphs_match_direct(precision, monkeypatch):
         assert np.array_equal(a, b)
     assert np.array_equal(i1, i2)
     assert np.array_equal(e1, e2)
+
+
+def test_pipe_peaks_are_physical():
+    """pd_pipe_peaks (the compute-side roofline denominators): every rate
+    positive and below what the SMs could do at 2.2 GHz (128 FP32 lanes, 16
+    MUFU lanes and 4 issuing sub-partitions per SM)."""
+    import torch
+
+    from peridyn_b200 import _abi
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    r = _abi.pipe_peaks(0)
+    print(r)
+    clk = 2.2e9
+    assert 0 < r["ffma_lane_ops_per_s"] <= sms * 128 * clk
+    assert 0 < r["ffma2_lane_fmas_per_s"] <= 2 * sms * 128 * clk
+    for k in ("sqrt_approx_lane_ops_per_s", "rcp_approx_lane_ops_per_s"):
+        assert 0 < r[k] <= sms * 32 * clk
+    assert 0 < r["ffma_lop3_warp_instr_per_s"] <= sms * 4 * clk
+    # a full grid of independent chains keeps the FMA pipe busy
+    assert r["ffma_lane_ops_per_s"] >= 0.5 * sms * 128 * 1.0e9
