@@ -1505,30 +1505,19 @@ __device__ __forceinline__ void ypos(const StepArgs<R> &a, int64_t p, double &y0
     y2 = x.z + u2;
 }
 
-// The contact kernels run over the lists of particles with contact work
-// (act, nact entries; built with the neighbour lists), or over the whole
-// set when act is null.
-template <class R>
-__global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows, const int32_t *nb,
-                         const double *dens, CLawF law, const int32_t *act, int64_t nact) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= nact) return;
-    const int64_t i = act ? act[t] : t;
-    const int64_t p = first1 + i;
-    double yi0, yi1, yi2, a0 = 0, a1 = 0, a2 = 0;
-    ypos(a, p, yi0, yi1, yi2);
-    const double inv = 1.0 / dens[p];
-    for (int64_t r = 0; r < rows; ++r) {
-        const int32_t j = nb[r * n1 + i];
-        if (j < 0) break;
-        double yj0, yj1, yj2, F0, F1, F2;
-        ypos(a, j, yj0, yj1, yj2);
-        cfn(law, yi0 - yj0, yi1 - yj1, yi2 - yj2, F0, F1, F2);
-        const double s = a.x64[j].w * inv;
-        a0 += F0 * s;
-        a1 += F1 * s;
-        a2 += F2 * s;
+// Sum of the 32 lanes' partial sums in a fixed butterfly order (every lane
+// ends with the same bits: each stage adds the same two values).
+__device__ __forceinline__ void warp_sum3(double &a0, double &a1, double &a2) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
     }
+}
+
+template <class R>
+__device__ __forceinline__ void add_contact(const StepArgs<R> &a, int64_t p, double a0, double a1, double a2) {
     typename Tr<R>::V4 f = a.f[p];
     f.x += (R)a0;
     f.y += (R)a1;
@@ -1536,10 +1525,50 @@ __global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows
     a.f[p] = f;
 }
 
+// The contact kernels run over the lists of particles with contact work
+// (act, nact entries; built with the neighbour lists), or over the whole
+// set when act is null: one warp per listed particle, its lanes taking
+// every 32nd neighbour row, the lanes' sums combined in a fixed order, so
+// results do not depend on scheduling.  (A thread per particle left the
+// few thousand listed particles of an impact to a handful of warps, each
+// walking its rows one dependent load after another.)
+template <class R>
+__global__ void k_fc12_1(StepArgs<R> a, int64_t first1, int64_t n1, int64_t rows, const int32_t *nb,
+                         const double *dens, CLawF law, const int32_t *act, int64_t nact) {
+    const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= nact) return;  // whole warps
+    const int64_t i = act ? act[t] : t;
+    const int64_t p = first1 + i;
+    double yi0, yi1, yi2, a0 = 0, a1 = 0, a2 = 0;
+    ypos(a, p, yi0, yi1, yi2);
+    const double inv = 1.0 / dens[p];
+    for (int64_t r0 = 0; r0 < rows; r0 += 32) {
+        const int64_t r = r0 + lane;
+        const int32_t j = r < rows ? nb[r * n1 + i] : -1;
+        // a particle's rows end at the first -1; nothing past it is read
+        const uint32_t stop = __ballot_sync(0xffffffffu, j < 0);
+        const int nlive = stop ? __ffs(stop) - 1 : 32;
+        if (lane < nlive) {
+            double yj0, yj1, yj2, F0, F1, F2;
+            ypos(a, j, yj0, yj1, yj2);
+            cfn(law, yi0 - yj0, yi1 - yj1, yi2 - yj2, F0, F1, F2);
+            const double s = a.x64[j].w * inv;
+            a0 += F0 * s;
+            a1 += F1 * s;
+            a2 += F2 * s;
+        }
+        if (stop) break;
+    }
+    warp_sum3(a0, a1, a2);
+    if (lane == 0) add_contact(a, p, a0, a1, a2);
+}
+
 template <class R>
 __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_t *roff, const int32_t *rev,
                          const double *dens, CLawF law, const int32_t *act, int64_t nact) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (t >= nact) return;
     const int64_t j = act ? act[t] : t;
     const int32_t o = roff[j], e = roff[j + 1];
@@ -1548,7 +1577,7 @@ __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_
     double yj0, yj1, yj2, a0 = 0, a1 = 0, a2 = 0;
     ypos(a, q, yj0, yj1, yj2);
     const double inv = 1.0 / dens[q];
-    for (int32_t r = o; r < e; ++r) {
+    for (int32_t r = o + lane; r < e; r += 32) {
         const int32_t i = rev[r];
         double yi0, yi1, yi2, F0, F1, F2;
         ypos(a, i, yi0, yi1, yi2);
@@ -1558,18 +1587,16 @@ __global__ void k_fc12_2(StepArgs<R> a, int64_t first2, int64_t n2, const int32_
         a1 -= F1 * s;
         a2 -= F2 * s;
     }
-    typename Tr<R>::V4 f = a.f[q];
-    f.x += (R)a0;
-    f.y += (R)a1;
-    f.z += (R)a2;
-    a.f[q] = f;
+    warp_sum3(a0, a1, a2);
+    if (lane == 0) add_contact(a, q, a0, a1, a2);
 }
 
 template <class R>
 __global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, int64_t nbrows, const int32_t *nb11,
                        const int32_t *roff, const int32_t *rev, const double *dens, CLawF law, const int32_t *act,
                        int64_t nact) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t t = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (t >= nact) return;
     const int64_t li = act ? act[t] : t;
     const int64_t p = first + li;
@@ -1578,7 +1605,7 @@ __global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, int64_t nbrows, 
     double yp0, yp1, yp2, a0 = 0, a1 = 0, a2 = 0, F0, F1, F2;
     ypos(a, p, yp0, yp1, yp2);
     const double den = dens[p], vol = a.x64[p].w;
-    for (int32_t r = o; r < e; ++r) {
+    for (int32_t r = o + lane; r < e; r += 32) {
         double yi0, yi1, yi2;
         ypos(a, rev[r], yi0, yi1, yi2);
         cfn(law, yi0 - yp0, yi1 - yp1, yi2 - yp2, F0, F1, F2);
@@ -1586,22 +1613,24 @@ __global__ void k_fc11(StepArgs<R> a, int64_t first, int64_t n, int64_t nbrows, 
         a1 -= F1 * (vol / den);
         a2 -= F2 * (vol / den);
     }
-    for (int64_t k = 0; k < nbrows; ++k) {
-        const int32_t q = nb11[k * n + li];
-        if (q < 0) break;
-        double yq0, yq1, yq2;
-        ypos(a, q, yq0, yq1, yq2);
-        cfn(law, yp0 - yq0, yp1 - yq1, yp2 - yq2, F0, F1, F2);
-        const double s = a.x64[q].w / den;
-        a0 += F0 * s;
-        a1 += F1 * s;
-        a2 += F2 * s;
+    for (int64_t k0 = 0; k0 < nbrows; k0 += 32) {
+        const int64_t k = k0 + lane;
+        const int32_t q = k < nbrows ? nb11[k * n + li] : -1;
+        const uint32_t stop = __ballot_sync(0xffffffffu, q < 0);
+        const int nlive = stop ? __ffs(stop) - 1 : 32;
+        if (lane < nlive) {
+            double yq0, yq1, yq2;
+            ypos(a, q, yq0, yq1, yq2);
+            cfn(law, yp0 - yq0, yp1 - yq1, yp2 - yq2, F0, F1, F2);
+            const double s = a.x64[q].w / den;
+            a0 += F0 * s;
+            a1 += F1 * s;
+            a2 += F2 * s;
+        }
+        if (stop) break;
     }
-    typename Tr<R>::V4 f = a.f[p];
-    f.x += (R)a0;
-    f.y += (R)a1;
-    f.z += (R)a2;
-    a.f[p] = f;
+    warp_sum3(a0, a1, a2);
+    if (lane == 0) add_contact(a, p, a0, a1, a2);
 }
 
 // ----------------------------------------------------------------------
@@ -2108,18 +2137,18 @@ pd_status contacts_fast(pd_env *env, StepArgs<R> &a) {
             const int64_t n2 = lists ? dc.nact2 : dc.n2;
             const int32_t *a2 = lists ? dc.act2.p : nullptr;
             if (n1 > 0) {
-                k_fc12_1<R><<<gridn(n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.rows, dc.nb.p, env->dens.p,
-                                                                 law, a1, n1);
+                k_fc12_1<R><<<gridn(32 * n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.rows, dc.nb.p,
+                                                                      env->dens.p, law, a1, n1);
                 note_launch();
             }
             if (n2 > 0) {
-                k_fc12_2<R><<<gridn(n2, 256), 256, 0, env->st>>>(a, dc.first2, dc.n2, dc.rev_off.p, dc.rev.p,
-                                                                 env->dens.p, law, a2, n2);
+                k_fc12_2<R><<<gridn(32 * n2, 256), 256, 0, env->st>>>(a, dc.first2, dc.n2, dc.rev_off.p,
+                                                                      dc.rev.p, env->dens.p, law, a2, n2);
                 note_launch();
             }
         } else if (n1 > 0) {
-            k_fc11<R><<<gridn(n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nbrows, dc.nb.p, dc.rev_off.p,
-                                                           dc.rev.p, env->dens.p, law, a1, n1);
+            k_fc11<R><<<gridn(32 * n1, 256), 256, 0, env->st>>>(a, dc.first1, dc.n1, dc.nbrows, dc.nb.p,
+                                                                dc.rev_off.p, dc.rev.p, env->dens.p, law, a1, n1);
             note_launch();
         }
     }
