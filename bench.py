@@ -608,6 +608,9 @@ def main():
     }
     line["config"]["bond_layout"] = layout
     line["config"]["slot_efficiency"] = float(bonds_start) / max(1, layout["slots"])
+    # the same over the slots the kernels walk (without each slice's padding
+    # of its slot list to a multiple of 32)
+    line["config"]["slot_efficiency_walked"] = float(bonds_start) / max(1, layout["walked_slots"])
     line["config"]["setup_s"] = setup_s
     line["config"]["kernel_shape"] = {"warps_per_slice": shape[0], "unroll": shape[1], "chosen_by":
                                       "PD_KERNEL_SHAPE" if os.environ.get("PD_KERNEL_SHAPE") else "autotuner"}
@@ -615,7 +618,7 @@ def main():
                                      "CUDA graphs of 32 steps" if not work["contacts"] else
                                      "CUDA graphs of 32 steps between contact neighbour updates")
     if args.precision == "fp32c" and not lps and not args.no_pipe_peaks:
-        line["compute"] = compute_roofline(layout["slots"], avg_ms, local)
+        line["compute"] = compute_roofline(layout["walked_slots"], avg_ms, local)
     if fp64_cmp is not None:
         line["fp64_compare"] = fp64_cmp
     if world == 1 and not args.no_cpu_baseline:

@@ -276,7 +276,11 @@ PD_API pd_status pd_env_check_finite(pd_env *env);
  * environment at finalize disables the stencil form. */
 PD_API pd_status pd_env_layout(const pd_env *env, int64_t *out4);
 /* The same and more (extension): out[0..3] as pd_env_layout, out[4] =
- * slices with a record staging plan.  Writes min(n, 5) values. */
+ * slices with a record staging plan, out[5] = slots the step kernels walk
+ * (per slice, 32 lanes x the slots up to the last family member of any of
+ * its particles; bond slots also count the padding of each slice's slot
+ * list to a multiple of 32, which no kernel walks).  Writes min(n, 6)
+ * values. */
 PD_API pd_status pd_env_layout_stats(const pd_env *env, int64_t *out, int64_t n);
 
 /* Halo exchange of a slab decomposition of one specimen (extension: the

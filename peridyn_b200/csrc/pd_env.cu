@@ -488,6 +488,19 @@ struct SetupClock {
 // {ranges, records, (first record, count) per range}, and per stencil slot
 // the staged position of lane 0's record.  nbr_size: entries of the
 // runtime neighbour array (spos has one per entry).
+// Slots the step kernels walk: a slice's warps together visit the slots up
+// to the largest slot count of its 32 particles (whatever the kernel shape),
+// 32 lanes each.
+static int64_t walked_slots(const std::vector<int32_t> &cnt) {
+    int64_t w = 0;
+    for (size_t s0 = 0; s0 < cnt.size(); s0 += kSlice) {
+        int32_t m = 0;
+        for (size_t l = s0; l < s0 + kSlice && l < cnt.size(); ++l) m = std::max(m, cnt[l]);
+        w += (int64_t)kSlice * m;
+    }
+    return w;
+}
+
 static pd_status upload_stage_plans(pd_env *env, const std::vector<SliceInfo> &si,
                                     const std::vector<std::vector<int32_t>> &uni, size_t nbr_size) {
     const int64_t N = env->N, S = N / kSlice;
@@ -638,6 +651,7 @@ static pd_status build_runtime_layout(pd_env *env, const std::vector<int64_t> &s
     env->sinfo_h = si;
     env->cnt_h = cnt;
     env->nnz = (int64_t)kSlice * nwords;
+    env->walked = walked_slots(env->cnt_h);
     env->nbr_len = nbr_len;
     env->stencil_slices = nst;
     cudaStream_t st = env->st;
@@ -745,6 +759,7 @@ static pd_status build_runtime_layout_device(pd_env *env, const std::vector<int6
     env->sinfo_h = si;
     env->cnt_h = cnt_b;
     env->nnz = (int64_t)kSlice * nwords;
+    env->walked = walked_slots(env->cnt_h);
     env->nbr_len = nbr_len;
     env->stencil_slices = nst;
     return PD_OK;
@@ -1443,8 +1458,9 @@ extern "C" pd_status pd_env_layout(const pd_env *env, int64_t *out4) {
 extern "C" pd_status pd_env_layout_stats(const pd_env *env, int64_t *out, int64_t n) {
     PD_TRY(need_final(env));
     if (!out || n < 0) return fail(PD_ERR_ARG, "out is NULL or n < 0");
-    const int64_t v[5] = {env->N / kSlice, env->stencil_slices, env->nnz, env->nbr_len, env->splan_slices};
-    for (int64_t i = 0; i < n && i < 5; ++i) out[i] = v[i];
+    const int64_t v[6] = {env->N / kSlice, env->stencil_slices, env->nnz, env->nbr_len, env->splan_slices,
+                          env->walked};
+    for (int64_t i = 0; i < n && i < 6; ++i) out[i] = v[i];
     return PD_OK;
 }
 

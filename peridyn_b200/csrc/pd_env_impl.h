@@ -200,6 +200,7 @@ struct pd_env {
     std::vector<pd::SliceInfo> sinfo_h;
     std::vector<int32_t> cnt_h;
     int64_t nnz = 0;       // bond slots (bits per bit array)
+    int64_t walked = 0;    // slots the walks visit: per slice 32 x its largest slot count
     int64_t nbr_len = 0;   // entries of nbr[]
     int64_t stencil_slices = 0;
     // Record staging plans of stencil slices (throughput path): the

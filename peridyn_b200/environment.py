@@ -255,11 +255,11 @@ class GeneralEnvironment:
 
     def layout(self):
         """Bond storage: slices, stencil slices, bond slots, index entries,
-        slices with a record staging plan."""
-        out = np.zeros(5, dtype=np.int64)
-        _abi.check(_abi.lib().pd_env_layout_stats(self._h, _abi.i64ptr(out), 5))
+        slices with a record staging plan, slots the step kernels walk."""
+        out = np.zeros(6, dtype=np.int64)
+        _abi.check(_abi.lib().pd_env_layout_stats(self._h, _abi.i64ptr(out), 6))
         return {"slices": int(out[0]), "stencil_slices": int(out[1]), "slots": int(out[2]),
-                "index_entries": int(out[3]), "staged_slices": int(out[4])}
+                "index_entries": int(out[3]), "staged_slices": int(out[4]), "walked_slots": int(out[5])}
 
 
 def Env(id, materials, short_range_contact, boundary_conds, dt, state=2, bskin=0.5, units=False, **kwargs):

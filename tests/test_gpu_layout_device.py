@@ -55,6 +55,9 @@ def test_device_layout_equals_host_layout(name, layout, monkeypatch):
     eh = _env(w, monkeypatch, host=True)
     ed = _env(w, monkeypatch, host=False)
     assert eh.layout() == ed.layout()
+    lay = ed.layout()
+    # every bond is walked; no slice walks past its slot list
+    assert ed.num_bonds() <= lay["walked_slots"] <= lay["slots"]
     if layout == "auto" and name != "cloud":
         assert ed.layout()["stencil_slices"] > 0
     for b in range(len(w["materials"])):
