@@ -61,7 +61,7 @@ def build_workload(name, args):
     if name == "pmb_cube":
         return configs.pmb_cube()
     if name == "batched":
-        return configs.batched_cubes(nspec=args.nspec)
+        return configs.batched_cubes(nspec=args.nspec, cubes=args.cubes)
     if name == "disk_impact":
         return configs.disk_impact()
     if name == "elasto_plastic":
@@ -408,6 +408,8 @@ def main():
                     help="skip timing the plain FP64 GPU path beside an FP32C run")
     ap.add_argument("--sim-steps", type=int, default=0, help="VV steps per bench step (default: workload's)")
     ap.add_argument("--nspec", type=int, default=256)
+    ap.add_argument("--cubes", action="store_true",
+                    help="batched: one drawn edge per specimen (cubes) instead of one per axis")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")

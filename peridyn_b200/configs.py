@@ -55,14 +55,16 @@ def lps_bar(nx=100, ny=20, nz=20, spacing=5.0e-4, horizon_factor=3.0, E=70e9, nu
 
 
 def batched_cubes(nspec=256, seed=4, edge_lo=12, edge_hi=32, spacing=1.0e-3, steps=2000, dt=1.0e-8,
-                  cs_lo=0.002, cs_hi=0.01, v_lo=5.0, v_hi=50.0):
+                  cs_lo=0.002, cs_hi=0.01, v_lo=5.0, v_hi=50.0, cubes=False):
     """Independent PMB cuboids of uneven size (edges uniform over
     edge_lo..edge_hi per axis), critical stretch U(cs_lo, cs_hi), pulse peak
-    U(v_lo, v_hi).  Specimens are separate blocks (type id = block index)."""
+    U(v_lo, v_hi).  Specimens are separate blocks (type id = block index).
+    cubes=True: one drawn edge per specimen (cubes of edge_lo^3 to
+    edge_hi^3 particles) instead of one per axis."""
     u = lattice.uniform(seed, 5 * nspec)
     mats = []
     for s in range(nspec):
-        e = [edge_lo + int(u[5 * s + d] * (edge_hi - edge_lo + 1)) for d in range(3)]
+        e = [edge_lo + int(u[5 * s + (0 if cubes else d)] * (edge_hi - edge_lo + 1)) for d in range(3)]
         cs = cs_lo + (cs_hi - cs_lo) * u[5 * s + 3]
         peak = v_lo + (v_hi - v_lo) * u[5 * s + 4]
         origin = (s * 40 * spacing, 0.0, 0.0)
@@ -70,7 +72,7 @@ def batched_cubes(nspec=256, seed=4, edge_lo=12, edge_hi=32, spacing=1.0e-3, ste
                      type_id=s + 1, name=f"specimen{s}", dt=dt, steps=steps)
         mats.extend(w["materials"])
     return {"materials": mats, "contacts": [], "bcs": [], "dt": dt, "steps": steps,
-            "workload": f"batched_{nspec}_pmb"}
+            "workload": f"batched_{nspec}_pmb" + ("_cubes" if cubes else "")}
 
 
 def disk_impact(radius=0.05, thickness=0.005, spacing=2.5e-4, sphere_radius=0.01, speed=100.0, cs=0.003,
