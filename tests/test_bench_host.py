@@ -1,6 +1,7 @@
 """Host logic of bench.py: the algorithmic byte model behind the roofline
-(the per-bond and per-particle figures of the survey's measurement table)
-and the bounded CPU sample of the batched workload."""
+(the per-bond and per-particle figures of the survey's measurement table),
+the compute roofline's arithmetic, the bounded CPU sample of the batched
+workload and its cube-edge variant."""
 import bench
 from peridyn_b200 import configs
 
@@ -26,3 +27,32 @@ def test_cpu_sample_of_batched_workload_is_its_first_specimens():
     assert text.startswith(f"first {len(sub['materials'])} of 32 specimens")
     bar = configs.lps_bar(nx=20, ny=5, nz=5)
     assert bench.cpu_workload(bar)[0] is bar
+
+
+def test_compute_roofline_fractions(monkeypatch):
+    """The compute object: walked slots x (29 FP32-pipe, 3 MUFU) lane
+    operations over the step time, against the measured pipe rates (here a
+    fake of pd_pipe_peaks: no GPU call)."""
+    from peridyn_b200 import _abi
+
+    fake = dict(zip(_abi.PIPE_KEYS, (3.5e13, 3.7e13, 4.6e12, 4.5e12, 1.1e12)))
+    monkeypatch.setattr(_abi, "pipe_peaks", lambda device=0: fake)
+    c = bench.compute_roofline(320_000_000, 0.5, 0)
+    t = 0.5e-3
+    assert c["fp32_achieved"] == 29 * 320_000_000 / t
+    assert c["fp32_frac"] == c["fp32_achieved"] / 3.5e13
+    # the slower MUFU operation sets the MUFU peak
+    assert c["mufu_peak"] == 4.5e12 and c["mufu_frac"] == 3 * 320_000_000 / t / 4.5e12
+    assert c["slots_per_launch"] == 320_000_000
+    # no step time: only the measured rates
+    assert set(bench.compute_roofline(1, 0.0, 0)) == {"pipe_peaks"}
+
+
+def test_cube_edge_variant_draws_one_edge_per_specimen():
+    w = configs.batched_cubes(nspec=6, cubes=True)
+    for m in w["materials"]:
+        n = round(m.general.n ** (1.0 / 3.0))
+        assert n ** 3 == m.general.n
+    assert w["workload"] == "batched_6_pmb_cubes"
+    # the per-axis default keeps its draws (same specimens as before)
+    assert configs.batched_cubes(nspec=6)["workload"] == "batched_6_pmb"
