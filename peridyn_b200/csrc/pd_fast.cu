@@ -1328,9 +1328,14 @@ __device__ __forceinline__ bool grid_barrier(GridBar *gb, unsigned nblocks) {
     return *(volatile int *)&gb->err == 0;
 }
 
+// The grid is at most what the device holds at once; each block walks the
+// slice groups blockIdx.x, blockIdx.x + gridDim.x, ... of every phase (a
+// block synchronises between groups when its warps share a slice, so the
+// partial sums of one group are read before the next group writes them).
 template <class R, int WPS, int U, bool LPS>
 __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1)
-    k_persist(StepArgs<R> a, typename Tr<R>::V4 *b0, typename Tr<R>::V4 *b1, int nsteps, GridBar *gb) {
+    k_persist(StepArgs<R> a, typename Tr<R>::V4 *b0, typename Tr<R>::V4 *b1, int nsteps, GridBar *gb,
+              int64_t ngroups) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
     __shared__ R sh1[WPS > 1 ? NW : 1][1][32];
@@ -1345,10 +1350,16 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         a.xn = (s & 1) ? b0 : b1;
         a.ts = ts0 + s;
         if (LPS) {
-            theta_body<R, WPS, U, false>(a, blockIdx.x, sh1, arrive);
+            for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+                theta_body<R, WPS, U, false>(a, g, sh1, arrive);
+                if (WPS > 1) __syncthreads();
+            }
             if (!grid_barrier(gb, gridDim.x)) return;
         }
-        step_body<R, WPS, U, 1, false>(a, blockIdx.x, sh, arrive);
+        for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+            step_body<R, WPS, U, 1, false>(a, g, sh, arrive);
+            if (WPS > 1) __syncthreads();
+        }
         if (s + 1 < nsteps && !grid_barrier(gb, gridDim.x)) return;
     }
 }
@@ -2546,18 +2557,21 @@ int64_t flip_free_run(const pd_env *env, int64_t maxn) {
     return n;
 }
 
-// Launch nsteps full steps as one persistent cooperative kernel when the
-// whole grid (at the largest warps-per-slice that fits) can be resident;
-// *done = false leaves the steps to the caller.
+// Launch nsteps full steps as one persistent cooperative kernel of at most
+// as many blocks as the device holds at once (each block walks several
+// slice groups when there are more); *done = false (no block fits) leaves
+// the steps to the caller.
 template <class R, int WPS, int U, bool LPS>
 pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
     constexpr int BT = Split<WPS>::BT, SPB = Split<WPS>::SPB;
-    void (*kern)(StepArgs<R>, typename Tr<R>::V4 *, typename Tr<R>::V4 *, int, GridBar *) = k_persist<R, WPS, U, LPS>;
-    const int64_t blocks = ((env->N + 31) / 32 + SPB - 1) / SPB;
+    void (*kern)(StepArgs<R>, typename Tr<R>::V4 *, typename Tr<R>::V4 *, int, GridBar *, int64_t) =
+        k_persist<R, WPS, U, LPS>;
+    int64_t ngroups = ((env->N + 31) / 32 + SPB - 1) / SPB;
     int per_sm = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, 0));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, env->device));
-    if (blocks > (int64_t)per_sm * sms) {
+    const int64_t blocks = std::min<int64_t>(ngroups, (int64_t)per_sm * sms);
+    if (blocks < 1) {
         *done = false;
         return PD_OK;
     }
@@ -2571,7 +2585,7 @@ pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
     a.ts = env->ts + 1;
     typename Tr<R>::V4 *b0 = F.xu[F.cur].p, *b1 = F.xu[1 - F.cur].p;
     GridBar *gb = F.gbar.p;
-    void *kargs[] = {&a, &b0, &b1, &nsteps, &gb};
+    void *kargs[] = {&a, &b0, &b1, &nsteps, &gb, &ngroups};
     CK(cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)blocks), dim3(BT), kargs, 0, env->st));
     add_launches(1);
     for (int k = 0; k < nsteps; ++k) advance_bc_clock(env);
@@ -2635,12 +2649,15 @@ pd_status vv_chunk(pd_env *env, Fast<R> &F, int64_t nsteps, bool blocking = true
             const int64_t m = flip_free_run(env, std::min<int64_t>(nsteps - 1 - s, 1 << 20));
             if (m >= 8) {
                 bool done = false;
+                prof_begin(env, st);
                 if (lps) PD_TRY((persist_any<R, true>(env, F, (int)m, &done)));
                 else PD_TRY((persist_any<R, false>(env, F, (int)m, &done)));
                 if (done) {
+                    prof_end(env, st, m);
                     s += m;
                     continue;
                 }
+                prof_end(env, st, 0);
                 persist_fits = false;
             }
         }

@@ -251,10 +251,18 @@ def test_scaling_and_container_bcs_fast(oracle, precision, kind):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-def test_persistent_chunks_match_graph_replays(precision, monkeypatch):
+@pytest.mark.parametrize("case", ["bar_2warps", "batch16_1warp", "batch16_2warps"])
+def test_persistent_chunks_match_graph_replays(precision, case, monkeypatch):
     # PD_PERSIST=1: flip-free runs of a deformed problem in one cooperative
-    # launch with grid barriers; same shape, so the same numbers
-    w = configs.lps_bar(nx=30, ny=8, nz=8)
+    # launch with grid barriers; same shape, so the same numbers.  The
+    # 16-specimen batch has more slice groups than the device holds blocks
+    # at once, so each block walks several groups per phase.
+    from peridyn_b200 import _abi
+
+    if case == "bar_2warps":
+        w, wps = configs.lps_bar(nx=30, ny=8, nz=8), 2
+    else:
+        w, wps = configs.batched_cubes(nspec=16), 1 if case == "batch16_1warp" else 2
 
     def run(persist):
         if persist:
@@ -262,15 +270,20 @@ def test_persistent_chunks_match_graph_replays(precision, monkeypatch):
         else:
             monkeypatch.delenv("PD_PERSIST", raising=False)
         env = pb.Env(1, w["materials"], w["contacts"], w["bcs"], w["dt"], precision=precision)
-        env.set_kernel_shape(2, 2 if precision == "fp32c" else 1)
-        pb.apply_bc_at0(env, 0)
+        env.set_kernel_shape(wps, (4 if wps == 1 else 2) if precision == "fp32c" else 1)
+        if w["bcs"]:
+            pb.apply_bc_at0(env, 0)
         pb.velocity_verlet_step(env, nsteps=40)   # deforms: the gate drops out
+        n0 = _abi.kernel_launches()
         pb.velocity_verlet_step(env, nsteps=120)  # persistent when enabled
+        launches = _abi.kernel_launches() - n0
         out = env.get_state()
         env.close()
-        return out
+        return out, launches
 
-    for a, b in zip(run(False), run(True)):
+    (s0, l0), (s1, l1) = run(False), run(True)
+    assert l1 < l0 // 4  # one cooperative launch instead of graph replays of 120 steps
+    for a, b in zip(s0, s1):
         assert np.array_equal(a, b)
 
 
