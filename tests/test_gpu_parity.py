@@ -165,6 +165,22 @@ def test_bond_breaking_trajectory_bit_exact(oracle):
     env.close()
 
 
+def test_lps_bond_breaking_trajectory_bit_exact(oracle):
+    # state-based cube, low critical stretch, 150 m/s pulse: ~2.8 k of 114 k
+    # bonds break in 80 steps; the dilatation of each step uses the previous
+    # step's intact bonds (peri.jl:155-172), the force pass breaks
+    w = configs.lps_cube((12, 11, 10), cs=0.002, peak=150.0)
+    env, ora = _pair(oracle, w)
+    for _ in range(80):
+        ora.vv_step()
+    pb.velocity_verlet_step(env, nsteps=80)
+    assert int((ora.blocks[0].family > 0).sum() - ora.blocks[0].intact.sum()) > 1000
+    _assert_state_equal(env, ora)
+    _assert_bonds_equal(env, ora)
+    assert np.array_equal(pb.cal_damage(env), ora.damage())
+    env.close()
+
+
 def test_rigid_translation_gate(oracle):
     w = configs.pmb_cube(n=8, peak=0.0)
     mat = w["materials"][0]
