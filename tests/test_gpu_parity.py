@@ -330,6 +330,24 @@ def test_family_overflow_is_reported():
     assert e.value.status == _abi.PD_ERR_FAMILY_OVERFLOW
 
 
+def test_family_at_the_max_neigh_boundary(oracle):
+    # 122 neighbours in the exact lattice's interior: max_neigh = 122 is one
+    # short (the overflow above, and the oracle's BoundsError), 123 builds
+    # the same family as the oracle
+    x, vol = lattice.cuboid(7, 7, 7, 1.0)
+    with pytest.raises(IndexError):
+        oracle.cal_family(x, 3.015, 122)
+    fam_ref, _ = oracle.cal_family(x, 3.015, 123)
+    gen = pb.GeneralMaterial(x.copy(order="F"), np.zeros_like(x, order="F"), x, vol, np.ones(x.shape[1], np.int64),
+                             3.015, max_neigh=123)
+    mat = pb.PeridynamicsMaterial(gen, pb.BondBasedSpecific([1.0], [0.1], [1.0]))
+    env = pb.Env(1, [mat], [], [], 1e-3)
+    fam, intact = env._family(0)
+    assert int((fam > 0).sum(axis=0).max()) == 122
+    assert np.array_equal(fam, fam_ref) and np.array_equal(intact, fam > 0)
+    env.close()
+
+
 @pytest.mark.parametrize("kind", ["delta", "scalefixwait", "container"])
 def test_scaling_and_container_bcs_bit_exact(oracle, kind):
     # DeltaScaleBC.jl, ScaleFixWaitBC.jl (check! every 10 steps), ContainerBC.jl
