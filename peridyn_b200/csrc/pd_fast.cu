@@ -1302,6 +1302,7 @@ constexpr unsigned kBarrierSpins = 1u << 25;  // x >= 64 ns: gives up after ~2 s
 // Grid-wide barrier of a cooperative launch; false (and the error flag set)
 // when a block waited past kBarrierSpins.
 __device__ __forceinline__ bool grid_barrier(GridBar *gb, unsigned nblocks) {
+    __shared__ int ok;  // thread 0's reading of the error flag, so the whole block leaves together
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *vgen = &gb->gen;
@@ -1322,10 +1323,11 @@ __device__ __forceinline__ bool grid_barrier(GridBar *gb, unsigned nblocks) {
             }
         }
         __threadfence();
+        ok = *verr == 0;
     }
     __syncthreads();
     __threadfence();
-    return *(volatile int *)&gb->err == 0;
+    return ok != 0;
 }
 
 // The grid is at most what the device holds at once; each block walks the
