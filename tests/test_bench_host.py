@@ -14,7 +14,7 @@ def test_step_bytes_model():
     assert bench.step_bytes(1000, 10, "fp64", False) == 4.125 * 1000 + 168 * 10
     # state-based: two bond sweeps and the dilatation (8 B) per particle
     assert bench.step_bytes(1000, 10, "fp32c", True) == 2 * 4.125 * 1000 + 92 * 10
-    # the C4 figure quoted in the design notes: 290,639,420 bonds, 2,815,119 particles
+    # the 256-specimen batched workload: 290,639,420 bonds, 2,815,119 particles, 1.435 GB per step
     assert abs(bench.step_bytes(290639420, 2815119, "fp32c", False) - 1.4352e9) < 1e6
 
 

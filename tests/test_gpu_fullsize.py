@@ -1,22 +1,22 @@
 """Parity at full size and with bond breaking, against the FP64 oracle.
 
-  C1 (8,000-particle jittered PMB cube, 1,000 steps) with a 100 m/s pulse,
+  The 8,000-particle jittered PMB cube (1,000 steps) with a 100 m/s pulse,
      which breaks ~4,000 bonds: the serial-order FP64 path bit-exact; the
      one-pass FP64 path within 1e-10 and FP32C within 1e-4 relative L2 of
      displacement, velocity and damage.
-  C4 batch: 16 independent PMB cuboids from the batched generator (edges
+  A batch of 16 independent PMB cuboids from the batched generator (edges
      U{12..16} per axis, per-specimen critical stretch U(0.002, 0.01) and
      pulse U(5, 50) m/s) for 600 steps, all three precisions against the
      oracle.
-  C3 geometry, scaled (radius 6 mm, 5 layers at the C3 spacing, sphere of
-     radius 1.5 mm at 100 m/s): a bond-based disk struck by a stiff sphere
-     with nonlinear contact (exponent 2, stiffness 15 c, d_eq = spacing),
-     contact neighbours rebuilt every 10 steps; 200 steps, by which ~6,800
-     bonds under the sphere have broken but the disk has not fragmented;
-     FP64 and FP32C against the oracle.
+  The disk-impact geometry, scaled (radius 6 mm, 5 layers at its 0.25 mm
+     spacing, sphere of radius 1.5 mm at 100 m/s): a bond-based disk struck
+     by a stiff sphere with nonlinear contact (exponent 2, stiffness 15 c,
+     d_eq = spacing), contact neighbours rebuilt every 10 steps; 200 steps,
+     by which ~6,800 bonds under the sphere have broken but the disk has
+     not fragmented; FP64 and FP32C against the oracle.
 
 Tolerances: FP64 one-pass 1e-10 (summation order differs from the serial
-loop), except the C4 batch's velocity, 1e-9: its pulses of up to 50 m/s
+loop), except the 16-cuboid batch's velocity, 1e-9: its pulses of up to 50 m/s
 against critical stretches down to 0.002 keep bonds near their limits for
 600 steps, and the one-ulp differences of the summation order grow to
 ~2e-10 in velocity (measured on B200: displacement 2.0e-11, velocity
@@ -88,20 +88,20 @@ def _compare(env, ref, label):
     return eu, ev, ed, mism, broken, (y, v, f)
 
 
-# --------------------------------------------------------------------- C1
-C1_STEPS = 1000
+# ------------------------------------------------- 8,000-particle PMB cube
+CUBE_STEPS = 1000
 
 
 @pytest.fixture(scope="module")
-def c1(oracle):
+def cube8k(oracle):
     w = configs.pmb_cube(peak=100.0)
-    return w, _oracle_run(oracle, w, C1_STEPS)
+    return w, _oracle_run(oracle, w, CUBE_STEPS)
 
 
-def test_c1_full_size_serial_bit_exact(c1):
-    w, ref = c1
-    env = _gpu_run(w, "fp64_serial", C1_STEPS)
-    eu, ev, ed, mism, broken, (y, v, f) = _compare(env, ref, "C1 fp64_serial")
+def test_cube8k_full_size_serial_bit_exact(cube8k):
+    w, ref = cube8k
+    env = _gpu_run(w, "fp64_serial", CUBE_STEPS)
+    eu, ev, ed, mism, broken, (y, v, f) = _compare(env, ref, "8k cube fp64_serial")
     assert broken > 1000
     assert np.array_equal(y, ref["y"]) and np.array_equal(v, ref["v"]) and np.array_equal(f, ref["f"])
     assert mism == 0
@@ -109,32 +109,32 @@ def test_c1_full_size_serial_bit_exact(c1):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-def test_c1_full_size_throughput(c1, precision):
-    w, ref = c1
-    env = _gpu_run(w, precision, C1_STEPS)
-    eu, ev, ed, mism, broken, _ = _compare(env, ref, f"C1 {precision}")
+def test_cube8k_full_size_throughput(cube8k, precision):
+    w, ref = cube8k
+    env = _gpu_run(w, precision, CUBE_STEPS)
+    eu, ev, ed, mism, broken, _ = _compare(env, ref, f"8k cube {precision}")
     assert eu <= TOL[precision] and ev <= TOL[precision] and ed <= TOL[precision], (eu, ev, ed)
     assert mism <= (0 if precision == "fp64" else broken // 100), f"{mism} of {broken} broken bonds differ"
     env.close()
 
 
-# --------------------------------------------------------------------- C4
-C4_STEPS = 600
+# ------------------------------------------------- batch of 16 PMB cuboids
+BATCH_STEPS = 600
 
 
 @pytest.fixture(scope="module")
-def c4(oracle):
+def batch16(oracle):
     w = configs.batched_cubes(nspec=16, edge_lo=12, edge_hi=16)
-    return w, _oracle_run(oracle, w, C4_STEPS)
+    return w, _oracle_run(oracle, w, BATCH_STEPS)
 
 
 @pytest.mark.parametrize("precision", ["fp64_serial", "fp64", "fp32c"])
-def test_c4_batch_against_oracle(c4, precision):
-    w, ref = c4
+def test_batch16_against_oracle(batch16, precision):
+    w, ref = batch16
     assert len(w["materials"]) == 16
     assert len({float(np.ravel(m.specific.critical_stretch)[0]) for m in w["materials"]}) == 16  # per-specimen cs
-    env = _gpu_run(w, precision, C4_STEPS)
-    eu, ev, ed, mism, broken, (y, v, f) = _compare(env, ref, f"C4 16 specimens {precision}")
+    env = _gpu_run(w, precision, BATCH_STEPS)
+    eu, ev, ed, mism, broken, (y, v, f) = _compare(env, ref, f"16 specimens {precision}")
     assert broken > 100
     if precision == "fp64_serial":
         assert np.array_equal(y, ref["y"]) and np.array_equal(v, ref["v"]) and mism == 0
@@ -145,22 +145,22 @@ def test_c4_batch_against_oracle(c4, precision):
     env.close()
 
 
-# --------------------------------------------------------------------- C3
-C3_STEPS = 200
+# ------------------------------------------------- scaled disk impact
+IMPACT_STEPS = 200
 
 
 @pytest.fixture(scope="module")
-def c3(oracle):
+def impact_scaled(oracle):
     w = configs.disk_impact(radius=6.0e-3, thickness=1.25e-3, spacing=2.5e-4, sphere_radius=1.5e-3, speed=100.0,
                             cs=0.003)
-    return w, _oracle_run(oracle, w, C3_STEPS, neighs_every=10)
+    return w, _oracle_run(oracle, w, IMPACT_STEPS, neighs_every=10)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32c"])
-def test_c3_scaled_disk_impact_before_fragmentation(c3, precision):
-    w, ref = c3
-    env = _gpu_run(w, precision, C3_STEPS, neighs_every=10)
-    eu, ev, ed, mism, broken, _ = _compare(env, ref, f"C3 scaled {precision}")
+def test_scaled_disk_impact_before_fragmentation(impact_scaled, precision):
+    w, ref = impact_scaled
+    env = _gpu_run(w, precision, IMPACT_STEPS, neighs_every=10)
+    eu, ev, ed, mism, broken, _ = _compare(env, ref, f"scaled disk impact {precision}")
     assert broken > 0
     assert eu <= TOL[precision] and ev <= TOL[precision], (eu, ev)
     assert mism <= (0 if precision == "fp64" else max(1, broken // 100)), f"{mism} of {broken} broken bonds differ"
