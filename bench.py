@@ -413,6 +413,8 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving stream measured after the timed runs")
     ap.add_argument("--persist", action="store_true",
                     help="run flip-free stretches as one persistent cooperative launch (PD_PERSIST=1)")
     args = ap.parse_args()
@@ -632,9 +634,32 @@ def main():
                                           + ("(OpenMP over particles, atomic scatter)" if nth > 1 else
                                              "(single thread)")}
     env.close()
+    if world == 1 and not args.no_serving:
+        line["serving"] = serving_sample(args, local)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def serving_sample(args, device):
+    """One serving stream after the timed runs (outside the timed region):
+    args.jobs FP32C jobs of mixed size and kind (log-uniform 5e3..5e5
+    particles, U{500..5000} steps, PMB and state-based) submitted to a
+    pd_server at Poisson arrival times (50 jobs/s, seed 5), after a warm-up
+    stream of 4 small jobs; p50/p99 latency from submission to result and
+    the aggregate bond-updates/s over the stream's wall time."""
+    import peridyn_b200 as pb
+    from peridyn_b200 import configs
+
+    jobs, arrivals = configs.serving_jobs(args.jobs, seed=5, precision="fp32c")
+    warm, _ = configs.serving_jobs(4, seed=99, n_lo=5e3, n_hi=2e4, steps_lo=100, steps_hi=200, precision="fp32c")
+    with pb.Server(device=device, max_active=args.max_active) as srv:
+        pb.serve_stream(srv, warm, [0.0] * len(warm))
+        _, summary = pb.serve_stream(srv, jobs, arrivals)
+    return {"workload": f"serving_{args.jobs}_jobs_poisson50", "precision": "fp32c", "max_active": args.max_active,
+            "jobs": summary["jobs"], "wall_s": summary["wall_s"], "latency_ms": summary["latency_ms"],
+            "aggregate_bond_updates_per_s": summary["bond_updates_per_s"],
+            "timing": "wall clock from the first submission to the last result, after the timed runs"}
 
 
 # Per slot of the FP32C bond-based stencil walk (one lane, one bond slot),
