@@ -1334,10 +1334,35 @@ __device__ __forceinline__ bool grid_barrier(GridBar *gb, unsigned nblocks) {
 // slice groups blockIdx.x, blockIdx.x + gridDim.x, ... of every phase (a
 // block synchronises between groups when its warps share a slice, so the
 // partial sums of one group are read before the next group writes them).
+//
+// The step arguments come as two read-only kernel parameters, one per
+// record-buffer parity (a0: even steps read b0 and write b1; a1: the
+// reverse), and are never modified: the walks then read every field from
+// the parameter bank, as k_step does, instead of from a per-thread copy of
+// the 1.8 KB structure in local memory.  The time step stays at the
+// launch's value: persistent runs, like graph replays, carry no
+// time-dependent boundary condition.
+template <class R, int WPS, int U, bool LPS>
+__device__ __forceinline__ bool persist_step(const StepArgs<R> &a, int64_t ngroups, GridBar *gb, R (*sh)[3][32],
+                                             R (*sh1)[1][32], int *arrive) {
+    if (LPS) {
+        for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+            theta_body<R, WPS, U, false>(a, g, sh1, arrive);
+            if (WPS > 1) __syncthreads();
+        }
+        if (!grid_barrier(gb, gridDim.x)) return false;
+    }
+    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        step_body<R, WPS, U, 1, false>(a, g, sh, arrive);
+        if (WPS > 1) __syncthreads();
+    }
+    return true;
+}
+
 template <class R, int WPS, int U, bool LPS>
 __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::MINB : 1)
-    k_persist(StepArgs<R> a, typename Tr<R>::V4 *b0, typename Tr<R>::V4 *b1, int nsteps, GridBar *gb,
-              int64_t ngroups) {
+    k_persist(const __grid_constant__ StepArgs<R> a0, const __grid_constant__ StepArgs<R> a1, int nsteps,
+              GridBar *gb, int64_t ngroups) {
     constexpr int NW = Split<WPS>::NW, SPB = Split<WPS>::SPB;
     __shared__ R sh[WPS > 1 ? NW : 1][3][32];
     __shared__ R sh1[WPS > 1 ? NW : 1][1][32];
@@ -1346,22 +1371,10 @@ __global__ void __launch_bounds__(Split<WPS>::BT, sizeof(R) == 4 ? Split<WPS>::M
         if (threadIdx.x < SPB) arrive[threadIdx.x] = 0;
         __syncthreads();
     }
-    const int64_t ts0 = a.ts;
     for (int s = 0; s < nsteps; ++s) {
-        a.xu = (s & 1) ? b1 : b0;
-        a.xn = (s & 1) ? b0 : b1;
-        a.ts = ts0 + s;
-        if (LPS) {
-            for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-                theta_body<R, WPS, U, false>(a, g, sh1, arrive);
-                if (WPS > 1) __syncthreads();
-            }
-            if (!grid_barrier(gb, gridDim.x)) return;
-        }
-        for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-            step_body<R, WPS, U, 1, false>(a, g, sh, arrive);
-            if (WPS > 1) __syncthreads();
-        }
+        const bool ok = (s & 1) ? persist_step<R, WPS, U, LPS>(a1, ngroups, gb, sh, sh1, arrive)
+                                : persist_step<R, WPS, U, LPS>(a0, ngroups, gb, sh, sh1, arrive);
+        if (!ok) return;
         if (s + 1 < nsteps && !grid_barrier(gb, gridDim.x)) return;
     }
 }
@@ -2566,8 +2579,7 @@ int64_t flip_free_run(const pd_env *env, int64_t maxn) {
 template <class R, int WPS, int U, bool LPS>
 pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
     constexpr int BT = Split<WPS>::BT, SPB = Split<WPS>::SPB;
-    void (*kern)(StepArgs<R>, typename Tr<R>::V4 *, typename Tr<R>::V4 *, int, GridBar *, int64_t) =
-        k_persist<R, WPS, U, LPS>;
+    void (*kern)(const StepArgs<R>, const StepArgs<R>, int, GridBar *, int64_t) = k_persist<R, WPS, U, LPS>;
     int64_t ngroups = ((env->N + 31) / 32 + SPB - 1) / SPB;
     int per_sm = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, 0));
@@ -2581,13 +2593,19 @@ pd_status persist_try(pd_env *env, Fast<R> &F, int nsteps, bool *done) {
         PD_TRY(F.gbar.alloc(1));
         CK(cudaMemsetAsync(F.gbar.p, 0, sizeof(GridBar), env->st));
     }
-    StepArgs<R> a = args(env, F);
-    a.swz_g = 0;  // the cooperative grid covers the slices in order
-    a.dir_vel = a.dir_pos = dir_bits(env);
-    a.ts = env->ts + 1;
+    StepArgs<R> a0 = args(env, F);
+    a0.swz_g = 0;  // the cooperative grid covers the slices in order
+    a0.dir_vel = a0.dir_pos = dir_bits(env);
+    a0.ts = env->ts + 1;
+    // even steps read the current record buffer and write the other one
     typename Tr<R>::V4 *b0 = F.xu[F.cur].p, *b1 = F.xu[1 - F.cur].p;
+    a0.xu = b0;
+    a0.xn = b1;
+    StepArgs<R> a1 = a0;
+    a1.xu = b1;
+    a1.xn = b0;
     GridBar *gb = F.gbar.p;
-    void *kargs[] = {&a, &b0, &b1, &nsteps, &gb, &ngroups};
+    void *kargs[] = {&a0, &a1, &nsteps, &gb, &ngroups};
     CK(cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)blocks), dim3(BT), kargs, 0, env->st));
     add_launches(1);
     for (int k = 0; k < nsteps; ++k) advance_bc_clock(env);
