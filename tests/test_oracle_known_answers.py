@@ -133,6 +133,45 @@ def test_momentum_conservation(oracle):
     assert np.abs(mf.sum(axis=1)).max() <= 1e-9 * np.abs(mf).sum()
 
 
+def pmb_energy(env):
+    """Kinetic plus bond energy of a bond-based block.  The reference's
+    per-bond term (t = c s, bond_based.jl:195-197; f_i += t/(2|Y|) Y V_j /
+    rho_i from each of the bond's two visits, general_material.jl:340-360)
+    is the force of the pair potential phi = c |xi| s^2 V_i V_j / 2, so
+    velocity-Verlet must conserve sum m v^2 / 2 + sum over intact bonds of
+    phi to O(dt^2)."""
+    B = env.blocks[0]
+    fam = B.family
+    i = np.broadcast_to(np.arange(B.n), fam.shape)[fam > 0]
+    j = fam[fam > 0] - 1
+    xi = B.x[:, j] - B.x[:, i]
+    Y = env.y[:, j] - env.y[:, i]
+    lx = np.sqrt((xi * xi).sum(axis=0))
+    s = (np.sqrt((Y * Y).sum(axis=0)) - lx) / lx
+    live = B.intact[fam > 0] > 0
+    phi = 0.5 * B.c[0, 0] * lx * s * s * B.vol[i] * B.vol[j]
+    bond = 0.5 * phi[live].sum()  # every bond is listed in both families
+    kinetic = 0.5 * (env.mass * (env.v * env.v).sum(axis=0)).sum()
+    return kinetic, bond
+
+
+def test_pmb_energy_is_conserved(oracle):
+    w = configs.pmb_cube(n=8, spacing=1e-3, jitter=1e-5, peak=2.0, sigma=2e-3, cs=1.0)
+    env = oracle.OracleEnv(w["materials"], [], [], w["dt"])
+    env.update_acc()
+    k0, b0 = pmb_energy(env)
+    assert b0 == 0.0 and k0 > 0.0
+    energies = []
+    for _ in range(300):
+        env.vv_step()
+        energies.append(pmb_energy(env))
+    assert env.blocks[0].intact.sum() == (env.blocks[0].family > 0).sum()  # nothing broke
+    total = np.array([k + b for k, b in energies])
+    # the pulse's energy has moved into the bonds, and the sum has stayed put
+    assert max(b for _, b in energies) > 0.2 * k0
+    assert np.abs(total - k0).max() <= 1e-4 * k0, np.abs(total - k0).max() / k0
+
+
 @pytest.mark.parametrize("kind", ["pmb", "lps"])
 def test_gather_order_reproduces_serial_loop(oracle, kind):
     """The GPU's per-particle A/B/C gather equals the reference's serial
