@@ -172,6 +172,58 @@ def test_pmb_energy_is_conserved(oracle):
     assert np.abs(total - k0).max() <= 1e-4 * k0, np.abs(total - k0).max() / k0
 
 
+def lps_energy(env):
+    """Kinetic plus strain energy of a state-based block: the linear
+    peridynamic solid's W_i = K theta_i^2 / 2 + 15 G / (2 m_i) sum_j
+    omega (e - theta_i |xi| / 3)^2 V_j with omega = 1/|xi|, m_i = sum_j
+    |xi| V_j (peri.jl:342-354) and theta_i = 3/m_i sum_j e V_j
+    (peri.jl:155-172), computed here from the current positions.  Its
+    gradient is the reference's bond term t = (3K - 5G)(theta_i/m_i +
+    theta_j/m_j) omega |xi| + 15 G e omega (1/m_i + 1/m_j)
+    (ordinary_state_based.jl:176-187)."""
+    B = env.blocks[0]
+    fam = B.family
+    i = np.broadcast_to(np.arange(B.n), fam.shape)[fam > 0]
+    j = fam[fam > 0] - 1
+    xi = B.x[:, j] - B.x[:, i]
+    Y = env.y[:, j] - env.y[:, i]
+    lx = np.sqrt((xi * xi).sum(axis=0))
+    e = np.sqrt((Y * Y).sum(axis=0)) - lx
+    live = B.intact[fam > 0] > 0
+    il, vl = i[live], B.vol[j[live]]
+    m = np.zeros(B.n)
+    np.add.at(m, il, lx[live] * vl)
+    theta = np.zeros(B.n)
+    np.add.at(theta, il, e[live] * vl)
+    theta *= 3.0 / m
+    ed = e[live] - theta[il] * lx[live] / 3.0
+    dev = np.zeros(B.n)
+    np.add.at(dev, il, ed * ed / lx[live] * vl)
+    K, G = B.K[0, 0], B.G[0, 0]
+    strain = (B.vol * (0.5 * K * theta * theta + 7.5 * G / m * dev)).sum()
+    kinetic = 0.5 * (env.mass * (env.v * env.v).sum(axis=0)).sum()
+    return kinetic, strain
+
+
+def test_lps_energy_is_conserved(oracle):
+    x, vol = lattice.cuboid(8, 8, 8, 1.0e-3, jitter=1.0e-5, seed=3)
+    gen = GeneralMaterial(x.copy(order="F"), lattice.gaussian_pulse(x, 2.0, 2.0e-3), x, vol,
+                          np.ones(x.shape[1], dtype=np.int64), 3.015e-3, max_neigh=200)
+    mat = PeridynamicsMaterial(gen, OrdinaryStateBasedSpecific([14.9e9], [9.0e9], [1.0], [2200.0]))
+    env = oracle.OracleEnv([mat], [], [], 1.0e-8)
+    env.update_acc()
+    k0, s0 = lps_energy(env)
+    assert s0 == 0.0 and k0 > 0.0
+    energies = []
+    for _ in range(300):
+        env.vv_step()
+        energies.append(lps_energy(env))
+    assert env.blocks[0].intact.sum() == (env.blocks[0].family > 0).sum()  # nothing broke
+    total = np.array([k + s for k, s in energies])
+    assert max(s for _, s in energies) > 0.2 * k0
+    assert np.abs(total - k0).max() <= 1e-4 * k0, np.abs(total - k0).max() / k0
+
+
 @pytest.mark.parametrize("kind", ["pmb", "lps"])
 def test_gather_order_reproduces_serial_loop(oracle, kind):
     """The GPU's per-particle A/B/C gather equals the reference's serial
