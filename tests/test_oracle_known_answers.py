@@ -6,8 +6,8 @@ import math
 import numpy as np
 import pytest
 
-from peridyn_b200 import (BondBasedSpecific, GeneralMaterial, OrdinaryStateBasedSpecific, PeridynamicsMaterial,
-                          configs, julia_pow_int, lattice, make_matrix)
+from peridyn_b200 import (BondBasedSpecific, GeneralMaterial, NonLinearSpringContactModel, OrdinaryStateBasedSpecific,
+                          PeridynamicsMaterial, configs, julia_pow_int, lattice, make_matrix)
 from tests import gather_order
 
 
@@ -222,6 +222,67 @@ def test_lps_energy_is_conserved(oracle):
     total = np.array([k + s for k, s in energies])
     assert max(s for _, s in energies) > 0.2 * k0
     assert np.abs(total - k0).max() <= 1e-4 * k0, np.abs(total - k0).max() / k0
+
+
+def test_contact12_energy_is_conserved(oracle):
+    """Two bond-based cubes pressed together across a 0.9-spacing gap with
+    nonlinear contact (exponent p = 2, stiffness 15 c).  The contact term
+    (nonlinearspring.jl:124-145: K ((d - r)/d)^p / (r + 1e-10) dr, applied
+    as F V2_j / rho1_i and -F V1_i / rho2_j, contacts.jl:210-247) is the
+    force of the pair potential V1_i V2_j K d/(p+1) (1 - r/d)^(p+1) for
+    r < d (the 1e-10 shifts it by ~1e-7 relative), so kinetic + bond +
+    contact energy must stay put while the overlap pushes the cubes apart.
+    Neighbours are rebuilt every step, and max_neighs exceeds the partner
+    block's size, so every pair closer than d is listed."""
+    sp, hf, K, rho = 1.0e-3, 3.015, 14.9e9, 2200.0
+
+    def cube(origin, vx, t):
+        x, vol = lattice.cuboid(5, 5, 5, sp, origin=origin, jitter=1e-5, seed=t + 2)
+        v = np.zeros_like(x, order="F")
+        v[0] = vx
+        gen = GeneralMaterial(x.copy(order="F"), v, x, vol, np.full(x.shape[1], t, dtype=np.int64), hf * sp,
+                              max_neigh=200)
+        return PeridynamicsMaterial(gen, BondBasedSpecific([K], [1.0], [rho]), name=f"cube{t}")
+
+    m1, m2 = cube((0.0, 0.0, 0.0), 5.0, 1), cube((4.9 * sp, 0.0, 0.0), -5.0, 2)
+    c = 18 * K / math.pi / julia_pow_int(hf * sp, 4)
+    con = NonLinearSpringContactModel(2.0, 15 * c, m1, m2, distanceX=3.0, max_neighs=200)
+    env = oracle.OracleEnv([m1, m2], [con], [], 1e-8)
+    d, p, Kc = con.equi_dist, 2.0, 15 * c
+
+    def energy():
+        kinetic = 0.5 * (env.mass * (env.v * env.v).sum(axis=0)).sum()
+        bond = 0.0
+        for B in env.blocks:
+            fam = B.family
+            i = np.broadcast_to(np.arange(B.n), fam.shape)[fam > 0]
+            j = fam[fam > 0] - 1
+            y = env.y[:, B.off:B.off + B.n]
+            xi, Y = B.x[:, j] - B.x[:, i], y[:, j] - y[:, i]
+            lx = np.sqrt((xi * xi).sum(axis=0))
+            s = (np.sqrt((Y * Y).sum(axis=0)) - lx) / lx
+            live = B.intact[fam > 0] > 0
+            bond += 0.25 * (B.c[0, 0] * lx * s * s * B.vol[i] * B.vol[j])[live].sum()
+        B1, B2 = env.blocks
+        y1, y2 = env.y[:, B1.off:B1.off + B1.n], env.y[:, B2.off:B2.off + B2.n]
+        r = np.sqrt(((y1[:, :, None] - y2[:, None, :]) ** 2).sum(axis=0))
+        w = np.clip(1.0 - r / d, 0.0, None)
+        contact = (B1.vol[:, None] * B2.vol[None, :] * Kc * d / (p + 1) * w ** (p + 1)).sum()
+        return kinetic, bond, contact
+
+    env.update_neighs()
+    env.update_acc()
+    k0, b0, c0 = energy()
+    assert c0 > 10 * k0  # the cubes start overlapped by 0.1 d
+    e0 = k0 + b0 + c0
+    energies = []
+    for _ in range(600):
+        env.update_neighs()
+        env.vv_step()
+        energies.append(energy())
+    total = np.array([sum(e) for e in energies])
+    assert energies[-1][2] == 0.0 and energies[-1][0] > 0.5 * e0  # pushed apart: contact energy back in motion
+    assert np.abs(total - e0).max() <= 1e-4 * e0, np.abs(total - e0).max() / e0
 
 
 @pytest.mark.parametrize("kind", ["pmb", "lps"])
