@@ -8,6 +8,12 @@
  * relative to the PeriDyn source tree, src/).  Index arithmetic is 1-based
  * in the data (family entries, neighbour lists) exactly as in Julia; the C
  * loops themselves are 0-based.
+ *
+ * Parity unpinned by the reference itself: the reference is Julia (not
+ * available here) and ships no tests or golden vectors, so this
+ * restatement is pinned by analytical known answers instead (homogeneous
+ * stretch, lattice neighbour counts, momentum and energy conservation of
+ * the bond, state-based and contact terms).
  */
 #include "pd_oracle.h"
 
