@@ -2,7 +2,7 @@
 (4.125 B per intact directed bond and per bond sweep, 84 / 168 B per
 particle, 8 B more for state-based blocks),
 the compute roofline's arithmetic, the bounded CPU sample of the batched
-workload and its cube-edge variant."""
+workload and its cube-edge variant, and the serving sample's stream."""
 import bench
 from peridyn_b200 import configs
 
@@ -57,3 +57,41 @@ def test_cube_edge_variant_draws_one_edge_per_specimen():
     assert w["workload"] == "batched_6_pmb_cubes"
     # the per-axis default keeps its draws (same specimens as before)
     assert configs.batched_cubes(nspec=6)["workload"] == "batched_6_pmb"
+
+
+def test_serving_sample_reports_the_stream(monkeypatch):
+    """The bench line's serving object: one warm-up stream of 4 small jobs,
+    then the measured stream of args.jobs FP32C jobs at their Poisson
+    arrival times, its latency percentiles and aggregate rate carried over
+    (a fake server here: no GPU call)."""
+    import types
+
+    import peridyn_b200 as pb
+
+    calls = []
+
+    class FakeServer:
+        def __init__(self, device, max_active):
+            calls.append(("server", device, max_active))
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+    def fake_stream(srv, jobs, arrivals):
+        calls.append(("stream", len(jobs), list(arrivals)))
+        assert all(j["precision"] == "fp32c" for j in jobs)
+        return [], {"jobs": len(jobs), "wall_s": 2.0, "latency_ms": {"p50": 10.0, "p99": 20.0, "max": 21.0},
+                    "bond_updates": 8, "bond_updates_per_s": 4.0}
+
+    monkeypatch.setattr(pb, "Server", FakeServer)
+    monkeypatch.setattr(pb, "serve_stream", fake_stream)
+    args = types.SimpleNamespace(jobs=3, max_active=5)
+    out = bench.serving_sample(args, 0)
+    assert calls[0] == ("server", 0, 5)
+    assert calls[1][:2] == ("stream", 4) and calls[1][2] == [0.0] * 4  # warm-up, submitted at once
+    assert calls[2][1] == 3 and calls[2][2] == sorted(calls[2][2]) and calls[2][2][-1] > 0.0
+    assert out["jobs"] == 3 and out["latency_ms"]["p99"] == 20.0
+    assert out["aggregate_bond_updates_per_s"] == 4.0 and out["workload"] == "serving_3_jobs_poisson50"
