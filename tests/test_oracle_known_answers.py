@@ -411,6 +411,40 @@ def test_contact12_neighs_bruteforce(oracle):
         assert np.array_equal(nb[:, i], expect)
 
 
+def test_fix_and_tofro_bcs_known_answers(oracle):
+    """FixBC.jl:46-65: the masked coordinates stay at their t0 snapshot with
+    zero velocity.  ToFroBC.jl:51-111 within velocity_verlet.jl:57-89: each
+    step moves the masked coordinates by dt * direction * rate from where
+    the previous step left them and sets v = direction * rate; check! after
+    the step flips the direction when time_step > applyafter and time_step
+    % freq == 0 (time_step counted before its increment).  Unconstrained
+    coordinates (dims false) move freely."""
+    from peridyn_b200 import FixBC, ToFroBC
+
+    mat = lattice_block(6, 1.0e-3, 3.015, kind="lps")
+    x = mat.general.x
+    left, right = x[0] < x[0].min() + 1.5e-3, x[0] > x[0].max() - 1.5e-3
+    rate = np.array([2.0, 0.3, 0.0])
+    bcs = [FixBC(left), ToFroBC(right, rate, 4, dims=(True, True, False), applyafter=2)]
+    env = oracle.OracleEnv([mat], [], bcs, 1.0e-8)
+    env.apply_bc_at0()
+    y0 = env.y.copy()
+    il, ir = np.nonzero(left)[0], np.nonzero(right)[0]
+    direction, moved = 1, np.zeros(3)
+    for ts in range(14):
+        env.vv_step()
+        moved += env.dt * direction * rate
+        assert np.array_equal(env.y[:, il], y0[:, il]) and np.all(env.v[:, il] == 0.0)
+        for d in (0, 1):
+            assert np.allclose(env.y[d, ir], y0[d, ir] + moved[d], rtol=0, atol=1e-15)
+            assert np.all(env.v[d, ir] == direction * rate[d])
+        if ts > 2 and ts % 4 == 0:
+            direction = -direction
+    # flips after steps 4, 8 and 12: the run ends moving in the negative direction
+    assert direction == -1 and np.all(env.v[0, ir] == -rate[0])
+    assert not np.array_equal(env.y[2, ir], y0[2, ir])  # z is not constrained and has moved
+
+
 def test_scaling_bcs_known_answers(oracle):
     # DeltaScaleBC.jl:52-55: y = (last - fix) * (1 + scale*dt*time_step) + fix
     from tests.cases import bar_with_bcs
